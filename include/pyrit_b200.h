@@ -1,0 +1,201 @@
+/* pyrit_b200 -- B200-native (sm_100a) sparse-voxel-DAG build for Pyrit.
+ *
+ * C ABI that replaces the GPU build seam of the reference, src/gpu_build.zig
+ * (build :94-96, buildChunks :119-122, downsample :128-131, Built :26-47,
+ * Exec :14-23). Plain pointers and sizes only; device buffers are passed as
+ * 64-bit device addresses exactly like the reference's `u64` fields.
+ *
+ * Output layout (bit-exact with the reference GPU build):
+ *   nodes   u32[node_words]  level by level (8^3 nodes first, root last); a node is
+ *           [child mask, saturating voxel count, one ref per child]; refs of 8^3
+ *           nodes are leaf indices, all others word offsets (src/device/dag.zig:1-16)
+ *   leaves  u64[leaf_count]  unique 4^3 brick masks in first-occurrence Morton order
+ *   keys    u64[voxel_count] sorted unique voxel keys (brick Morton << 6 | bit), with
+ *           the chunk number above 3*log2_size bits in chunk batches
+ *   attrs   u32[voxel_count] attributes in Morton (= depth-first) order
+ *   prims   {u32 node, u32 attr_base, u64 cell}[prim_count], aabbs f32[prim_count][6]
+ *           (src/device/types.zig:518-526) at edge 2^rt_log2
+ * All output buffers belong to the caller; free them with pyrb_built_free.
+ *
+ * Thread safety: one build at a time per stream; different streams may build
+ * concurrently. No call synchronises the device, only the caller's stream.
+ */
+#ifndef PYRIT_B200_H
+#define PYRIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define PYRB_API __declspec(dllexport)
+#else
+#define PYRB_API __attribute__((visibility("default")))
+#endif
+
+/* Result codes: the PyrResult values of include/pyrit.h:343-353 that the build can return. */
+typedef int32_t pyrb_result;
+#define PYRB_OK                      0
+#define PYRB_ERROR_INVALID_ARGUMENT -1
+#define PYRB_ERROR_OUT_OF_MEMORY    -3
+#define PYRB_ERROR_CUDA             -6
+
+/* Memory and stream of a build (replaces gpu_build.Exec, src/gpu_build.zig:14-23).
+ * alloc/free may be NULL: the library then allocates stream-ordered from its own
+ * device memory pool (cudaMallocAsync on `stream`), which is what the reference's
+ * Context.execOn does with cuMemAllocAsync (src/context.zig:873-911).
+ * alloc returns 0 on failure. free must accept pointers returned by alloc. */
+typedef struct pyrb_exec {
+    void*    ctx;
+    void*    stream;                                  /* cudaStream_t / CUstream; NULL = legacy default stream */
+    uint64_t (*alloc)(void* ctx, uint64_t bytes);
+    void     (*free)(void* ctx, uint64_t ptr);
+} pyrb_exec;
+
+/* gpu_build.Built (src/gpu_build.zig:26-47); all buffers are device memory owned by the caller. */
+typedef struct pyrb_built {
+    uint32_t log2_size;
+    uint32_t rt_log2;
+    uint64_t nodes;
+    uint32_t node_words;
+    uint32_t root;
+    uint64_t leaves;
+    uint32_t leaf_count;
+    uint32_t reserved0;
+    uint64_t keys;
+    uint64_t attrs;
+    uint32_t voxel_count;
+    uint32_t reserved1;
+    uint64_t prims;
+    uint64_t aabbs;
+    uint32_t prim_count;
+    uint32_t reserved2;
+} pyrb_built;
+
+/* Build statistics of the last successful build on the calling thread. */
+typedef struct pyrb_stats {
+    uint32_t brick_count;            /* non-empty 4^3 bricks (B) */
+    uint32_t level_parents[24];      /* P_l: parent nodes of level l before dedup (l = 2 .. log2-1) */
+    uint32_t level_unique[24];       /* U_l: unique nodes of level l */
+    uint32_t sort_passes;            /* radix passes of the onesweep sort */
+    uint32_t radix_bits;             /* widest digit */
+    uint32_t kernel_launches;        /* kernels launched by the build */
+    uint32_t reserved;
+    uint64_t scratch_bytes;          /* device scratch of the build (without outputs) */
+    uint64_t output_bytes;           /* device bytes of the output buffers (upper bounds) */
+} pyrb_stats;
+
+/* gpu_build.build (src/gpu_build.zig:94-96): a DAG from n_old already sorted unique
+ * voxels (old_keys u64 / old_vals u32, e.g. the previous version of an editable
+ * geometry; copied, not consumed) and n_new entries `edits` (PyrVoxel[n_new],
+ * {int32 x, y, z; uint32 attribute}) in any order. New entries override old ones,
+ * the last of equal coordinates wins, attribute 0 deletes, coordinates outside
+ * [0, 2^log2_size) are dropped. log2_size in [3, 20]; rt_log2_req is clamped to
+ * [3, log2_size]. Synchronises `stream` once at the end to read the counts. */
+PYRB_API pyrb_result pyrb_build(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                uint64_t old_keys, uint64_t old_vals, uint32_t n_old,
+                                uint64_t edits, uint32_t n_new, pyrb_built* out);
+
+/* Asynchronous form of pyrb_build (no synchronisation at all): the counts are copied
+ * into `host_counts` (pinned host memory, PYRB_COUNTS_WORDS u32) on the stream. Once
+ * the stream has passed that copy, pyrb_build_finish fills the counts of `out`
+ * (node_words, root, leaf_count, voxel_count, prim_count) and reports device-side
+ * errors. The buffer pointers of `out` are valid immediately in stream order.
+ * Scratch is released stream-ordered, so this form needs the default allocator or
+ * stream-ordered alloc/free callbacks. */
+#define PYRB_COUNTS_WORDS 176
+PYRB_API pyrb_result pyrb_build_async(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                      uint64_t old_keys, uint64_t old_vals, uint32_t n_old,
+                                      uint64_t edits, uint32_t n_new, uint32_t* host_counts, pyrb_built* out);
+PYRB_API pyrb_result pyrb_build_finish(const uint32_t* host_counts, pyrb_built* out);
+
+/* gpu_build.ChunkBatch (src/gpu_build.zig:105-111): `voxels` holds `count` segments of
+ * `capacity` PyrVoxels in chunk-local coordinates; segment c is filled up to
+ * offsets[c+1] - offsets[c] (device u32[count+1], exclusive prefix sum), total = offsets[count]. */
+typedef struct pyrb_chunk_batch {
+    uint32_t count;
+    uint32_t capacity;
+    uint64_t voxels;
+    uint64_t offsets;
+    uint32_t total;
+    uint32_t reserved;
+} pyrb_chunk_batch;
+
+/* gpu_build.buildChunks (src/gpu_build.zig:119-122): all chunks in one build sharing
+ * node, leaf and attribute buffers (dedup across chunks per level). Host outputs
+ * roots/first_voxel/first_prim (u32[count]; 0xFFFFFFFF = empty chunk). */
+PYRB_API pyrb_result pyrb_build_chunks(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                       const pyrb_chunk_batch* batch, uint32_t* roots, uint32_t* first_voxel,
+                                       uint32_t* first_prim, pyrb_built* out);
+
+/* World path with the pyr_world_edit overlay merged into the build
+ * (replaces worldedit apply/compact/append, src/device/worldedit.zig:26-90, and the
+ * buildChunks call of World.gpuWorkImpl, src/world.zig:984-1020). `counts` (device
+ * u32[count]) are the generator's per-chunk counts (PyrWorldGenParams.counts);
+ * `edits` (device PyrVoxel[]) hold each chunk's overlay entries in chunk-local
+ * coordinates, chunk c at [edit_offsets[c], edit_offsets[c+1]) (device u32[count+1]);
+ * edit_total = edit_offsets[count] (host copy, sizes the scratch).
+ * Edits act as if applied after the generated voxels in list order: attribute 0
+ * removes, anything else sets. Counts above capacity are clamped (the reference
+ * grows the capacity and retries, src/world.zig:989-996). */
+PYRB_API pyrb_result pyrb_build_chunks_edits(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                             uint32_t count, uint32_t capacity, uint64_t voxels, uint64_t counts,
+                                             uint64_t edits, uint64_t edit_offsets, uint32_t edit_total,
+                                             uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim,
+                                             pyrb_built* out);
+
+/* gpu_build.downsample (src/gpu_build.zig:128-131): LOD of edge 2^(log2_src - shift)
+ * from the sorted voxels of an editable geometry; per coarse cell the source voxel
+ * with the largest key wins. shift >= 1 and shift + 3 <= log2_src. */
+PYRB_API pyrb_result pyrb_downsample(const pyrb_exec* e, uint32_t log2_src, uint32_t rt_log2_req, uint64_t src_keys,
+                                     uint64_t src_vals, uint32_t n_src, uint32_t shift, pyrb_built* out);
+
+/* pyr_geometry_build's input handling (include/pyrit.h:464-466, src/context.zig:918-928):
+ * like pyrb_build with n_old = 0, but with PYRB_BUILD_HOST_INPUT `voxels` is a host
+ * pointer that is uploaded on the stream first. */
+#define PYRB_BUILD_HOST_INPUT 0x1u
+PYRB_API pyrb_result pyrb_geometry_build(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                         const void* voxels, uint32_t count, uint32_t flags, pyrb_built* out);
+
+/* Built.free (src/gpu_build.zig:42-46): frees the six output buffers (stream-ordered
+ * with the default allocator) and zeroes `b`. */
+PYRB_API void pyrb_built_free(const pyrb_exec* e, pyrb_built* b);
+
+/* Copies the statistics of the calling thread's last successful build. */
+PYRB_API void pyrb_last_stats(pyrb_stats* out);
+
+/* Message of the calling thread's last error (diag.zig:17-38 / pyr_error_message). */
+PYRB_API const char* pyrb_error_message(void);
+PYRB_API const char* pyrb_result_string(pyrb_result r);
+
+/* Tuning of the sort and the dedup tables (digit width 4, 8 or 11 bits; keys per
+ * sort tile 1024, 2048 or 4096; hash load factor in percent, 25..90). Applies to
+ * builds started afterwards on any thread. Returns PYRB_ERROR_INVALID_ARGUMENT for
+ * unsupported values. */
+typedef struct pyrb_tuning {
+    uint32_t radix_bits;
+    uint32_t tile_keys;
+    uint32_t load_factor_pct;
+    uint32_t reserved;
+} pyrb_tuning;
+PYRB_API pyrb_result pyrb_set_tuning(const pyrb_tuning* t);
+PYRB_API void pyrb_get_tuning(pyrb_tuning* t);
+
+/* Per-stage CUDA events of the calling thread's builds (off by default). After the
+ * stream of the last build has synchronised, pyrb_profile_read returns the number of
+ * stages and writes up to `cap` durations (ms) and NUL-terminated stage names
+ * (`name_len` bytes each, e.g. "sort_pass:1", "node_build:3"). */
+PYRB_API void pyrb_profile_enable(int on);
+PYRB_API uint32_t pyrb_profile_read(float* ms, char* names, uint32_t name_len, uint32_t cap);
+
+/* Library version (major << 16 | minor). */
+PYRB_API uint32_t pyrb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYRIT_B200_H */

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 
 CUDA_SOURCES = ["pyrb_build.cu"]
-CUDA_HEADERS = ["pyrb_device.cuh", "pyrb_internal.h"]
+CUDA_HEADERS = ["pyrb_device.cuh", "pyrb_internal.h", "pyrb_kernels.cuh"]
 WORKLOAD_SOURCES = ["workloads.cpp"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,798 @@
+// Host orchestration of the DAG build and the C ABI of include/pyrit_b200.h.
+//
+// A build is one stream-ordered sequence of kernels (no host round trip until the
+// final read of the counters): every buffer is sized from upper bounds that the
+// host can compute from the input sizes, the real counts stay on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "pyrit_b200.h"
+#include "pyrb_internal.h"
+#include "pyrb_kernels.cuh"
+
+using namespace pyrb;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// diagnostics (thread-local like the reference's diag.zig)
+// ---------------------------------------------------------------------------
+thread_local char g_msg[512] = "";
+thread_local pyrb_stats g_stats = {};
+
+pyrb_result fail(pyrb_result r, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+    va_end(ap);
+    return r;
+}
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t err_ = (call);                                                                 \
+        if (err_ != cudaSuccess) return fail(PYRB_ERROR_CUDA, "%s: %s", #call, cudaGetErrorString(err_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// tuning
+// ---------------------------------------------------------------------------
+std::atomic<uint32_t> g_radix_bits{8};
+std::atomic<uint32_t> g_tile_keys{4096};
+std::atomic<uint32_t> g_load_pct{50};
+
+// ---------------------------------------------------------------------------
+// memory: caller callbacks, else a library-owned stream-ordered pool per device
+// ---------------------------------------------------------------------------
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+
+cudaMemPool_t device_pool(int dev) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+        uint64_t thr = ~0ull;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr);
+        g_pools[dev] = p;
+    }
+    return g_pools[dev];
+}
+
+struct Mem {
+    const pyrb_exec* e;
+    cudaStream_t st;
+    cudaMemPool_t pool = nullptr;
+
+    uint64_t get(uint64_t bytes) {
+        bytes = std::max<uint64_t>(bytes, 16);
+        if (e && e->alloc) return e->alloc(e->ctx, bytes);
+        if (!pool) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            pool = device_pool(dev);
+            if (!pool) return 0;
+        }
+        void* p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, bytes, pool, st) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return reinterpret_cast<uint64_t>(p);
+    }
+    void put(uint64_t p) {
+        if (!p) return;
+        if (e && e->free) e->free(e->ctx, p);
+        else cudaFreeAsync(reinterpret_cast<void*>(p), st);
+    }
+};
+
+uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+uint32_t next_pow2(uint64_t v, uint32_t minimum) {
+    uint64_t c = minimum;
+    while (c < v) c <<= 1;
+    return uint32_t(c);
+}
+
+// Bump layout of one scratch block.
+struct Layout {
+    uint64_t size = 0;
+    uint64_t take(uint64_t bytes) {
+        uint64_t off = align_up(size, 256);
+        size = off + std::max<uint64_t>(bytes, 16);
+        return off;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// job description
+// ---------------------------------------------------------------------------
+struct Job {
+    uint32_t mode = kModePlain;
+    uint32_t log2 = 0, rt_req = 0, K = 1;
+    uint64_t old_keys = 0, old_vals = 0;
+    uint32_t n_old = 0;
+    uint64_t voxels = 0;
+    uint32_t n_new = 0;
+    uint32_t capacity = 0;
+    uint64_t offsets = 0;
+    uint32_t total = 0;
+    uint64_t gen_counts = 0, edits = 0, edit_offsets = 0;
+    uint32_t edit_total = 0;
+    uint64_t src_keys = 0, src_vals = 0;
+    uint32_t shift = 0;
+    uint32_t* roots = nullptr;
+    uint32_t* first_voxel = nullptr;
+    uint32_t* first_prim = nullptr;
+};
+
+// Optional per-stage CUDA events (pyrb_profile_enable): one event after every
+// launch of a build; durations are read after the stream has synchronised.
+thread_local bool g_prof_on = false;
+thread_local std::vector<cudaEvent_t> g_prof_events;
+thread_local std::vector<std::pair<const char*, uint32_t>> g_prof_names;
+
+// PYRB_SYNC_CHECK=1 synchronises after every launch and names the first stage
+// that reports an error (like the reference's PYR_CREATE_DEBUG, src/context.zig:741-745).
+bool sync_check_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("PYRB_SYNC_CHECK");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
+thread_local char g_failed_stage[64] = "";
+
+struct Prof {
+    cudaStream_t st;
+    size_t n = 0;
+    explicit Prof(cudaStream_t s) : st(s) {
+        g_failed_stage[0] = 0;
+        if (!g_prof_on) return;
+        g_prof_names.clear();
+        record();
+    }
+    void record() {
+        if (g_prof_events.size() <= n) {
+            cudaEvent_t ev;
+            cudaEventCreate(&ev);
+            g_prof_events.push_back(ev);
+        }
+        cudaEventRecord(g_prof_events[n], st);
+        ++n;
+    }
+    void mark(const char* name, uint32_t arg = 0) {
+        if (sync_check_enabled() && !g_failed_stage[0]) {
+            cudaError_t err = cudaStreamSynchronize(st);
+            if (err == cudaSuccess) err = cudaGetLastError();
+            if (err != cudaSuccess) {
+                snprintf(g_failed_stage, sizeof(g_failed_stage), "%s:%u", name, arg);
+                fprintf(stderr, "pyrb: stage %s failed: %s\n", g_failed_stage, cudaGetErrorString(err));
+            }
+        }
+        if (!g_prof_on) return;
+        record();
+        g_prof_names.emplace_back(name, arg);
+    }
+};
+
+pyrb_result device_error(uint32_t bits) {
+    return fail(PYRB_ERROR_CUDA, "device-side build error 0x%x (%s%s%s)", bits,
+                (bits & kErrSpin) ? "look-back wait limit " : "", (bits & kErrTable) ? "dedup table full " : "",
+                (bits & kErrBound) ? "upper bound exceeded" : "");
+}
+
+void fill_counts(const uint32_t* ctr, pyrb_built* out) {
+    out->node_words = ctr[kCtrWords];
+    out->root = ctr[kCtrRoot];
+    out->leaf_count = ctr[kCtrLeaves];
+    out->voxel_count = ctr[kCtrUnique];
+    out->prim_count = ctr[kCtrPrims];
+}
+
+// meta: log2, rt, passes, radix bits, launches, scratch bytes (2 words), output bytes (2 words)
+void fill_stats(const uint32_t* ctr, const uint32_t* meta) {
+    pyrb_stats s = {};
+    s.brick_count = ctr[kCtrBricks];
+    for (uint32_t lv = 2; lv < meta[0] && lv < 24; ++lv) {
+        s.level_parents[lv] = ctr[kCtrParents + lv];
+        s.level_unique[lv] = ctr[kCtrUniqueLv + lv];
+    }
+    s.sort_passes = meta[2];
+    s.radix_bits = meta[3];
+    s.kernel_launches = meta[4];
+    std::memcpy(&s.scratch_bytes, meta + 5, 8);
+    std::memcpy(&s.output_bytes, meta + 7, 8);
+    g_stats = s;
+}
+
+template <int RB, int IT>
+cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
+    const size_t hist_smem = size_t(d.passes) * (1u << RB) * 4;
+    const size_t sort_smem = sort_smem_bytes<RB, IT>();
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        cudaFuncSetAttribute(k_encode_hist<RB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        cudaFuncSetAttribute(k_sort_pass<RB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
+    });
+    k_encode_hist<RB, IT><<<d.sort_tiles, kBlock, hist_smem, st>>>(d);
+    prof.mark("encode_hist");
+    for (uint32_t p = 0; p < d.passes; ++p) {
+        k_sort_pass<RB, IT><<<d.sort_tiles, kBlock, sort_smem, st>>>(d, p, p & 1);
+        prof.mark("sort_pass", p);
+    }
+    k_unique<IT><<<d.sort_tiles, kBlock, 0, st>>>(d, d.passes & 1);
+    prof.mark("unique");
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_any(uint32_t rb, uint32_t it, const BuildDesc& d, cudaStream_t st, Prof& prof) {
+    if (rb == 8 && it == 16) return launch_sort<8, 16>(d, st, prof);
+    if (rb == 8 && it == 8) return launch_sort<8, 8>(d, st, prof);
+    if (rb == 8 && it == 4) return launch_sort<8, 4>(d, st, prof);
+    if (rb == 4 && it == 16) return launch_sort<4, 16>(d, st, prof);
+    if (rb == 4 && it == 8) return launch_sort<4, 8>(d, st, prof);
+    if (rb == 4 && it == 4) return launch_sort<4, 4>(d, st, prof);
+    if (rb == 11 && it == 16) return launch_sort<11, 16>(d, st, prof);
+    if (rb == 11 && it == 8) return launch_sort<11, 8>(d, st, prof);
+    if (rb == 11 && it == 4) return launch_sort<11, 4>(d, st, prof);
+    return cudaErrorInvalidValue;
+}
+
+pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint32_t* host_counts = nullptr) {
+    if (!out) return fail(PYRB_ERROR_INVALID_ARGUMENT, "out is NULL");
+    std::memset(out, 0, sizeof(*out));
+    const uint32_t log2 = job.log2;
+    if (log2 < 3 || log2 > 20) return fail(PYRB_ERROR_INVALID_ARGUMENT, "log2_size must lie in [3, 20] (got %u)", log2);
+    const uint32_t lb = 3 * log2;
+    if (lb + 1 > 32)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT,
+                    "log2_size %u needs 64-bit sort keys; this build sorts 32-bit keys (log2_size <= 10)", log2);
+    const uint32_t K = job.K;
+    const bool chunked = job.mode == kModeChunks || job.mode == kModeChunksEdits;
+    if (chunked) {
+        uint32_t bits = 0;
+        while ((uint64_t(1) << bits) < K) ++bits;
+        if (lb + bits + 1 > 64) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many chunks for this chunk size");
+    }
+    const uint32_t rt = std::min(std::max(job.rt_req, 3u), log2);
+    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+    Mem mem{e, st};
+
+    // raw entries (upper bound for the chunk modes)
+    uint64_t n64 = 0;
+    switch (job.mode) {
+        case kModePlain: n64 = uint64_t(job.n_old) + job.n_new; break;
+        case kModeChunks: n64 = job.total; break;
+        case kModeChunksEdits: n64 = uint64_t(K) * job.capacity + job.edit_total; break;
+        default: n64 = job.n_new; break;
+    }
+    if (n64 >= (uint64_t(1) << 31)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many entries for one build (%llu)", (unsigned long long)n64);
+    const uint32_t n = uint32_t(n64);
+    const uint32_t nmax = std::max(n, 1u);
+
+    // tuning
+    const uint32_t rb = g_radix_bits.load();
+    const uint32_t tile_keys = g_tile_keys.load();
+    const uint32_t it = tile_keys / kBlock;
+    const uint32_t lf = g_load_pct.load();
+
+    BuildDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.mode = job.mode;
+    d.log2 = log2;
+    d.rt_log2 = rt;
+    d.lb = lb;
+    d.seg_count = K;
+    d.capacity = job.capacity;
+    d.shift = job.shift;
+    d.n_old = job.n_old;
+    d.n_new = job.n_new;
+    d.n_total = n;
+    d.top = log2 - 1;
+    d.old_keys = reinterpret_cast<const uint64_t*>(job.old_keys);
+    d.old_vals = reinterpret_cast<const uint32_t*>(job.old_vals);
+    d.voxels = reinterpret_cast<const uint4*>(job.voxels);
+    d.offsets = reinterpret_cast<const uint32_t*>(job.offsets);
+    d.gen_counts = reinterpret_cast<const uint32_t*>(job.gen_counts);
+    d.edits = reinterpret_cast<const uint4*>(job.edits);
+    d.edit_offsets = reinterpret_cast<const uint32_t*>(job.edit_offsets);
+    d.src_keys = reinterpret_cast<const uint64_t*>(job.src_keys);
+    d.src_vals = reinterpret_cast<const uint32_t*>(job.src_vals);
+    d.chunked = chunked ? 1u : 0u;
+
+    // digit plan over lb + 1 bits (the invalid bit on top)
+    const uint32_t sort_bits = lb + 1;
+    const uint32_t passes = (sort_bits + rb - 1) / rb;
+    d.passes = passes;
+    d.radix = 1u << rb;
+    {
+        uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 0;
+        for (uint32_t p = 0; p < passes; ++p) {
+            uint32_t b = base + (p < extra ? 1 : 0);
+            d.pass_shift[p] = sh;
+            d.pass_bits[p] = b;
+            sh += b;
+        }
+    }
+    d.tile_keys = tile_keys;
+    d.sort_tiles = (K == 1 ? (n + tile_keys - 1) / tile_keys : (n + tile_keys - 1) / tile_keys + K);
+    d.sort_tiles = std::max(d.sort_tiles, 1u);
+
+    // per-level upper bounds
+    auto cells = [&](uint32_t edge_log2) -> uint64_t {  // cells of edge 2^edge_log2 in all chunks
+        uint32_t e3 = 3 * (log2 - edge_log2);
+        if (e3 >= 40) return ~0ull >> 1;
+        return (uint64_t(1) << e3) * K;
+    };
+    const uint32_t B = uint32_t(std::max<uint64_t>(std::min<uint64_t>(nmax, cells(2)), 1));
+    uint32_t P[kMaxLevels + 2] = {};
+    uint64_t words = 2;
+    for (uint32_t lv = 2; lv < log2; ++lv) {
+        uint64_t prev = lv == 2 ? B : P[lv - 1];
+        P[lv] = uint32_t(std::max<uint64_t>(std::min<uint64_t>(prev, cells(lv + 1)), 1));
+        words += uint64_t(P[lv]) * kNodeStride;
+    }
+    if (words >= (uint64_t(1) << 32)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "node buffer bound exceeds 2^32 words");
+    d.brick_bound = B;
+    d.brick_tiles = std::max((nmax + kBrickTile - 1) / kBrickTile, 1u);
+    d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
+    d.leaf_cap = next_pow2(uint64_t(B) * 100 / lf + 1, 1024);
+    d.node_bound = uint32_t(words);
+    d.prim_bound = P[rt - 1];
+
+    // ---- scratch layout
+    Layout zl;  // zero-initialised region
+    const uint64_t o_counters = zl.take(kCtrCount * 4);
+    const uint64_t o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
+    const uint64_t o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
+    const uint64_t o_uniq_status = zl.take(uint64_t(d.sort_tiles) * 8);
+    const uint64_t o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
+    const uint64_t o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
+    const uint64_t o_leaf_table = zl.take(uint64_t(d.leaf_cap) * 16);
+    uint64_t o_table[kMaxLevels + 2], o_bstat[kMaxLevels + 2], o_ostat[kMaxLevels + 2];
+    uint32_t cap[kMaxLevels + 2], btiles[kMaxLevels + 2], otiles[kMaxLevels + 2];
+    for (uint32_t lv = 2; lv < log2; ++lv) {
+        cap[lv] = next_pow2(uint64_t(P[lv]) * 100 / lf + 1, 1024);
+        uint32_t child = lv == 2 ? B : P[lv - 1];
+        btiles[lv] = std::max((child + kNodeTile - 1) / kNodeTile, 1u);
+        otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
+        o_table[lv] = zl.take(uint64_t(cap[lv]) * 16);
+        o_bstat[lv] = zl.take(uint64_t(btiles[lv]) * 8);
+        o_ostat[lv] = zl.take(uint64_t(otiles[lv]) * 8);
+    }
+    const uint64_t zero_bytes = align_up(zl.size, 256);
+    Layout fl = zl;  // 0xFF region follows
+    fl.size = zero_bytes;
+    const uint64_t o_chunk_first = fl.take(uint64_t(K) * 4);
+    const uint64_t o_roots = fl.take(uint64_t(K) * 4);
+    const uint64_t o_prim_start = fl.take(uint64_t(K) * 4);
+    const uint64_t ff_bytes = align_up(fl.size, 256) - zero_bytes;
+    Layout ol = fl;
+    ol.size = zero_bytes + ff_bytes;
+    const uint64_t o_seg_entry = ol.take(uint64_t(K + 1) * 4);
+    const uint64_t o_seg_tile = ol.take(uint64_t(K + 1) * 4);
+    const uint64_t o_k0 = ol.take(uint64_t(nmax) * 4), o_v0 = ol.take(uint64_t(nmax) * 4);
+    const uint64_t o_k1 = ol.take(uint64_t(nmax) * 4), o_v1 = ol.take(uint64_t(nmax) * 4);
+    const uint64_t o_bkey = ol.take(uint64_t(B) * 8), o_bmask = ol.take(uint64_t(B) * 8);
+    const uint64_t o_bfirst = ol.take(uint64_t(B) * 4), o_bslot = ol.take(uint64_t(B) * 4);
+    // parent record sets: A for even offsets from level 2, B for odd
+    uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
+    uint64_t o_set[2][7];
+    for (int s = 0; s < 2; ++s) {
+        uint64_t m = std::max(setn[s], 1u);
+        o_set[s][0] = ol.take(m * 8);                 // key
+        o_set[s][1] = ol.take(m * 4);                 // cnt
+        o_set[s][2] = ol.take(m * 4);                 // first
+        o_set[s][3] = ol.take(m * 4);                 // slot
+        o_set[s][4] = ol.take(m * 8);                 // lo
+        o_set[s][5] = ol.take(m * 8);                 // hi
+        o_set[s][6] = ol.take(m * kNodeStride * 4);   // words
+    }
+    const uint64_t scratch_bytes = align_up(ol.size, 256);
+
+    // ---- allocations
+    uint64_t scratch = mem.get(scratch_bytes);
+    if (!scratch) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the build scratch (%llu bytes)", (unsigned long long)scratch_bytes);
+    uint64_t o_nodes = mem.get(uint64_t(d.node_bound) * 4);
+    uint64_t o_leaves = mem.get(uint64_t(B) * 8);
+    uint64_t o_ukey = mem.get(uint64_t(nmax) * 8);
+    uint64_t o_uval = mem.get(uint64_t(nmax) * 4);
+    uint64_t o_prims = mem.get(uint64_t(std::max(d.prim_bound, 1u)) * 16);
+    uint64_t o_aabbs = mem.get(uint64_t(std::max(d.prim_bound, 1u)) * 24);
+    auto release_outputs = [&] {
+        for (uint64_t p : {o_nodes, o_leaves, o_ukey, o_uval, o_prims, o_aabbs}) mem.put(p);
+    };
+    if (!o_nodes || !o_leaves || !o_ukey || !o_uval || !o_prims || !o_aabbs) {
+        release_outputs();
+        mem.put(scratch);
+        return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the build outputs");
+    }
+    auto at = [&](uint64_t off) { return reinterpret_cast<void*>(scratch + off); };
+    d.counters = static_cast<uint32_t*>(at(o_counters));
+    d.hist = static_cast<uint32_t*>(at(o_hist));
+    d.sort_status = static_cast<uint64_t*>(at(o_sort_status));
+    d.uniq_status = static_cast<uint64_t*>(at(o_uniq_status));
+    d.brick_status = static_cast<uint64_t*>(at(o_brick_status));
+    d.leafown_status = static_cast<uint64_t*>(at(o_leafown_status));
+    d.leaf_table = static_cast<uint4*>(at(o_leaf_table));
+    d.chunk_first = static_cast<uint32_t*>(at(o_chunk_first));
+    d.roots = static_cast<uint32_t*>(at(o_roots));
+    d.prim_start = static_cast<uint32_t*>(at(o_prim_start));
+    d.seg_entry = static_cast<uint32_t*>(at(o_seg_entry));
+    d.seg_tile = static_cast<uint32_t*>(at(o_seg_tile));
+    d.kbuf[0] = static_cast<uint32_t*>(at(o_k0));
+    d.vbuf[0] = static_cast<uint32_t*>(at(o_v0));
+    d.kbuf[1] = static_cast<uint32_t*>(at(o_k1));
+    d.vbuf[1] = static_cast<uint32_t*>(at(o_v1));
+    d.bkey = static_cast<uint64_t*>(at(o_bkey));
+    d.bmask = static_cast<uint64_t*>(at(o_bmask));
+    d.bfirst = static_cast<uint32_t*>(at(o_bfirst));
+    d.bslot = static_cast<uint32_t*>(at(o_bslot));
+    d.ukey = reinterpret_cast<uint64_t*>(o_ukey);
+    d.uval = reinterpret_cast<uint32_t*>(o_uval);
+    d.leaves = reinterpret_cast<uint64_t*>(o_leaves);
+    d.nodes = reinterpret_cast<uint32_t*>(o_nodes);
+    d.prims = reinterpret_cast<uint8_t*>(o_prims);
+    d.aabbs = reinterpret_cast<float*>(o_aabbs);
+
+    std::vector<LevelDesc> levels;
+    for (uint32_t lv = 2; lv < log2; ++lv) {
+        LevelDesc L;
+        std::memset(&L, 0, sizeof(L));
+        L.lv = lv;
+        L.child_bound = lv == 2 ? B : P[lv - 1];
+        L.parent_bound = P[lv];
+        L.build_tiles = btiles[lv];
+        L.own_tiles = otiles[lv];
+        L.need_box = lv + 1 <= rt ? 1u : 0u;
+        L.pcap = cap[lv];
+        L.tile_ctr_build = 12 + 2 * (lv - 2);
+        L.tile_ctr_own = 13 + 2 * (lv - 2);
+        const int ps = (lv - 2) & 1;
+        L.pkey = static_cast<uint64_t*>(at(o_set[ps][0]));
+        L.pcnt = static_cast<uint32_t*>(at(o_set[ps][1]));
+        L.pfirst = static_cast<uint32_t*>(at(o_set[ps][2]));
+        L.pslot = static_cast<uint32_t*>(at(o_set[ps][3]));
+        L.plo = static_cast<uint64_t*>(at(o_set[ps][4]));
+        L.phi = static_cast<uint64_t*>(at(o_set[ps][5]));
+        L.pwords = static_cast<uint32_t*>(at(o_set[ps][6]));
+        L.ptable = static_cast<uint4*>(at(o_table[lv]));
+        L.build_status = static_cast<uint64_t*>(at(o_bstat[lv]));
+        L.own_status = static_cast<uint64_t*>(at(o_ostat[lv]));
+        if (lv == 2) {
+            L.ckey = d.bkey;
+            L.cmask = d.bmask;
+            L.cfirst = d.bfirst;
+            L.cslot = d.bslot;
+            L.ctable = d.leaf_table;
+        } else {
+            const LevelDesc& C = levels.back();
+            L.ckey = C.pkey;
+            L.ccnt = C.pcnt;
+            L.cfirst = C.pfirst;
+            L.cslot = C.pslot;
+            L.clo = C.plo;
+            L.chi = C.phi;
+            L.ctable = C.ptable;
+        }
+        levels.push_back(L);
+    }
+
+    // ---- launches
+    auto cleanup = [&] {
+        release_outputs();
+        mem.put(scratch);
+    };
+#define CUL(call)                                                                                 \
+    do {                                                                                          \
+        cudaError_t err_ = (call);                                                                \
+        if (err_ != cudaSuccess) {                                                                \
+            cleanup();                                                                            \
+            return fail(PYRB_ERROR_CUDA, "%s: %s", #call, cudaGetErrorString(err_));              \
+        }                                                                                         \
+    } while (0)
+    Prof prof(st);
+    CUL(cudaMemsetAsync(at(0), 0, zero_bytes, st));
+    CUL(cudaMemsetAsync(at(zero_bytes), 0xFF, ff_bytes, st));
+    prof.mark("memset");
+    uint32_t launches = 0;
+    k_plan<<<1, 1024, 0, st>>>(d);
+    ++launches;
+    prof.mark("plan");
+    CUL(cudaGetLastError());
+    CUL(launch_sort_any(rb, it, d, st, prof));
+    launches += 2 + passes;
+    k_brick<<<d.brick_tiles, kBlock, 0, st>>>(d);
+    prof.mark("brick");
+    k_leaf_own<<<d.leafown_tiles, kBlock, 0, st>>>(d);
+    prof.mark("leaf_own");
+    launches += 2;
+    for (const LevelDesc& L : levels) {
+        k_node_build<<<L.build_tiles, kBlock, 0, st>>>(d, L);
+        prof.mark("node_build", L.lv);
+        k_node_own<<<L.own_tiles, kBlock, 0, st>>>(d, L);
+        prof.mark("node_own", L.lv);
+        launches += 2;
+        if (L.lv + 1 == rt) {
+            k_prims<<<std::max((L.parent_bound + kBlock - 1) / kBlock, 1u), kBlock, 0, st>>>(d, L);
+            prof.mark("prims", L.lv);
+            ++launches;
+        }
+    }
+    k_finalize<<<1, kBlock, 0, st>>>(d, levels.back());
+    prof.mark("finalize");
+    ++launches;
+    CUL(cudaGetLastError());
+
+    const uint64_t out_bytes = uint64_t(d.node_bound) * 4 + uint64_t(B) * 8 + uint64_t(nmax) * 12 +
+                               uint64_t(std::max(d.prim_bound, 1u)) * 40;
+    // ---- asynchronous form: counts land in pinned host memory, no synchronisation
+    if (host_counts) {
+        CUL(cudaMemcpyAsync(host_counts, d.counters, kCtrCount * 4, cudaMemcpyDeviceToHost, st));
+        if (chunked) {
+            if (job.roots) CUL(cudaMemcpyAsync(job.roots, d.roots, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
+            if (job.first_voxel) CUL(cudaMemcpyAsync(job.first_voxel, d.chunk_first, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
+            if (job.first_prim) CUL(cudaMemcpyAsync(job.first_prim, d.prim_start, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
+        }
+        mem.put(scratch);
+        uint32_t* meta = host_counts + kCtrCount;
+        meta[0] = log2; meta[1] = rt; meta[2] = passes; meta[3] = rb; meta[4] = launches;
+        std::memcpy(meta + 5, &scratch_bytes, 8);
+        std::memcpy(meta + 7, &out_bytes, 8);
+        out->log2_size = log2;
+        out->rt_log2 = rt;
+        out->nodes = o_nodes;
+        out->leaves = o_leaves;
+        out->keys = o_ukey;
+        out->attrs = o_uval;
+        out->prims = o_prims;
+        out->aabbs = o_aabbs;
+        return PYRB_OK;
+    }
+    // ---- read back
+    uint32_t ctr[kCtrCount];
+    CUL(cudaMemcpyAsync(ctr, d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    if (chunked) {
+        if (job.roots) CUL(cudaMemcpyAsync(job.roots, d.roots, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
+        if (job.first_voxel) CUL(cudaMemcpyAsync(job.first_voxel, d.chunk_first, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
+        if (job.first_prim) CUL(cudaMemcpyAsync(job.first_prim, d.prim_start, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CUL(cudaStreamSynchronize(st));
+    mem.put(scratch);
+    scratch = 0;
+#undef CUL
+    if (ctr[kCtrError]) {
+        release_outputs();
+        return device_error(ctr[kCtrError]);
+    }
+    out->log2_size = log2;
+    out->rt_log2 = rt;
+    out->nodes = o_nodes;
+    out->leaves = o_leaves;
+    out->keys = o_ukey;
+    out->attrs = o_uval;
+    out->prims = o_prims;
+    out->aabbs = o_aabbs;
+    fill_counts(ctr, out);
+    uint32_t meta[16] = {log2, rt, passes, rb, launches};
+    std::memcpy(meta + 5, &scratch_bytes, 8);
+    std::memcpy(meta + 7, &out_bytes, 8);
+    fill_stats(ctr, meta);
+    return PYRB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+PYRB_API pyrb_result pyrb_build(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req, uint64_t old_keys,
+                                uint64_t old_vals, uint32_t n_old, uint64_t edits, uint32_t n_new, pyrb_built* out) {
+    if ((n_old && (!old_keys || !old_vals)) || (n_new && !edits))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL input pointer with a non-zero count");
+    Job j;
+    j.mode = kModePlain;
+    j.log2 = log2_size;
+    j.rt_req = rt_log2_req;
+    j.old_keys = old_keys;
+    j.old_vals = old_vals;
+    j.n_old = n_old;
+    j.voxels = edits;
+    j.n_new = n_new;
+    return run_build(e, j, out);
+}
+
+PYRB_API pyrb_result pyrb_build_chunks(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                       const pyrb_chunk_batch* batch, uint32_t* roots, uint32_t* first_voxel,
+                                       uint32_t* first_prim, pyrb_built* out) {
+    if (!batch || batch->count == 0 || batch->capacity == 0)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "empty chunk batch");
+    if (!batch->offsets || (batch->total && !batch->voxels))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL chunk buffers");
+    Job j;
+    j.mode = kModeChunks;
+    j.log2 = log2_size;
+    j.rt_req = rt_log2_req;
+    j.K = batch->count;
+    j.capacity = batch->capacity;
+    j.voxels = batch->voxels;
+    j.offsets = batch->offsets;
+    j.total = batch->total;
+    j.roots = roots;
+    j.first_voxel = first_voxel;
+    j.first_prim = first_prim;
+    return run_build(e, j, out);
+}
+
+PYRB_API pyrb_result pyrb_build_chunks_edits(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                             uint32_t count, uint32_t capacity, uint64_t voxels, uint64_t counts,
+                                             uint64_t edits, uint64_t edit_offsets, uint32_t edit_total,
+                                             uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim,
+                                             pyrb_built* out) {
+    if (count == 0 || capacity == 0) return fail(PYRB_ERROR_INVALID_ARGUMENT, "empty chunk batch");
+    if (!voxels || !counts || !edit_offsets || (edit_total && !edits))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL chunk buffers");
+    Job j;
+    j.mode = kModeChunksEdits;
+    j.log2 = log2_size;
+    j.rt_req = rt_log2_req;
+    j.K = count;
+    j.capacity = capacity;
+    j.voxels = voxels;
+    j.gen_counts = counts;
+    j.edits = edits;
+    j.edit_offsets = edit_offsets;
+    j.edit_total = edit_total;
+    j.roots = roots;
+    j.first_voxel = first_voxel;
+    j.first_prim = first_prim;
+    return run_build(e, j, out);
+}
+
+PYRB_API pyrb_result pyrb_downsample(const pyrb_exec* e, uint32_t log2_src, uint32_t rt_log2_req, uint64_t src_keys,
+                                     uint64_t src_vals, uint32_t n_src, uint32_t shift, pyrb_built* out) {
+    if (shift == 0 || shift + 3 > log2_src)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "downsampling by 2^%u is not possible at 2^%u (result at least 2^3)",
+                    shift, log2_src);
+    if (n_src && (!src_keys || !src_vals)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL source buffers");
+    Job j;
+    j.mode = kModeDownsample;
+    j.log2 = log2_src - shift;
+    j.rt_req = rt_log2_req;
+    j.src_keys = src_keys;
+    j.src_vals = src_vals;
+    j.n_new = n_src;
+    j.shift = shift;
+    return run_build(e, j, out);
+}
+
+PYRB_API pyrb_result pyrb_geometry_build(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
+                                         const void* voxels, uint32_t count, uint32_t flags, pyrb_built* out) {
+    if (count && !voxels) return fail(PYRB_ERROR_INVALID_ARGUMENT, "voxels is NULL");
+    if (!(flags & PYRB_BUILD_HOST_INPUT) || count == 0)
+        return pyrb_build(e, log2_size, rt_log2_req, 0, 0, 0, reinterpret_cast<uint64_t>(voxels), count, out);
+    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+    Mem mem{e, st};
+    const uint64_t bytes = uint64_t(count) * 16;
+    uint64_t dev = mem.get(bytes);
+    if (!dev) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the voxel upload (%llu bytes)", (unsigned long long)bytes);
+    cudaError_t err = cudaMemcpyAsync(reinterpret_cast<void*>(dev), voxels, bytes, cudaMemcpyHostToDevice, st);
+    if (err != cudaSuccess) {
+        mem.put(dev);
+        return fail(PYRB_ERROR_CUDA, "upload: %s", cudaGetErrorString(err));
+    }
+    pyrb_result r = pyrb_build(e, log2_size, rt_log2_req, 0, 0, 0, dev, count, out);
+    mem.put(dev);
+    return r;
+}
+
+PYRB_API void pyrb_built_free(const pyrb_exec* e, pyrb_built* b) {
+    if (!b) return;
+    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+    Mem mem{e, st};
+    for (uint64_t p : {b->nodes, b->leaves, b->keys, b->attrs, b->prims, b->aabbs}) mem.put(p);
+    std::memset(b, 0, sizeof(*b));
+}
+
+PYRB_API pyrb_result pyrb_build_async(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req, uint64_t old_keys,
+                                      uint64_t old_vals, uint32_t n_old, uint64_t edits, uint32_t n_new,
+                                      uint32_t* host_counts, pyrb_built* out) {
+    if (!host_counts) return fail(PYRB_ERROR_INVALID_ARGUMENT, "host_counts is NULL");
+    if ((n_old && (!old_keys || !old_vals)) || (n_new && !edits))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL input pointer with a non-zero count");
+    Job j;
+    j.mode = kModePlain;
+    j.log2 = log2_size;
+    j.rt_req = rt_log2_req;
+    j.old_keys = old_keys;
+    j.old_vals = old_vals;
+    j.n_old = n_old;
+    j.voxels = edits;
+    j.n_new = n_new;
+    return run_build(e, j, out, host_counts);
+}
+
+PYRB_API pyrb_result pyrb_build_finish(const uint32_t* host_counts, pyrb_built* out) {
+    if (!host_counts || !out) return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (host_counts[kCtrError]) return device_error(host_counts[kCtrError]);
+    fill_counts(host_counts, out);
+    fill_stats(host_counts, host_counts + kCtrCount);
+    return PYRB_OK;
+}
+
+PYRB_API void pyrb_profile_enable(int on) { g_prof_on = on != 0; }
+
+PYRB_API uint32_t pyrb_profile_read(float* ms, char* names, uint32_t name_len, uint32_t cap) {
+    uint32_t n = uint32_t(g_prof_names.size());
+    for (uint32_t i = 0; i < n && i < cap; ++i) {
+        float t = 0;
+        cudaEventElapsedTime(&t, g_prof_events[i], g_prof_events[i + 1]);
+        if (ms) ms[i] = t;
+        if (names && name_len) {
+            snprintf(names + uint64_t(i) * name_len, name_len, "%s%s%u", g_prof_names[i].first,
+                     g_prof_names[i].second || std::strcmp(g_prof_names[i].first, "sort_pass") == 0 ? ":" : "",
+                     g_prof_names[i].second);
+            if (!(g_prof_names[i].second || std::strcmp(g_prof_names[i].first, "sort_pass") == 0))
+                snprintf(names + uint64_t(i) * name_len, name_len, "%s", g_prof_names[i].first);
+        }
+    }
+    return n;
+}
+
+PYRB_API void pyrb_last_stats(pyrb_stats* out) {
+    if (out) *out = g_stats;
+}
+
+PYRB_API const char* pyrb_error_message(void) { return g_msg; }
+
+PYRB_API const char* pyrb_result_string(pyrb_result r) {
+    switch (r) {
+        case PYRB_OK: return "ok";
+        case PYRB_ERROR_INVALID_ARGUMENT: return "invalid argument";
+        case PYRB_ERROR_OUT_OF_MEMORY: return "out of memory";
+        case PYRB_ERROR_CUDA: return "CUDA error";
+        default: return "unknown result";
+    }
+}
+
+PYRB_API pyrb_result pyrb_set_tuning(const pyrb_tuning* t) {
+    if (!t) return fail(PYRB_ERROR_INVALID_ARGUMENT, "tuning is NULL");
+    if (t->radix_bits != 4 && t->radix_bits != 8 && t->radix_bits != 11)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "radix_bits must be 4, 8 or 11");
+    if (t->tile_keys != 1024 && t->tile_keys != 2048 && t->tile_keys != 4096)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "tile_keys must be 1024, 2048 or 4096");
+    if (t->load_factor_pct < 25 || t->load_factor_pct > 90)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "load_factor_pct must lie in [25, 90]");
+    g_radix_bits = t->radix_bits;
+    g_tile_keys = t->tile_keys;
+    g_load_pct = t->load_factor_pct;
+    return PYRB_OK;
+}
+
+PYRB_API void pyrb_get_tuning(pyrb_tuning* t) {
+    if (!t) return;
+    t->radix_bits = g_radix_bits;
+    t->tile_keys = g_tile_keys;
+    t->load_factor_pct = g_load_pct;
+    t->reserved = 0;
+}
+
+PYRB_API uint32_t pyrb_version(void) { return (0u << 16) | 1u; }
+
+}  // extern "C"

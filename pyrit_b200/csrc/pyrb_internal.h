@@ -1,0 +1,147 @@
+// Internal layout shared by the host orchestration and the kernels.
+#pragma once
+
+#include <cstdint>
+
+namespace pyrb {
+
+// Error bits in counters[kCtrError] (device-side, read back by the host).
+constexpr uint32_t kErrSpin = 1u;       // a look-back or wait gave up after its poll limit
+constexpr uint32_t kErrTable = 2u;      // a dedup table had no free slot
+constexpr uint32_t kErrBound = 4u;      // a count exceeded its allocated upper bound
+
+// Counter block (u32) read back at the end of a build.
+constexpr int kCtrUnique = 0;      // voxel_count
+constexpr int kCtrBricks = 1;      // non-empty bricks
+constexpr int kCtrLeaves = 2;      // leaf_count
+constexpr int kCtrWords = 3;       // node_words
+constexpr int kCtrRoot = 4;
+constexpr int kCtrPrims = 5;
+constexpr int kCtrError = 6;
+constexpr int kCtrCursor = 8;      // + lv: first node word of level lv (lv = 2..25)
+constexpr int kCtrParents = 36;    // + lv: P_lv
+constexpr int kCtrUniqueLv = 64;   // + lv: U_lv
+constexpr int kCtrTiles = 96;      // dynamic tile counters, one per launch
+constexpr int kCtrCount = 160;
+
+constexpr int kMaxLevels = 24;
+constexpr int kMaxPasses = 8;
+
+// Input modes of the first (encode) stage.
+enum Mode : uint32_t {
+    kModePlain = 0,        // [old sorted keys | PyrVoxel edits], one segment
+    kModeChunks = 1,       // segments of `capacity` PyrVoxels, filled per offsets[]
+    kModeChunksEdits = 2,  // generated voxels per counts[] followed by overlay edits per edit_offsets[]
+    kModeDownsample = 3,   // coarse keys of sorted source keys
+};
+
+// Everything a build's kernels need, passed by value (kernel parameter space).
+struct BuildDesc {
+    uint32_t mode;
+    uint32_t log2;          // edge of the (uniform) chunk / geometry
+    uint32_t rt_log2;
+    uint32_t lb;            // local key bits: 3 * log2
+    uint32_t seg_count;     // K segments (1 for plain builds)
+    uint32_t capacity;
+    uint32_t shift;         // downsample
+    uint32_t n_old;
+    uint32_t n_new;
+    uint32_t n_total;       // raw entries of the encode stage
+    uint32_t top;           // top level = log2 - 1
+    uint32_t chunked;       // chunk batch: per-chunk roots, first voxels, first prims
+
+    // inputs
+    const uint64_t* old_keys;
+    const uint32_t* old_vals;
+    const uint4* voxels;          // PyrVoxel entries (edits / chunk voxels / generated voxels)
+    const uint32_t* offsets;      // kModeChunks: u32[K+1]
+    const uint32_t* gen_counts;   // kModeChunksEdits: u32[K]
+    const uint4* edits;           // kModeChunksEdits
+    const uint32_t* edit_offsets; // kModeChunksEdits: u32[K+1]
+    const uint64_t* src_keys;     // kModeDownsample
+    const uint32_t* src_vals;
+
+    // segment tiling of the sort / unique stages
+    uint32_t* seg_entry;     // u32[K+1]: first raw entry of each segment
+    uint32_t* seg_tile;      // u32[K+1]: first sort tile of each segment
+    uint32_t tile_keys;
+    uint32_t sort_tiles;     // upper bound of sort tiles (grid)
+
+    // sort
+    uint32_t passes;
+    uint32_t radix;          // 1 << widest digit
+    uint32_t pass_shift[kMaxPasses];
+    uint32_t pass_bits[kMaxPasses];
+    uint32_t* hist;          // [K][passes][radix]
+    uint64_t* sort_status;   // [passes][sort_tiles][radix]
+    uint32_t* kbuf[2];
+    uint32_t* vbuf[2];
+
+    // unique voxels (outputs)
+    uint64_t* uniq_status;   // [sort_tiles]
+    uint64_t* ukey;
+    uint32_t* uval;
+    uint32_t* chunk_first;   // [K], 0xFFFFFFFF initialised
+
+    // bricks + leaves
+    uint32_t brick_bound;
+    uint32_t brick_tiles;
+    uint64_t* brick_status;  // [brick_tiles]
+    uint64_t* bkey;
+    uint64_t* bmask;
+    uint32_t* bfirst;
+    uint32_t* bslot;
+    uint4* leaf_table;       // {mask lo, mask hi, ~owner, leaf index}
+    uint32_t leaf_cap;
+    uint32_t leafown_tiles;
+    uint64_t* leafown_status;
+    uint64_t* leaves;        // output
+
+    uint32_t* counters;      // u32[kCtrCount]
+
+    // outputs
+    uint32_t* nodes;
+    uint32_t node_bound;     // words
+    uint8_t* prims;
+    float* aabbs;
+    uint32_t prim_bound;
+    uint32_t* roots;         // [K] (chunk builds), 0xFFFFFFFF initialised
+    uint32_t* prim_start;    // [K]
+};
+
+// One node level: children (bricks at level 2) -> parents of edge 2^(lv+1).
+struct LevelDesc {
+    uint32_t lv;
+    uint32_t child_bound;
+    uint32_t parent_bound;
+    uint32_t build_tiles;
+    uint32_t own_tiles;
+    uint32_t need_box;       // parents need a bounding box (lv + 1 <= rt_log2)
+    uint32_t pcap;           // table capacity (power of two)
+    uint32_t tile_ctr_build; // counter index of the dynamic tile ids
+    uint32_t tile_ctr_own;
+    // children
+    const uint64_t* ckey;    // lv == 2: brick keys (voxel key >> 6)
+    const uint32_t* ccnt;    // lv >  2
+    const uint32_t* cfirst;
+    const uint32_t* cslot;
+    const uint64_t* cmask;   // lv == 2
+    const uint64_t* clo;     // lv >  2
+    const uint64_t* chi;
+    const uint4* ctable;     // .w = reference of the child (leaf index / node offset)
+    // parents
+    uint64_t* pkey;
+    uint32_t* pcnt;
+    uint32_t* pfirst;
+    uint32_t* pslot;
+    uint64_t* plo;
+    uint64_t* phi;
+    uint32_t* pwords;        // [parent_bound][10]
+    uint4* ptable;           // {index + 1, -, ~owner, node offset}
+    uint64_t* build_status;
+    uint64_t* own_status;
+};
+
+constexpr uint32_t kNodeStride = 10;
+
+}  // namespace pyrb

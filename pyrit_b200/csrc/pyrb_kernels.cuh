@@ -1,0 +1,891 @@
+// Kernels of the DAG build (sm_100a). One build = plan -> encode/histogram ->
+// onesweep radix passes -> unique -> bricks (+ leaf insert) -> leaf owners ->
+// per level {node build (+ insert), node owners} -> prims -> finalize.
+//
+// Every kernel that assigns output positions uses a decoupled look-back over
+// dynamically numbered tiles: a tile only ever waits for tiles with smaller
+// numbers, which were taken by blocks that are already running, so the waits
+// always end; each wait is additionally bounded (kSpinLimit) and reports
+// kErrSpin instead of hanging.
+#pragma once
+
+#include "pyrb_device.cuh"
+
+namespace pyrb {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Largest s in [0, n) with arr[s] <= v (arr non-decreasing, arr[0] <= v).
+__device__ __forceinline__ uint32_t upper_index(const uint32_t* arr, uint32_t n, uint32_t v) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(arr + mid) <= v) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t dyn_tile(uint32_t* counters, uint32_t ctr, uint32_t* s_slot) {
+    if (threadIdx.x == 0) *s_slot = atomicAdd(counters + kCtrTiles + ctr, 1u);
+    __syncthreads();
+    uint32_t t = *s_slot;
+    __syncthreads();
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Segment plan: first entry and first sort tile of every segment.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
+    __shared__ uint32_t s_scan[2][1024];
+    __shared__ uint32_t s_carry[2];
+    const uint32_t K = d.seg_count;
+    if (threadIdx.x == 0) { s_carry[0] = 0; s_carry[1] = 0; }
+    __syncthreads();
+    for (uint32_t base = 0; base < K; base += 1024) {
+        uint32_t c = base + threadIdx.x;
+        uint32_t size = 0;
+        if (c < K) {
+            switch (d.mode) {
+                case kModeChunks: size = __ldg(d.offsets + c + 1) - __ldg(d.offsets + c); break;
+                case kModeChunksEdits:
+                    size = min(__ldg(d.gen_counts + c), d.capacity) + (__ldg(d.edit_offsets + c + 1) - __ldg(d.edit_offsets + c));
+                    break;
+                default: size = d.n_total; break;
+            }
+        }
+        uint32_t tiles = (size + d.tile_keys - 1) / d.tile_keys;
+        s_scan[0][threadIdx.x] = size;
+        s_scan[1][threadIdx.x] = tiles;
+        __syncthreads();
+        // inclusive Hillis-Steele scan of both arrays
+        for (uint32_t o = 1; o < 1024; o <<= 1) {
+            uint32_t a = threadIdx.x >= o ? s_scan[0][threadIdx.x - o] : 0;
+            uint32_t b = threadIdx.x >= o ? s_scan[1][threadIdx.x - o] : 0;
+            __syncthreads();
+            s_scan[0][threadIdx.x] += a;
+            s_scan[1][threadIdx.x] += b;
+            __syncthreads();
+        }
+        if (c < K) {
+            d.seg_entry[c] = s_carry[0] + s_scan[0][threadIdx.x] - size;
+            d.seg_tile[c] = s_carry[1] + s_scan[1][threadIdx.x] - tiles;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) { s_carry[0] += s_scan[0][1023]; s_carry[1] += s_scan[1][1023]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        d.seg_entry[K] = s_carry[0];
+        d.seg_tile[K] = s_carry[1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Encode: raw entry -> (key, value). Out-of-range voxels get the invalid bit
+// (bit lb), which sorts them behind every valid key of their segment; the
+// unique stage drops them (same rule as gbuild.encode / packChunks).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void encode_voxel(uint4 v, uint32_t log2, uint32_t lb, uint32_t& key, uint32_t& val) {
+    const int32_t n = int32_t(1u << log2);
+    int32_t x = int32_t(v.x), y = int32_t(v.y), z = int32_t(v.z);
+    if (x < 0 || y < 0 || z < 0 || x >= n || y >= n || z >= n) {
+        key = 1u << lb;
+        val = 0;
+    } else {
+        key = uint32_t(voxel_key(uint32_t(x), uint32_t(y), uint32_t(z)));
+        val = v.w;
+    }
+}
+
+__device__ __forceinline__ void load_raw(const BuildDesc& d, uint32_t seg, uint32_t j, uint32_t& key, uint32_t& val) {
+    switch (d.mode) {
+        case kModePlain:
+            if (j < d.n_old) {
+                key = uint32_t(__ldg(d.old_keys + j));
+                val = __ldg(d.old_vals + j);
+            } else {
+                encode_voxel(__ldg(d.voxels + (j - d.n_old)), d.log2, d.lb, key, val);
+            }
+            break;
+        case kModeChunks:
+            if (j < d.capacity) encode_voxel(__ldg(d.voxels + uint64_t(seg) * d.capacity + j), d.log2, d.lb, key, val);
+            else { key = 1u << d.lb; val = 0; }
+            break;
+        case kModeChunksEdits: {
+            uint32_t g = min(__ldg(d.gen_counts + seg), d.capacity);
+            uint4 v = j < g ? __ldg(d.voxels + uint64_t(seg) * d.capacity + j)
+                            : __ldg(d.edits + __ldg(d.edit_offsets + seg) + (j - g));
+            encode_voxel(v, d.log2, d.lb, key, val);
+            break;
+        }
+        default: {  // downsample (gbuild.zig:262-274): coarse key of the source voxel
+            uint64_t k = __ldg(d.src_keys + j);
+            uint64_t brick = k >> 6;
+            uint32_t bit = uint32_t(k & 63), sh = d.shift;
+            uint32_t x = ((compact3(brick) << 2) | (bit & 3)) >> sh;
+            uint32_t y = ((compact3(brick >> 1) << 2) | ((bit >> 2) & 3)) >> sh;
+            uint32_t z = ((compact3(brick >> 2) << 2) | (bit >> 4)) >> sh;
+            key = uint32_t(voxel_key(x, y, z));
+            val = __ldg(d.src_vals + j);
+            break;
+        }
+    }
+}
+
+// Tile -> (segment, first entry, entry count) of the per-segment sort tiling.
+struct TileSpan { uint32_t seg, start, count, first_tile; };
+__device__ __forceinline__ TileSpan tile_span(const BuildDesc& d, uint32_t tile) {
+    TileSpan t;
+    t.seg = upper_index(d.seg_tile, d.seg_count + 1, tile);
+    // empty segments share tile numbers with the next one: move to the segment owning the tile
+    while (t.seg + 1 < d.seg_count && __ldg(d.seg_tile + t.seg + 1) <= tile) ++t.seg;
+    t.first_tile = __ldg(d.seg_tile + t.seg);
+    uint32_t seg_begin = __ldg(d.seg_entry + t.seg), seg_end = __ldg(d.seg_entry + t.seg + 1);
+    t.start = seg_begin + (tile - t.first_tile) * d.tile_keys;
+    t.count = min(d.tile_keys, seg_end - t.start);
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Encode + histogram of every pass ("onesweep" upfront histogram).
+// ---------------------------------------------------------------------------
+template <int RB, int IT>
+__global__ void __launch_bounds__(kBlock) k_encode_hist(BuildDesc d) {
+    constexpr int RADIX = 1 << RB;
+    extern __shared__ uint32_t smem[];
+    uint32_t* hist = smem;  // [passes][RADIX]
+    const uint32_t tile = blockIdx.x;
+    if (tile >= d.seg_tile[d.seg_count]) return;
+    const TileSpan sp = tile_span(d, tile);
+    for (uint32_t i = threadIdx.x; i < d.passes * RADIX; i += kBlock) hist[i] = 0;
+    __syncthreads();
+    const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
+#pragma unroll 4
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = j * kBlock + threadIdx.x;
+        bool valid = idx < sp.count;
+        uint32_t key = 0, val = 0;
+        if (valid) {
+            uint32_t e = sp.start + idx;
+            load_raw(d, sp.seg, e - seg_begin, key, val);
+            d.kbuf[0][e] = key;
+            d.vbuf[0][e] = val;
+        }
+        for (uint32_t p = 0; p < d.passes; ++p) {
+            uint32_t dig = valid ? (key >> d.pass_shift[p]) & ((1u << d.pass_bits[p]) - 1) : 0xFFFFFFFFu;
+            unsigned peers = __match_any_sync(kFull, dig);
+            if (valid && (threadIdx.x & 31) == unsigned(__ffs(peers) - 1)) atomicAdd(hist + p * RADIX + dig, __popc(peers));
+        }
+    }
+    __syncthreads();
+    uint32_t* gh = d.hist + uint64_t(sp.seg) * d.passes * RADIX;
+    for (uint32_t i = threadIdx.x; i < d.passes * RADIX; i += kBlock) {
+        uint32_t v = hist[i];
+        if (v) atomicAdd(gh + i, v);
+    }
+}
+
+// Exclusive scan of RADIX digit counts in smem (in -> out), DPT consecutive digits per thread.
+template <int RADIX>
+__device__ __forceinline__ void scan_digits(const uint32_t* in, uint32_t* out, uint32_t* scratch) {
+    constexpr int DPT = (RADIX + kBlock - 1) / kBlock;
+    uint32_t local[DPT];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) {
+        uint32_t dg = threadIdx.x * DPT + k;
+        local[k] = dg < uint32_t(RADIX) ? in[dg] : 0;
+        sum += local[k];
+    }
+    uint32_t total;
+    uint32_t run = block_excl_scan(sum, scratch, &total);
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) {
+        uint32_t dg = threadIdx.x * DPT + k;
+        if (dg < uint32_t(RADIX)) out[dg] = run;
+        run += local[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One LSD pass of the onesweep radix sort: stable within the tile (warp-striped
+// items ranked in order with match_any), decoupled look-back per digit across the
+// tiles of the segment, staged in shared memory so that the global writes of a
+// digit run are contiguous.
+// ---------------------------------------------------------------------------
+template <int RB, int IT>
+constexpr size_t sort_smem_bytes() {
+    constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
+    constexpr int U = (kWarps * RADIX > 2 * TILE) ? kWarps * RADIX : 2 * TILE;
+    return size_t(U + 3 * RADIX + 2 * kWarps + 8) * 4;
+}
+
+template <int RB, int IT>
+__global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass, uint32_t src) {
+    constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
+    constexpr int U = (kWarps * RADIX > 2 * TILE) ? kWarps * RADIX : 2 * TILE;
+    constexpr int DPT = (RADIX + kBlock - 1) / kBlock;
+    extern __shared__ uint32_t smem[];
+    uint32_t* whist = smem;               // [kWarps][RADIX], later staging keys|vals
+    uint32_t* tcnt = smem + U;            // tile count per digit
+    uint32_t* texcl = tcnt + RADIX;       // tile-exclusive digit offsets
+    uint32_t* gofs = texcl + RADIX;       // segment digit start, then global write offset
+    uint32_t* scratch = gofs + RADIX;     // 2*kWarps + 1 words
+    uint32_t* s_tile = scratch + 2 * kWarps + 4;
+
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = dyn_tile(d.counters, pass, s_tile);
+    if (tile >= d.seg_tile[d.seg_count]) return;
+    const TileSpan sp = tile_span(d, tile);
+    const uint32_t shift = d.pass_shift[pass], dmask = (1u << d.pass_bits[pass]) - 1;
+    const uint32_t* kin = d.kbuf[src];
+    const uint32_t* vin = d.vbuf[src];
+    uint32_t* kout = d.kbuf[src ^ 1];
+    uint32_t* vout = d.vbuf[src ^ 1];
+
+    for (uint32_t i = threadIdx.x; i < uint32_t(kWarps * RADIX); i += kBlock) whist[i] = 0;
+    // segment digit starts (exclusive scan of the segment histogram of this pass)
+    const uint32_t* gh = d.hist + (uint64_t(sp.seg) * d.passes + pass) * RADIX;
+    for (uint32_t i = threadIdx.x; i < uint32_t(RADIX); i += kBlock) tcnt[i] = __ldg(gh + i);
+    __syncthreads();
+    scan_digits<RADIX>(tcnt, gofs, scratch);
+
+    uint32_t keys[IT], vals[IT], rank[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        if (idx < sp.count) {
+            keys[j] = kin[sp.start + idx];
+            vals[j] = vin[sp.start + idx];
+        } else {
+            keys[j] = 0;
+            vals[j] = 0;
+        }
+    }
+    const unsigned lt = lanemask_lt();
+    uint32_t* wh = whist + warp * RADIX;
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        bool valid = idx < sp.count;
+        uint32_t dig = valid ? (keys[j] >> shift) & dmask : 0xFFFFFFFFu;
+        unsigned peers = __match_any_sync(kFull, dig);
+        uint32_t cnt = valid ? wh[dig] : 0;
+        rank[j] = cnt + __popc(peers & lt);
+        __syncwarp();
+        if (valid && lane == unsigned(__ffs(peers) - 1)) wh[dig] = cnt + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // cross-warp exclusive offsets per digit, tile totals
+    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            uint32_t c = whist[w * RADIX + dg];
+            whist[w * RADIX + dg] = run;
+            run += c;
+        }
+        tcnt[dg] = run;
+    }
+    __syncthreads();
+    // publish the tile's digit counts as early as possible
+    uint64_t* status = d.sort_status + uint64_t(pass) * d.sort_tiles * RADIX;
+    if (tile != sp.first_tile) {
+        for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock)
+            st_relaxed(status + uint64_t(tile) * RADIX + dg, kFlagAgg | tcnt[dg]);
+    }
+    scan_digits<RADIX>(tcnt, texcl, scratch);
+    __syncthreads();
+    // look-back per digit
+    const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
+    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
+        uint64_t excl = lookback_serial(status + dg, RADIX, tile, sp.first_tile, tcnt[dg], d.counters + kCtrError);
+        gofs[dg] = seg_begin + gofs[dg] + uint32_t(excl) - texcl[dg];
+    }
+    (void)DPT;
+    // final tile-local ranks
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        if (idx < sp.count) {
+            uint32_t dig = (keys[j] >> shift) & dmask;
+            rank[j] += texcl[dig] + wh[dig];
+        }
+    }
+    __syncthreads();
+    uint32_t* sk = whist;
+    uint32_t* sv = whist + TILE;
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        if (idx < sp.count) {
+            sk[rank[j]] = keys[j];
+            sv[rank[j]] = vals[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
+    bool oob = false;
+    for (uint32_t i = threadIdx.x; i < sp.count; i += kBlock) {
+        uint32_t k = sk[i];
+        uint32_t pos = gofs[(k >> shift) & dmask] + i;
+        if (pos >= seg_begin && pos < seg_end) {
+            kout[pos] = k;
+            vout[pos] = sv[i];
+        } else {
+            oob = true;
+        }
+    }
+    if (oob) atomicOr(d.counters + kCtrError, kErrBound);
+}
+
+// ---------------------------------------------------------------------------
+// Unique voxels: the last entry of a run of equal keys decides; it is kept if it
+// is valid and its attribute is non-zero (gbuild.zig:366-388). Positions by a
+// look-back scan in global (segment-major) order; keys get the segment (chunk)
+// number above bit lb, like packChunks.
+// ---------------------------------------------------------------------------
+template <int IT>
+__global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_scan[2 * kWarps + 2];
+    __shared__ uint64_t s_base;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = dyn_tile(d.counters, 8, &s_tile);
+    const uint32_t ntiles = d.seg_tile[d.seg_count];
+    if (tile >= ntiles) return;
+    const TileSpan sp = tile_span(d, tile);
+    const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
+    const uint32_t* keys = d.kbuf[fin];
+    const uint32_t* vals = d.vbuf[fin];
+    const uint32_t inv = 1u << d.lb;
+    const uint32_t wbase = warp * 32 * IT;
+
+    uint32_t k[IT], v[IT];
+    unsigned keepb[IT];
+    uint32_t wcount = 0;
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = wbase + j * 32 + lane;
+        bool in = idx < sp.count;
+        uint32_t e = sp.start + idx;
+        k[j] = in ? keys[e] : inv;
+        v[j] = in ? vals[e] : 0;
+        uint32_t nk = __shfl_down_sync(kFull, k[j], 1);
+        if (lane == 31 || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~0u;
+        bool last = !in ? false : (e + 1 == seg_end || nk != k[j]);
+        bool keep = in && last && !(k[j] & inv) && v[j] != 0;
+        keepb[j] = __ballot_sync(kFull, keep);
+        wcount += __popc(keepb[j]);
+    }
+    uint32_t total;
+    uint32_t wexcl = block_excl_scan(lane == 0 ? wcount : 0, s_scan, &total);
+    wexcl = __shfl_sync(kFull, wexcl, 0);
+    if (warp == 0) {
+        if (lane == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | total);
+        // positions are global over all segments: look back to tile 0
+        uint64_t ex = lookback_warp(d.uniq_status, tile, 0, total, d.counters + kCtrError);
+        if (lane == 0) s_base = ex;
+    }
+    __syncthreads();
+    const uint64_t base = s_base + wexcl;
+    uint32_t run = 0;
+    const uint64_t segbits = uint64_t(sp.seg) << d.lb;
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        if ((keepb[j] >> lane) & 1) {
+            uint64_t pos = base + run + __popc(keepb[j] & lanemask_lt());
+            if (pos < d.n_total) {
+                d.ukey[pos] = segbits | k[j];
+                d.uval[pos] = v[j];
+            } else {
+                atomicOr(d.counters + kCtrError, kErrBound);
+            }
+        }
+        run += __popc(keepb[j]);
+    }
+    if (d.chunked && threadIdx.x == 0 && total > 0) atomicMin(d.chunk_first + sp.seg, uint32_t(s_base));
+    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrUnique] = uint32_t(s_base + total);
+}
+
+// ---------------------------------------------------------------------------
+// Dedup tables. Leaf table slot: {mask lo, mask hi, ~owner, leaf index};
+// node table slot: {parent index + 1, 0, ~owner, node offset}. ~owner with
+// atomicMax makes the minimum index the owner on zero-initialised tables.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void claim_owner(uint4* slot, uint32_t idx) {
+    uint32_t* op = &slot->z;
+    uint32_t inv = ~idx;
+    if (ld_relaxed32(op) < inv) atomicMax(op, inv);
+}
+
+__device__ __forceinline__ uint32_t leaf_insert(uint4* table, uint32_t cap, uint64_t mask, uint32_t idx, uint32_t* err) {
+    uint32_t h = uint32_t(mix64(mask)) & (cap - 1);
+    for (uint32_t probe = 0; probe < cap; ++probe) {
+        unsigned long long* kp = reinterpret_cast<unsigned long long*>(table + h);
+        unsigned long long cur = ld_relaxed(reinterpret_cast<const uint64_t*>(kp));
+        if (cur == 0) {
+            cur = atomicCAS(kp, 0ull, (unsigned long long)mask);
+            if (cur == 0) cur = mask;
+        }
+        if (cur == mask) {
+            claim_owner(table + h, idx);
+            return h;
+        }
+        h = (h + 1) & (cap - 1);
+    }
+    atomicOr(err, kErrTable);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Bricks: 4^3 runs of the sorted unique keys -> (brick key, mask, first voxel).
+// A warp owns 32*8 consecutive keys; a run is emitted by the warp that holds its
+// first key (reading at most 63 keys past its chunk). The emitting lanes insert
+// their masks into the leaf table, collapsing equal masks of a warp first.
+// ---------------------------------------------------------------------------
+constexpr int kBrickIT = 8;
+constexpr int kBrickTile = kBlock * kBrickIT;
+
+__global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_scan[2 * kWarps + 2];
+    __shared__ uint64_t s_base;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = dyn_tile(d.counters, 9, &s_tile);
+    const uint32_t U = min(d.counters[kCtrUnique], d.n_total);
+    const uint32_t ntiles = (U + kBrickTile - 1) / kBrickTile;
+    if (tile >= ntiles) return;
+    const uint32_t wstart = tile * kBrickTile + warp * 32 * kBrickIT;
+    const uint64_t* ukey = d.ukey;
+    const uint64_t NONE = ~0ull;
+
+    uint64_t key[kBrickIT];
+    unsigned hb[kBrickIT];
+    uint32_t wheads = 0;
+    uint64_t prev_last = (wstart > 0 && wstart - 1 < U) ? ukey[wstart - 1] : NONE;
+#pragma unroll
+    for (int j = 0; j < kBrickIT; ++j) {
+        uint32_t e = wstart + j * 32 + lane;
+        key[j] = e < U ? ukey[e] : NONE;
+        uint64_t pk = __shfl_up_sync(kFull, key[j], 1);
+        if (lane == 0) pk = prev_last;
+        prev_last = __shfl_sync(kFull, key[j], 31);
+        bool head = e < U && (e == 0 || (key[j] >> 6) != (pk >> 6));
+        hb[j] = __ballot_sync(kFull, head);
+        wheads += __popc(hb[j]);
+    }
+    uint32_t total;
+    uint32_t wexcl = block_excl_scan(lane == 0 ? wheads : 0, s_scan, &total);
+    wexcl = __shfl_sync(kFull, wexcl, 0);
+    if (warp == 0) {
+        if (lane == 0 && tile != 0) st_relaxed(d.brick_status + tile, kFlagAgg | total);
+        uint64_t ex = lookback_warp(d.brick_status, tile, 0, total, d.counters + kCtrError);
+        if (lane == 0) s_base = ex;
+    }
+    __syncthreads();
+    const uint32_t wbase = uint32_t(s_base) + wexcl;
+    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrBricks] = uint32_t(s_base + total);
+
+    bool c_on = false, c_own = false;
+    uint64_t c_brick = 0, c_mask = 0;
+    uint32_t c_idx = 0, c_first = 0, hcount = 0;
+#pragma unroll
+    for (int j = 0; j < kBrickIT + 2; ++j) {
+        if (j >= kBrickIT && !(c_on && c_own)) break;
+        uint32_t e = wstart + j * 32 + lane;
+        uint64_t kj;
+        unsigned hbj;
+        if (j < kBrickIT) { kj = key[j]; hbj = hb[j]; }
+        else { kj = e < U ? ukey[e] : NONE; hbj = 0; }
+        bool valid = e < U;
+        uint64_t bk = valid ? (kj >> 6) : NONE;
+        // brick of the entry after lane 31
+        uint32_t en = wstart + (j + 1) * 32;
+        uint64_t nextk;
+        if (j + 1 < kBrickIT) nextk = __shfl_sync(kFull, key[j + 1 < kBrickIT ? j + 1 : 0], 0);
+        else nextk = en < U ? ukey[en] : NONE;
+        uint64_t nb = nextk == NONE ? NONE : (nextk >> 6);
+        unsigned peers = __match_any_sync(kFull, bk);
+        unsigned gstart = __ffs(peers) - 1, glast = 31 - __clz(peers);
+        uint64_t v = valid ? (1ull << (kj & 63)) : 0;
+        bool cont = (gstart == 0) && c_on && bk == c_brick && !((hbj >> 0) & 1);
+        if (lane == 0 && cont) v |= c_mask;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(kFull, v, o);
+            if (lane >= gstart + o) v |= y;
+        }
+        bool ghead = (hbj >> gstart) & 1;
+        uint32_t idx = ghead ? wbase + hcount + __popc(hbj & ((2u << gstart) - 1)) - 1 : c_idx;
+        bool own = ghead ? (j < kBrickIT) : (cont && c_own);
+        uint32_t first = ghead ? wstart + j * 32 + gstart : c_first;
+        const uint64_t next_in_warp = __shfl_down_sync(kFull, bk, 1);  // every lane takes part
+        uint64_t after = (lane == 31) ? nb : next_in_warp;
+        bool ends = valid && lane == glast && after != bk;
+        bool emit = ends && own && (ghead || cont);
+        // carry of the group holding lane 31
+        bool l31_valid = __shfl_sync(kFull, valid ? 1 : 0, 31);
+        bool l31_ends = __shfl_sync(kFull, ends ? 1 : 0, 31);
+        const bool l31_seg = __shfl_sync(kFull, (ghead || cont) ? 1 : 0, 31) != 0;
+        c_on = l31_valid && !l31_ends && l31_seg;
+        c_brick = __shfl_sync(kFull, bk, 31);
+        c_mask = __shfl_sync(kFull, v, 31);
+        c_idx = __shfl_sync(kFull, idx, 31);
+        c_own = __shfl_sync(kFull, own ? 1 : 0, 31) != 0;
+        c_first = __shfl_sync(kFull, first, 31);
+        hcount += __popc(hbj);
+        unsigned em = __ballot_sync(kFull, emit);
+        if (emit) {
+            unsigned same = __match_any_sync(em, v);
+            unsigned leader = __ffs(same) - 1;
+            uint32_t slot = 0;
+            if (lane == leader) {
+                if (idx < d.brick_bound) slot = leaf_insert(d.leaf_table, d.leaf_cap, v, idx, d.counters + kCtrError);
+            }
+            slot = __shfl_sync(em, slot, leader);
+            if (idx < d.brick_bound) {
+                d.bkey[idx] = bk;
+                d.bmask[idx] = v;
+                d.bfirst[idx] = first;
+                d.bslot[idx] = slot;
+            } else {
+                atomicOr(d.counters + kCtrError, kErrBound);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Leaf owners: bricks whose mask they own get leaf positions in brick order
+// (= first occurrence in Morton order); the table slot records the leaf index.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_scan[2 * kWarps + 2];
+    __shared__ uint64_t s_base;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = dyn_tile(d.counters, 10, &s_tile);
+    const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
+    const uint32_t ntiles = (B + kBrickTile - 1) / kBrickTile;
+    if (tile >= ntiles) return;
+    const uint32_t wstart = tile * kBrickTile + warp * 32 * kBrickIT;
+    unsigned ob[kBrickIT];
+    uint32_t slot[kBrickIT];
+    uint32_t wc = 0;
+#pragma unroll
+    for (int j = 0; j < kBrickIT; ++j) {
+        uint32_t b = wstart + j * 32 + lane;
+        bool own = false;
+        slot[j] = 0;
+        if (b < B) {
+            slot[j] = d.bslot[b];
+            own = ~ld_relaxed32(&d.leaf_table[slot[j]].z) == b;
+        }
+        ob[j] = __ballot_sync(kFull, own);
+        wc += __popc(ob[j]);
+    }
+    uint32_t total;
+    uint32_t wexcl = block_excl_scan(lane == 0 ? wc : 0, s_scan, &total);
+    wexcl = __shfl_sync(kFull, wexcl, 0);
+    if (warp == 0) {
+        if (lane == 0 && tile != 0) st_relaxed(d.leafown_status + tile, kFlagAgg | total);
+        uint64_t ex = lookback_warp(d.leafown_status, tile, 0, total, d.counters + kCtrError);
+        if (lane == 0) s_base = ex;
+    }
+    __syncthreads();
+    uint32_t run = uint32_t(s_base) + wexcl;
+#pragma unroll
+    for (int j = 0; j < kBrickIT; ++j) {
+        uint32_t b = wstart + j * 32 + lane;
+        if ((ob[j] >> lane) & 1) {
+            uint32_t pos = run + __popc(ob[j] & lanemask_lt());
+            if (pos < d.brick_bound) d.leaves[pos] = d.bmask[b];
+            else atomicOr(d.counters + kCtrError, kErrBound);
+            d.leaf_table[slot[j]].w = pos;
+        }
+        run += __popc(ob[j]);
+    }
+    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrLeaves] = uint32_t(s_base + total);
+}
+
+// ---------------------------------------------------------------------------
+// Node level lv: children grouped by key >> 3 into parents (<= 8 children each),
+// words [mask, saturating count, refs...] (gbuild.zig:484-520), inserted into
+// the level's table (equal words -> same slot, owner = minimum parent index).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t hash_words(const uint32_t* w, uint32_t len) {
+    uint64_t h = len;
+    for (uint32_t k = 0; k < len; ++k) h = mix64(h ^ w[k]);
+    return h;
+}
+
+__device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, const uint32_t* all_words, uint32_t par,
+                                                const uint32_t* w, uint32_t len, uint32_t* err) {
+    uint32_t h = uint32_t(hash_words(w, len)) & (cap - 1);
+    for (uint32_t probe = 0; probe < cap; ++probe) {
+        uint32_t* kp = &table[h].x;
+        uint32_t cur = ld_relaxed32(kp);
+        if (cur == 0) {
+            cur = atomicCAS(kp, 0u, par + 1);
+            if (cur == 0) {
+                claim_owner(table + h, par);
+                return h;
+            }
+        }
+        // compare with the resident node (its words were made visible before its CAS)
+        __threadfence();
+        const uint32_t* ow = all_words + uint64_t(cur - 1) * kNodeStride;
+        uint32_t omask = __ldcg(ow);
+        if (2u + __popc(omask & 0xFF) == len) {
+            bool same = omask == w[0];
+            for (uint32_t k = 1; k < len && same; ++k) same = __ldcg(ow + k) == w[k];
+            if (same) {
+                claim_owner(table + h, par);
+                return h;
+            }
+        }
+        h = (h + 1) & (cap - 1);
+    }
+    atomicOr(err, kErrTable);
+    return 0;
+}
+
+constexpr int kNodeIT = 8;
+constexpr int kNodeTile = kBlock * kNodeIT;
+
+__global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_scan[2 * kWarps + 2];
+    __shared__ uint64_t s_base;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = dyn_tile(d.counters, L.tile_ctr_build, &s_tile);
+    const uint32_t C = L.lv == 2 ? min(d.counters[kCtrBricks], d.brick_bound)
+                                 : min(d.counters[kCtrParents + L.lv - 1], L.child_bound);
+    const uint32_t ntiles = (C + kNodeTile - 1) / kNodeTile;
+    if (tile >= ntiles) return;
+    const uint32_t wstart = tile * kNodeTile + warp * 32 * kNodeIT;
+    const uint64_t NONE = ~0ull;
+    unsigned hb[kNodeIT];
+    uint32_t wc = 0;
+    uint64_t prev = (wstart > 0 && wstart - 1 < C) ? L.ckey[wstart - 1] : NONE;
+#pragma unroll
+    for (int j = 0; j < kNodeIT; ++j) {
+        uint32_t e = wstart + j * 32 + lane;
+        uint64_t k = e < C ? L.ckey[e] : NONE;
+        uint64_t pk = __shfl_up_sync(kFull, k, 1);
+        if (lane == 0) pk = prev;
+        prev = __shfl_sync(kFull, k, 31);
+        bool head = e < C && (e == 0 || (k >> 3) != (pk >> 3));
+        hb[j] = __ballot_sync(kFull, head);
+        wc += __popc(hb[j]);
+    }
+    uint32_t total;
+    uint32_t wexcl = block_excl_scan(lane == 0 ? wc : 0, s_scan, &total);
+    wexcl = __shfl_sync(kFull, wexcl, 0);
+    if (warp == 0) {
+        if (lane == 0 && tile != 0) st_relaxed(L.build_status + tile, kFlagAgg | total);
+        uint64_t ex = lookback_warp(L.build_status, tile, 0, total, d.counters + kCtrError);
+        if (lane == 0) s_base = ex;
+    }
+    __syncthreads();
+    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrParents + L.lv] = uint32_t(s_base + total);
+    uint32_t run = uint32_t(s_base) + wexcl;
+    const uint32_t child_size = 1u << L.lv;
+#pragma unroll 1
+    for (int j = 0; j < kNodeIT; ++j) {
+        uint32_t e = wstart + j * 32 + lane;
+        if ((hb[j] >> lane) & 1) {
+            uint32_t par = run + __popc(hb[j] & lanemask_lt());
+            uint64_t pkey = L.ckey[e] >> 3;
+            uint32_t w[kNodeStride];
+            uint32_t mask = 0, count = 0, n = 0;
+            uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
+            for (uint32_t c = e; c < C && n < 8; ++c) {
+                uint64_t ck = L.ckey[c];
+                if ((ck >> 3) != pkey) break;
+                uint32_t idx = uint32_t(ck & 7);
+                mask |= 1u << idx;
+                w[2 + n] = __ldcg(&L.ctable[L.cslot[c]].w);
+                ++n;
+                uint64_t clo, chi;
+                if (L.lv == 2) {
+                    uint64_t m = L.cmask[c];
+                    count = sat_add(count, __popcll(m));
+                    if (L.need_box) brick_box(m, clo, chi);
+                } else {
+                    count = sat_add(count, L.ccnt[c]);
+                    if (L.need_box) { clo = L.clo[c]; chi = L.chi[c]; }
+                }
+                if (L.need_box) {
+                    uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size, oz = (idx >> 2) * child_size;
+                    lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
+                    lo[1] = min(lo[1], cell_y(clo) + oy); hi[1] = max(hi[1], cell_y(chi) + oy);
+                    lo[2] = min(lo[2], cell_z(clo) + oz); hi[2] = max(hi[2], cell_z(chi) + oz);
+                }
+            }
+            w[0] = mask;
+            w[1] = count;
+            if (par < L.parent_bound) {
+                uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
+                for (uint32_t k = 0; k < 2 + n; ++k) pw[k] = w[k];
+                L.pkey[par] = pkey;
+                L.pcnt[par] = count;
+                L.pfirst[par] = L.cfirst[e];
+                if (L.need_box) {
+                    L.plo[par] = pack_cell(lo[0], lo[1], lo[2]);
+                    L.phi[par] = pack_cell(hi[0], hi[1], hi[2]);
+                }
+                __threadfence();
+                L.pslot[par] = node_insert(L.ptable, L.pcap, L.pwords, par, w, 2 + n, d.counters + kCtrError);
+            } else {
+                atomicOr(d.counters + kCtrError, kErrBound);
+            }
+        }
+        run += __popc(hb[j]);
+    }
+}
+
+// Owners of level lv get word offsets (scan of their lengths) and write their words.
+__global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_scan[2 * kWarps + 2];
+    __shared__ uint64_t s_base;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = dyn_tile(d.counters, L.tile_ctr_own, &s_tile);
+    const uint32_t P = min(d.counters[kCtrParents + L.lv], L.parent_bound);
+    const uint32_t ntiles = (P + kNodeTile - 1) / kNodeTile;
+    if (tile >= ntiles) return;
+    const uint32_t cursor = d.counters[kCtrCursor + L.lv];
+    const uint32_t wstart = tile * kNodeTile + warp * 32 * kNodeIT;
+    uint32_t len[kNodeIT], slot[kNodeIT];
+    uint64_t wsum = 0;  // words | count << 31
+#pragma unroll
+    for (int j = 0; j < kNodeIT; ++j) {
+        uint32_t i = wstart + j * 32 + lane;
+        len[j] = 0;
+        slot[j] = 0;
+        if (i < P) {
+            slot[j] = L.pslot[i];
+            if (~ld_relaxed32(&L.ptable[slot[j]].z) == i) len[j] = 2 + __popc(L.pwords[uint64_t(i) * kNodeStride] & 0xFF);
+        }
+        uint64_t v = len[j] | (uint64_t(len[j] ? 1 : 0) << 31);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        wsum += v;
+    }
+    uint64_t total;
+    uint64_t wexcl = block_excl_scan64(lane == 0 ? wsum : 0, s_scan, &total);
+    wexcl = __shfl_sync(kFull, wexcl, 0);
+    if (warp == 0) {
+        if (lane == 0 && tile != 0) st_relaxed(L.own_status + tile, kFlagAgg | total);
+        uint64_t ex = lookback_warp(L.own_status, tile, 0, total, d.counters + kCtrError);
+        if (lane == 0) s_base = ex;
+    }
+    __syncthreads();
+    uint32_t run = uint32_t(s_base & 0x7FFFFFFFu) + uint32_t(wexcl & 0x7FFFFFFFu);
+#pragma unroll
+    for (int j = 0; j < kNodeIT; ++j) {
+        uint32_t i = wstart + j * 32 + lane;
+        uint32_t x = len[j];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(kFull, x, o);
+            if (lane >= unsigned(o)) x += y;
+        }
+        uint32_t off = run + x - len[j];
+        if (len[j]) {
+            uint32_t dst = cursor + off;
+            const uint32_t* src = L.pwords + uint64_t(i) * kNodeStride;
+            if (uint64_t(dst) + len[j] <= d.node_bound) {
+                for (uint32_t k = 0; k < len[j]; ++k) d.nodes[dst + k] = src[k];
+            } else {
+                atomicOr(d.counters + kCtrError, kErrBound);
+            }
+            L.ptable[slot[j]].w = dst;
+        }
+        run += __shfl_sync(kFull, x, 31);
+    }
+    if (tile == ntiles - 1 && threadIdx.x == 0) {
+        uint64_t t = s_base + total;
+        d.counters[kCtrCursor + L.lv + 1] = cursor + uint32_t(t & 0x7FFFFFFFu);
+        d.counters[kCtrUniqueLv + L.lv] = uint32_t(t >> 31);
+    }
+}
+
+// Empty levels still have to pass the cursor on.
+__global__ void k_level_cursor(BuildDesc d, uint32_t lv) {
+    if (threadIdx.x == 0 && d.counters[kCtrParents + lv] == 0) d.counters[kCtrCursor + lv + 1] = d.counters[kCtrCursor + lv];
+}
+
+// ---------------------------------------------------------------------------
+// RT prims of the parents of level rt_log2 - 1 (gbuild.zig:574-605): node
+// offset, attribute rank relative to the chunk, cell, AABB base + lo - 1/256 and
+// base + hi + 1/256 in f32 (adds in the reference's order, no FMA possible).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_prims(BuildDesc d, LevelDesc L) {
+    const uint32_t P = min(d.counters[kCtrParents + L.lv], L.parent_bound);
+    const uint32_t local_shift = 3 * (d.log2 - d.rt_log2);
+    const uint32_t size = 1u << d.rt_log2;
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < P; i += gridDim.x * kBlock) {
+        if (i >= d.prim_bound) { atomicOr(d.counters + kCtrError, kErrBound); break; }
+        uint64_t full = L.pkey[i];
+        uint64_t key = full & ((1ull << local_shift) - 1);
+        uint32_t chunk = uint32_t(full >> local_shift);
+        uint32_t cx = compact3(key), cy = compact3(key >> 1), cz = compact3(key >> 2);
+        uint32_t first = d.chunked ? d.chunk_first[chunk] : 0;
+        uint32_t node = __ldcg(&L.ptable[L.pslot[i]].w);
+        uint4 rec;
+        rec.x = node;
+        rec.y = L.pfirst[i] - first;
+        uint64_t pc = pack_cell(cx, cy, cz);
+        rec.z = uint32_t(pc);
+        rec.w = uint32_t(pc >> 32);
+        reinterpret_cast<uint4*>(d.prims)[i] = rec;
+        uint64_t lo = L.plo[i], hi = L.phi[i];
+        const float eps = 1.0f / 256.0f;
+        float* box = d.aabbs + uint64_t(i) * 6;
+        box[0] = __fsub_rn(__fadd_rn(float(cx * size), float(cell_x(lo))), eps);
+        box[1] = __fsub_rn(__fadd_rn(float(cy * size), float(cell_y(lo))), eps);
+        box[2] = __fsub_rn(__fadd_rn(float(cz * size), float(cell_z(lo))), eps);
+        box[3] = __fadd_rn(__fadd_rn(float(cx * size), float(cell_x(hi))), eps);
+        box[4] = __fadd_rn(__fadd_rn(float(cy * size), float(cell_y(hi))), eps);
+        box[5] = __fadd_rn(__fadd_rn(float(cz * size), float(cell_z(hi))), eps);
+        if (d.chunked && (i == 0 || (L.pkey[i - 1] >> local_shift) != chunk)) d.prim_start[chunk] = i;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.counters[kCtrPrims] = P;
+}
+
+// Root(s), node word count and the empty geometry (gbuild.zig:607-624).
+__global__ void __launch_bounds__(kBlock) k_finalize(BuildDesc d, LevelDesc top) {
+    const uint32_t P = min(d.counters[kCtrParents + top.lv], top.parent_bound);
+    if (d.chunked) {
+        for (uint32_t i = threadIdx.x; i < P; i += kBlock) {
+            uint32_t chunk = uint32_t(top.pkey[i]);
+            if (chunk < d.seg_count) d.roots[chunk] = __ldcg(&top.ptable[top.pslot[i]].w);
+        }
+    }
+    if (threadIdx.x == 0) {
+        uint32_t cursor = d.counters[kCtrCursor + top.lv + 1];
+        uint32_t root = P > 0 ? __ldcg(&top.ptable[top.pslot[0]].w) : 0;
+        if (d.counters[kCtrUnique] == 0) {
+            if (cursor + 2 <= d.node_bound) {
+                d.nodes[cursor] = 0;
+                d.nodes[cursor + 1] = 0;
+            }
+            root = cursor;
+            cursor += 2;
+            d.counters[kCtrPrims] = 0;
+        }
+        d.counters[kCtrRoot] = root;
+        d.counters[kCtrWords] = cursor;
+    }
+}
+
+}  // namespace pyrb

@@ -1,0 +1,202 @@
+"""Host mirror of the reference's GPU build interface (src/gpu_build.zig) over the C ABI.
+
+Same operations, argument meaning and error behaviour as the reference:
+
+* :func:`build`          gpu_build.build        (src/gpu_build.zig:94-96)
+* :func:`build_chunks`   gpu_build.buildChunks  (src/gpu_build.zig:119-122)
+* :func:`build_chunks_edits` World.applyEdits + buildChunks as one sort-merge
+                         (src/world.zig:902-1020, src/device/worldedit.zig:26-90)
+* :func:`downsample`     gpu_build.downsample   (src/gpu_build.zig:128-131)
+* :class:`Built`         gpu_build.Built        (src/gpu_build.zig:26-47)
+
+Device buffers are torch CUDA tensors (plumbing only) or raw device addresses;
+invalid arguments raise :class:`native.PyrbError` with result -1 (INVALID_ARGUMENT).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native
+
+
+def _addr(t) -> int:
+    if t is None:
+        return 0
+    if isinstance(t, int):
+        return t
+    return int(t.data_ptr())
+
+
+def _exec(stream=None) -> native.Exec:
+    e = native.Exec()
+    e.ctx = None
+    e.stream = None if stream is None else ctypes.c_void_p(int(stream))
+    return e
+
+
+def _current_stream():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+class Built:
+    """Result of a build. All buffers are device memory owned by this object (freed on
+    :meth:`free` / garbage collection) -- the reference's Built.free."""
+
+    def __init__(self, c: native.BuiltC, stream):
+        self._c = c
+        self._stream = stream
+        self.roots = self.first_voxel = self.first_prim = None
+
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+        return getattr(self._c, name)
+
+    def free(self):
+        if self._c is not None and self._c.nodes:
+            native.lib().pyrb_built_free(ctypes.byref(_exec(self._stream)), ctypes.byref(self._c))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def download(self) -> "HostBuilt":
+        """Copies the result to host arrays (synchronous)."""
+        from . import _cudart
+        c = self._c
+
+        def fetch(addr, n, dtype):
+            out = np.empty(n, dtype=dtype)
+            _cudart.dtoh(out.ctypes.data, addr, out.nbytes)
+            return out
+
+        return HostBuilt(
+            log2_size=c.log2_size, rt_log2=c.rt_log2, root=c.root,
+            nodes=fetch(c.nodes, c.node_words, np.uint32),
+            leaves=fetch(c.leaves, c.leaf_count, np.uint64),
+            keys=fetch(c.keys, c.voxel_count, np.uint64),
+            attrs=fetch(c.attrs, c.voxel_count, np.uint32),
+            prims=fetch(c.prims, c.prim_count * 16, np.uint8),
+            aabbs=fetch(c.aabbs, c.prim_count * 6, np.float32),
+            roots=self.roots, first_voxel=self.first_voxel, first_prim=self.first_prim,
+        )
+
+
+@dataclass
+class HostBuilt:
+    log2_size: int
+    rt_log2: int
+    root: int
+    nodes: np.ndarray
+    leaves: np.ndarray
+    keys: np.ndarray
+    attrs: np.ndarray
+    prims: np.ndarray
+    aabbs: np.ndarray
+    roots: np.ndarray | None = None
+    first_voxel: np.ndarray | None = None
+    first_prim: np.ndarray | None = None
+
+    @property
+    def node_words(self):
+        return len(self.nodes)
+
+    @property
+    def voxel_count(self):
+        return len(self.attrs)
+
+    @property
+    def prim_count(self):
+        return len(self.prims) // 16
+
+
+def build(log2_size: int, rt_log2_req: int, edits=None, n_new: int | None = None, old_keys=None, old_vals=None,
+          n_old: int = 0, stream=None) -> Built:
+    """gpu_build.build: `edits` is a device PyrVoxel array (uint32/int32 [n, 4] tensor or address);
+    `old_keys`/`old_vals` the sorted unique voxels of a previous build (copied, not consumed)."""
+    if n_new is None:
+        n_new = 0 if edits is None else int(edits.shape[0])
+    if old_keys is not None and not isinstance(old_keys, int) and n_old == 0:
+        n_old = int(old_keys.shape[0])
+    stream = _current_stream() if stream is None else stream
+    out = native.BuiltC()
+    native.check(native.lib().pyrb_build(ctypes.byref(_exec(stream)), log2_size, rt_log2_req, _addr(old_keys),
+                                         _addr(old_vals), n_old, _addr(edits), n_new, ctypes.byref(out)))
+    return Built(out, stream)
+
+
+def geometry_build(log2_size: int, rt_log2_req: int, voxels: np.ndarray, stream=None) -> Built:
+    """pyr_geometry_build with PYR_BUILD_HOST_INPUT: host PyrVoxel array uploaded by the library."""
+    v = np.ascontiguousarray(voxels, dtype=np.uint32)
+    stream = _current_stream() if stream is None else stream
+    out = native.BuiltC()
+    native.check(native.lib().pyrb_geometry_build(ctypes.byref(_exec(stream)), log2_size, rt_log2_req,
+                                                  v.ctypes.data if len(v) else None, len(v),
+                                                  native.PYRB_BUILD_HOST_INPUT, ctypes.byref(out)))
+    return Built(out, stream)
+
+
+def build_chunks(log2_size: int, rt_log2_req: int, count: int, capacity: int, voxels, offsets, total: int,
+                 stream=None) -> Built:
+    """gpu_build.buildChunks: voxels device PyrVoxel[count*capacity], offsets device u32[count+1]."""
+    stream = _current_stream() if stream is None else stream
+    b = native.ChunkBatch(count=count, capacity=capacity, voxels=_addr(voxels), offsets=_addr(offsets), total=total)
+    roots = np.zeros(count, np.uint32)
+    first = np.zeros(count, np.uint32)
+    prim = np.zeros(count, np.uint32)
+    out = native.BuiltC()
+    native.check(native.lib().pyrb_build_chunks(ctypes.byref(_exec(stream)), log2_size, rt_log2_req, ctypes.byref(b),
+                                                roots.ctypes.data, first.ctypes.data, prim.ctypes.data,
+                                                ctypes.byref(out)))
+    r = Built(out, stream)
+    r.roots, r.first_voxel, r.first_prim = roots, first, prim
+    return r
+
+
+def build_chunks_edits(log2_size: int, rt_log2_req: int, count: int, capacity: int, voxels, counts, edits,
+                       edit_offsets, edit_total: int, stream=None) -> Built:
+    """World path: generated voxels per chunk (counts) with each chunk's overlay edits merged."""
+    stream = _current_stream() if stream is None else stream
+    roots = np.zeros(count, np.uint32)
+    first = np.zeros(count, np.uint32)
+    prim = np.zeros(count, np.uint32)
+    out = native.BuiltC()
+    native.check(native.lib().pyrb_build_chunks_edits(
+        ctypes.byref(_exec(stream)), log2_size, rt_log2_req, count, capacity, _addr(voxels), _addr(counts),
+        _addr(edits), _addr(edit_offsets), edit_total, roots.ctypes.data, first.ctypes.data, prim.ctypes.data,
+        ctypes.byref(out)))
+    r = Built(out, stream)
+    r.roots, r.first_voxel, r.first_prim = roots, first, prim
+    return r
+
+
+def downsample(log2_src: int, rt_log2_req: int, src_keys, src_vals, n_src: int, shift: int, stream=None) -> Built:
+    """gpu_build.downsample: LOD from the sorted voxels (keys/attrs) of a previous build."""
+    stream = _current_stream() if stream is None else stream
+    out = native.BuiltC()
+    native.check(native.lib().pyrb_downsample(ctypes.byref(_exec(stream)), log2_src, rt_log2_req, _addr(src_keys),
+                                              _addr(src_vals), n_src, shift, ctypes.byref(out)))
+    return Built(out, stream)
+
+
+def last_stats() -> native.Stats:
+    s = native.Stats()
+    native.lib().pyrb_last_stats(ctypes.byref(s))
+    return s
+
+
+def set_tuning(radix_bits: int = 8, tile_keys: int = 4096, load_factor_pct: int = 50) -> None:
+    t = native.Tuning(radix_bits=radix_bits, tile_keys=tile_keys, load_factor_pct=load_factor_pct)
+    native.check(native.lib().pyrb_set_tuning(ctypes.byref(t)))
+
+
+def get_tuning() -> native.Tuning:
+    t = native.Tuning()
+    native.lib().pyrb_get_tuning(ctypes.byref(t))
+    return t

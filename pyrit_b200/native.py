@@ -1,0 +1,118 @@
+"""ctypes binding of libpyrit_b200.so (the C ABI of include/pyrit_b200.h).
+
+There is no fallback: if the CUDA library is missing or cannot be loaded, every
+entry point raises. The library is built in-tree by ``pyrit_b200._build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpyrit_b200.so")
+
+PYRB_OK = 0
+PYRB_ERROR_INVALID_ARGUMENT = -1
+PYRB_ERROR_OUT_OF_MEMORY = -3
+PYRB_ERROR_CUDA = -6
+PYRB_BUILD_HOST_INPUT = 0x1
+
+ALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64)
+FREE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint64)
+
+
+class Exec(ctypes.Structure):
+    """pyrb_exec: stream + optional allocator callbacks (gpu_build.Exec)."""
+    _fields_ = [("ctx", ctypes.c_void_p), ("stream", ctypes.c_void_p), ("alloc", ALLOC_FN), ("free", FREE_FN)]
+
+
+class BuiltC(ctypes.Structure):
+    """pyrb_built (gpu_build.Built, src/gpu_build.zig:26-47)."""
+    _fields_ = [
+        ("log2_size", ctypes.c_uint32), ("rt_log2", ctypes.c_uint32),
+        ("nodes", ctypes.c_uint64), ("node_words", ctypes.c_uint32), ("root", ctypes.c_uint32),
+        ("leaves", ctypes.c_uint64), ("leaf_count", ctypes.c_uint32), ("reserved0", ctypes.c_uint32),
+        ("keys", ctypes.c_uint64), ("attrs", ctypes.c_uint64), ("voxel_count", ctypes.c_uint32),
+        ("reserved1", ctypes.c_uint32),
+        ("prims", ctypes.c_uint64), ("aabbs", ctypes.c_uint64), ("prim_count", ctypes.c_uint32),
+        ("reserved2", ctypes.c_uint32),
+    ]
+
+
+class ChunkBatch(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint32), ("capacity", ctypes.c_uint32), ("voxels", ctypes.c_uint64),
+                ("offsets", ctypes.c_uint64), ("total", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("brick_count", ctypes.c_uint32), ("level_parents", ctypes.c_uint32 * 24),
+                ("level_unique", ctypes.c_uint32 * 24), ("sort_passes", ctypes.c_uint32),
+                ("radix_bits", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("scratch_bytes", ctypes.c_uint64),
+                ("output_bytes", ctypes.c_uint64)]
+
+
+COUNTS_WORDS = 176
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("radix_bits", ctypes.c_uint32), ("tile_keys", ctypes.c_uint32),
+                ("load_factor_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+# name -> (restype, argtypes); every symbol declared in include/pyrit_b200.h
+_u32, _u64, _p = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
+_pu32 = ctypes.POINTER(ctypes.c_uint32)
+SIGNATURES = {
+    "pyrb_build": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32, _u32, _u64, _u64, _u32, _u64, _u32,
+                                    ctypes.POINTER(BuiltC)]),
+    "pyrb_build_chunks": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32, _u32, ctypes.POINTER(ChunkBatch), _p, _p, _p,
+                                           ctypes.POINTER(BuiltC)]),
+    "pyrb_build_chunks_edits": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32, _u32, _u32, _u32, _u64, _u64, _u64,
+                                                 _u64, _u32, _p, _p, _p, ctypes.POINTER(BuiltC)]),
+    "pyrb_downsample": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32, _u32, _u64, _u64, _u32, _u32,
+                                         ctypes.POINTER(BuiltC)]),
+    "pyrb_geometry_build": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32, _u32, _p, _u32, _u32,
+                                             ctypes.POINTER(BuiltC)]),
+    "pyrb_build_async": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32, _u32, _u64, _u64, _u32, _u64, _u32, _p,
+                                          ctypes.POINTER(BuiltC)]),
+    "pyrb_build_finish": (ctypes.c_int32, [_p, ctypes.POINTER(BuiltC)]),
+    "pyrb_profile_enable": (None, [ctypes.c_int]),
+    "pyrb_profile_read": (ctypes.c_uint32, [_p, _p, _u32, _u32]),
+    "pyrb_built_free": (None, [ctypes.POINTER(Exec), ctypes.POINTER(BuiltC)]),
+    "pyrb_last_stats": (None, [ctypes.POINTER(Stats)]),
+    "pyrb_error_message": (ctypes.c_char_p, []),
+    "pyrb_result_string": (ctypes.c_char_p, [ctypes.c_int32]),
+    "pyrb_set_tuning": (ctypes.c_int32, [ctypes.POINTER(Tuning)]),
+    "pyrb_get_tuning": (None, [ctypes.POINTER(Tuning)]),
+    "pyrb_version": (ctypes.c_uint32, []),
+}
+
+_lib = None
+
+
+class PyrbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (result {code})")
+        self.code = code
+
+
+def lib():
+    """Loads the CUDA library; raises if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m pyrit_b200._build` "
+                               "(the DAG build has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int) -> None:
+    if code != PYRB_OK:
+        raise PyrbError(code, lib().pyrb_error_message().decode(errors="replace"))

@@ -1,0 +1,176 @@
+"""Bit-exact parity of the CUDA build with the oracle (restatement of the reference
+GPU algorithm, src/device/gbuild.zig + src/gpu_build.zig) on seeded inputs, and
+canonical parity with the CPU builder (src/dag_builder.zig). Calls go through the
+C ABI (libpyrit_b200.so) via pyrit_b200.gpu_build."""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from pyrit_b200 import workloads as wl
+
+from gpu_helpers import assert_same_build, dev
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gb():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    from pyrit_b200 import gpu_build
+    return gpu_build
+
+
+def _scene_points(log2, seed=21, dups=200):
+    dense = wl.scene_dense(log2)
+    pts = wl.dense_to_points(dense, log2)
+    np.random.default_rng(seed).shuffle(pts)
+    d = pts[:dups].copy()
+    pts = np.concatenate([pts, d, np.array([[0xFFFFFFFF, 0, 0, 5], [1 << log2, 0, 0, 5]], np.uint32)])
+    return dense, pts
+
+
+@pytest.mark.parametrize("log2,rt", [(6, 4), (6, 3), (6, 6), (5, 5), (3, 3), (4, 3)])
+def test_scene_matches_oracle(gb, log2, rt):
+    """tests/cpu_test.zig:758-807 input: shuffled scene with duplicates and outliers."""
+    _, pts = _scene_points(log2)
+    g = gb.build(log2, rt, dev(pts)).download()
+    o = orc.gb_build(log2, rt, pts)
+    assert_same_build(g, o, label=f"scene log2={log2} rt={rt}")
+
+
+def test_heightfield_matches_oracle_and_cpu_builder(gb):
+    """64^3 heightfield (plain single-chunk build): P1 bytes vs oracle, P2 canonical vs CPU builder."""
+    pts = wl.heightfield(6, 0)
+    g = gb.build(6, 4, dev(pts)).download()
+    o = orc.gb_build(6, 4, pts)
+    assert_same_build(g, o, label="heightfield")
+    c = orc.cpu_build_points(6, pts)
+    cn, croot, shared, lu = orc.canonicalize(6, c.nodes, c.root)
+    assert np.array_equal(g.leaves, c.leaves)
+    assert np.array_equal(g.attrs, c.attrs)
+    assert shared == 0
+    assert np.array_equal(cn, g.nodes) and croot == g.root
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_heightfield_seeds(gb, seed):
+    pts = wl.heightfield(6, seed)
+    g = gb.build(6, 4, dev(pts)).download()
+    assert_same_build(g, orc.gb_build(6, 4, pts), label=f"heightfield seed {seed}")
+
+
+def test_empty_and_tiny(gb):
+    for pts in [np.zeros((0, 4), np.uint32),
+                np.array([[5, 6, 7, 42]], np.uint32),
+                np.array([[5, 6, 7, 42], [5, 6, 7, 0]], np.uint32),          # deleted again
+                np.array([[-1 & 0xFFFFFFFF, 0, 0, 3], [16, 0, 0, 3]], np.uint32),  # all outside
+                np.array([[1, 1, 1, 9], [1, 1, 1, 10], [1, 1, 1, 11]], np.uint32)]:  # last wins
+        g = gb.build(4, 4, dev(pts), n_new=len(pts)).download()
+        assert_same_build(g, orc.gb_build(4, 4, pts), label=f"tiny {pts.tolist()}")
+
+
+def test_edit_path_matches_oracle(gb):
+    """cpu_test.zig:809-850: edits on top of the sorted voxels of a previous build."""
+    base = np.array([[x, 0, z, 0x10] for z in range(32) for x in range(32)], np.uint32)
+    b1 = gb.build(5, 3, dev(base))
+    edits = np.array([[10, y, 10, 0x20] for y in range(1, 20)] + [[x, 0, 3, 0] for x in range(8)] +
+                     [[20, 0, 20, 0x30]], np.uint32)
+    b2 = gb.build(5, 3, dev(edits), old_keys=b1.keys, old_vals=b1.attrs, n_old=b1.voxel_count).download()
+    o1 = orc.gb_build(5, 3, base)
+    o2 = orc.gb_build(5, 3, edits, o1.keys, o1.attrs)
+    assert_same_build(b2, o2, label="edit")
+
+
+def test_downsample_matches_oracle(gb):
+    log2 = 6
+    pts = wl.dense_to_points(wl.scene_dense(log2), log2)
+    full = gb.build(log2, 3, dev(pts))
+    ofull = orc.gb_build(log2, 3, pts)
+    for shift in (1, 2, 3):
+        g = gb.downsample(log2, 3, full.keys, full.attrs, full.voxel_count, shift).download()
+        o = orc.gb_downsample(log2, 3, ofull.keys, ofull.attrs, shift)
+        assert_same_build(g, o, label=f"downsample {shift}")
+
+
+def _shell_chunks(k=5, cap=8000, n=32):
+    vox = np.zeros((k * cap, 4), np.uint32)
+    cnt = np.zeros(k, np.uint32)
+    idx = np.arange(n ** 3)
+    x, y, z = idx % n, (idx // n) % n, idx // (n * n)
+    d2 = (x - 15.5) ** 2 + (y - 15.5) ** 2 + (z - 15.5) ** 2
+    for c in range(k):
+        if c == 3:
+            continue
+        r = 6 + 2 * c
+        sel = np.nonzero((d2 < r * r) & (d2 > (r - 2) ** 2))[0][:cap]
+        attrs = np.array([wl.lib().wl_attr_of(int(x[i] + c), int(y[i]), int(z[i])) for i in sel], np.uint32)
+        vox[c * cap:c * cap + len(sel)] = np.stack([x[sel], y[sel], z[sel], attrs], 1)
+        cnt[c] = len(sel)
+    offs = np.concatenate([[0], np.cumsum(cnt)]).astype(np.uint32)
+    return vox, cnt, offs
+
+
+@pytest.mark.parametrize("rt", [4, 3, 5])
+def test_chunks_match_oracle(gb, rt):
+    """cpu_test.zig:1001-1060 batch (chunk 3 empty) -- bytes, roots, first voxels, first prims."""
+    k, cap, log2 = 5, 8000, 5
+    vox, cnt, offs = _shell_chunks(k, cap)
+    g = gb.build_chunks(log2, rt, k, cap, dev(vox), dev(offs), int(offs[-1])).download()
+    o = orc.gb_build_chunks(log2, rt, cap, vox, offs)
+    assert_same_build(g, o, chunks=True, label=f"chunks rt={rt}")
+
+
+def test_many_small_chunks_match_oracle(gb):
+    """Many chunks of mixed occupancy (incl. empty ones): the per-segment sort tiling."""
+    rng = np.random.default_rng(5)
+    k, cap, log2 = 37, 3000, 4
+    vox = np.zeros((k * cap, 4), np.uint32)
+    cnt = np.zeros(k, np.uint32)
+    for c in range(k):
+        m = int(rng.integers(0, cap + 1)) if c % 5 else 0
+        v = rng.integers(0, 16, (m, 3)).astype(np.uint32)
+        a = rng.integers(0, 6, (m, 1)).astype(np.uint32)  # attribute 0 deletes
+        vox[c * cap:c * cap + m] = np.concatenate([v, a], 1)
+        cnt[c] = m
+    offs = np.concatenate([[0], np.cumsum(cnt)]).astype(np.uint32)
+    g = gb.build_chunks(log2, 3, k, cap, dev(vox), dev(offs), int(offs[-1])).download()
+    o = orc.gb_build_chunks(log2, 3, cap, vox, offs)
+    assert_same_build(g, o, chunks=True, label="many chunks")
+
+
+def test_noise256_with_edits_matches_oracle(gb):
+    """256^3 noise grid + 0.5% edit overlay (the headline plain-build workload)."""
+    vox = wl.noise_grid(8, 0)
+    ed = wl.noise_edits(8, 0)
+    pts = np.concatenate([vox, ed])
+    g = gb.build(8, 7, dev(pts)).download()
+    o = orc.gb_build(8, 7, pts)
+    assert_same_build(g, o, label="noise256")
+
+
+@pytest.mark.parametrize("radix_bits,tile_keys,lf", [(4, 1024, 50), (8, 2048, 70), (11, 4096, 50), (11, 1024, 90),
+                                                     (8, 4096, 25)])
+def test_tuning_variants_are_bit_exact(gb, radix_bits, tile_keys, lf):
+    """The autotuner's knobs (digit width, tile, load factor) never change the output."""
+    _, pts = _scene_points(6)
+    o = orc.gb_build(6, 4, pts)
+    old = gb.get_tuning()
+    try:
+        gb.set_tuning(radix_bits, tile_keys, lf)
+        g = gb.build(6, 4, dev(pts)).download()
+    finally:
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+    assert_same_build(g, o, label=f"tuning {radix_bits}/{tile_keys}/{lf}")
+
+
+def test_invalid_arguments(gb):
+    from pyrit_b200.native import PyrbError
+    pts = dev(np.array([[1, 1, 1, 1]], np.uint32))
+    for log2 in (2, 21):
+        with pytest.raises(PyrbError) as ei:
+            gb.build(log2, 3, pts, n_new=1)
+        assert ei.value.code == -1
+    with pytest.raises(PyrbError) as ei:
+        gb.downsample(6, 3, 0, 0, 0, 4)
+    assert ei.value.code == -1
