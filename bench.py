@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 DAG build (one JSON line on rank 0).
+
+Workload (N=1 and every rank of N>1): plain single-chunk build of a 256^3 grid of
+thresholded 3-octave value noise (~30% solid, materials 1..8 per 8^3 block) with a
+0.5% set/remove edit overlay applied in the same build -- seeded synthetic input of
+the shapes the metric is quoted on. A step is one full build (encode, onesweep
+sort, unique, bricks/leaves, all node levels, prims) of that input.
+
+  value   unique voxels built per second over all ranks, device time of the build
+          with the input resident in HBM (CUDA events per step; L2 is flushed by a
+          512 MiB write between steps, outside the timed events).
+  e2e     the same metric through the public C ABI with HOST input
+          (pyrb_geometry_build + PYRB_BUILD_HOST_INPUT from pinned memory), which
+          uploads the input and reads the counts back every step (wall clock).
+  roofline  the onesweep scatter pass (dominant kernel): algorithmic bytes per launch
+          (16 B per entry: key+value read and written) / mean launch time from
+          per-stage CUDA events, against the measured HBM copy bandwidth.
+  cpu_baseline  the reference's CPU builder (restated in oracle/: hash-map overlay
+          merge + buildPoints, src/dag_builder.zig) on one host core, one build.
+
+--impl reference runs that CPU builder alone (rank 0) on the same workload.
+Multi-GPU: every rank builds its own copy (replicas; a single volume does not
+shard), value = sum over ranks, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DAG-build voxels/s"
+WORKLOAD = "plain single-chunk build: 256^3 3-octave value noise > 70th percentile (~30% solid), +0.5% set/remove edits"
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def make_input():
+    from pyrit_b200 import workloads as wl
+    vox = wl.noise_grid(8, 0)
+    ed = wl.noise_edits(8, 0)
+    return vox, ed, np.concatenate([vox, ed])
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.strip().strip("|").split("|")
+        if len(parts) >= 3 and parts[0].strip() == kernel:
+            try:
+                return int(parts[2].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """NVML samples of SM clock and clock-event reasons while the timed region runs."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, device_index: int):
+        self.samples, self.reasons, self.ok = [], 0, False
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            try:
+                self.h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+
+    def _reasons(self):
+        try:
+            return self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        except Exception:
+            return self.nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                self.reasons |= int(self._reasons())
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        names = [n for b, n in self.REASONS.items() if self.reasons & b and b != 0x1]
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples)}
+
+
+def cpu_builder_time(vox, ed, reps=1):
+    """Reference CPU builder (oracle restatement) on one core: seconds per build, voxels."""
+    from oracle import oracle as orc
+    best, n = None, 0
+    for _ in range(reps):
+        t = time.perf_counter()
+        d = orc.cpu_build_overlay(8, vox, ed)
+        dt = time.perf_counter() - t
+        best = dt if best is None else min(best, dt)
+        n = d.voxel_count
+    return best, n
+
+
+def sub_volume(pts, log2):
+    """Entries of the workload inside the octant [0, 2^log2)^3 (a bounded CPU sample)."""
+    m = (pts[:, 0] < (1 << log2)) & (pts[:, 1] < (1 << log2)) & (pts[:, 2] < (1 << log2))
+    return pts[m]
+
+
+def run_reference(args):
+    rank = _env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    vox, ed, _ = make_input()
+    # one full build takes ~2-3 s on one core: shrink the per-step sample for long runs
+    runs = args.steps + args.warmup
+    log2 = 8 if runs <= 50 else (7 if runs <= 400 else 6)
+    if log2 < 8:
+        vox, ed = sub_volume(vox, log2), sub_volume(ed, log2)
+    from oracle import oracle as orc
+
+    def one():
+        t = time.perf_counter()
+        d = orc.cpu_build_overlay(log2, vox, ed)
+        return time.perf_counter() - t, d.voxel_count
+
+    for _ in range(args.warmup):
+        one()
+    times, n = [], 0
+    for _ in range(args.steps):
+        dt, n = one()
+        times.append(dt)
+    total = sum(times)
+    value = n * len(times) / total
+    sample = ("one full build of the workload per step" if log2 == 8 else
+              "per step the %d^3 octant of the workload (same voxels and edits inside it)" % (1 << log2))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "log2_size": 8, "sample_log2": log2, "unique_voxels_per_sample": n},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": 1, "kind": "port",
+                         "sample": sample + ": hash-map edit merge + buildPoints "
+                                   "(src/dag_builder.zig restated in oracle/dag_cpu.cpp), single thread"},
+        "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    from pyrit_b200 import gpu_build, native
+
+    rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    L = native.lib()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    vox, ed, pts = make_input()
+    n_in = len(pts)
+    dpts = torch.from_numpy(pts.view(np.int32)).cuda()
+    host = torch.from_numpy(pts.view(np.int32)).pin_memory()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    counts = torch.zeros(native.COUNTS_WORDS, dtype=torch.int32).pin_memory()
+    counts_ptr = counts.data_ptr()
+    ex = native.Exec()
+    ex.stream = ctypes.c_void_p(sptr)
+
+    def build_async():
+        out = native.BuiltC()
+        native.check(L.pyrb_build_async(ctypes.byref(ex), 8, 7, 0, 0, 0, dpts.data_ptr(), n_in,
+                                        ctypes.c_void_p(counts_ptr), ctypes.byref(out)))
+        return out
+
+    def release(out):
+        L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(out))
+
+    # warm-up (also validates one result against itself between runs)
+    for _ in range(max(args.warmup, 1)):
+        o = build_async()
+        release(o)
+    stream.synchronize()
+    o = native.BuiltC()
+    native.check(L.pyrb_build_finish(ctypes.c_void_p(counts_ptr), ctypes.byref(o)))
+    n_u = o.voxel_count
+    st = gpu_build.last_stats()
+    launches_per_build = st.kernel_launches
+
+    # timed region: K builds, L2 flushed between them outside the events
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            flush.fill_(s & 0xFF)
+            evs[s][0].record(stream)
+            o = build_async()
+            evs[s][1].record(stream)
+            release(o)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    o = native.BuiltC()
+    native.check(L.pyrb_build_finish(ctypes.c_void_p(counts_ptr), ctypes.byref(o)))
+    assert o.voxel_count == n_u, "result changed between runs"
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    t_ms = sum(step_ms)
+    t_max = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    t_ms = float(t_max.item())
+    value = world * n_u * args.steps / (t_ms / 1e3)
+
+    # per-stage profile (CUDA events after every launch of the build)
+    L.pyrb_profile_enable(1)
+    stage = {}
+    prof_steps = min(args.steps, 20)
+    for s in range(prof_steps):
+        flush.fill_(s & 0xFF)
+        b = gpu_build.build(8, 7, dpts, stream=sptr)
+        ms = (ctypes.c_float * 256)()
+        names = ctypes.create_string_buffer(256 * 32)
+        k = L.pyrb_profile_read(ms, names, 32, 256)
+        for i in range(min(k, 256)):
+            nm = names.raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode()
+            stage.setdefault(nm, []).append(ms[i])
+        b.free()
+    L.pyrb_profile_enable(0)
+    stage_ms = {k: statistics.mean(v) for k, v in stage.items()}
+    sort_keys = [k for k in stage_ms if k.startswith("sort_pass")]
+    sort_ms = statistics.mean(stage_ms[k] for k in sort_keys)
+    sort_bytes = 16 * n_in
+    peak, peak_kind = load_peaks()
+    achieved = sort_bytes / (sort_ms / 1e3) / 1e9
+    traffic = committed_traffic("k_sort_pass")
+
+    # whole-build algorithmic bytes (read input once; write keys+attrs, leaves, nodes, prims)
+    alg_bytes = 16 * n_in + 12 * n_u + 8 * o.leaf_count + 4 * o.node_words + 40 * o.prim_count
+    hbm_gbs = alg_bytes * args.steps / (t_ms / 1e3) / 1e9 / world
+
+    # e2e through the public C ABI with host input
+    e2e_steps = min(args.steps, 20)
+    e2e_times = []
+    if dist:
+        dist.barrier()
+    for s in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b = gpu_build.geometry_build(8, 7, host.numpy().view(np.uint32), stream=sptr)
+        e2e_times.append(time.perf_counter() - t0)
+        assert b.voxel_count == n_u
+        b.free()
+    e2e_s = torch.tensor([sum(e2e_times)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e_value = world * n_u * e2e_steps / float(e2e_s.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dt, n = cpu_builder_time(vox, ed, reps=1)
+        cpu = {"value": n / dt, "unit": "voxels/s", "cores": 1, "kind": "port",
+               "sample": "one full build of the same workload: hash-map edit merge + buildPoints "
+                         "(src/dag_builder.zig restated in oracle/dag_cpu.cpp), single thread, %.2f s" % dt}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded value noise + edit overlay)",
+            "config": {"workload": WORKLOAD, "log2_size": 8, "entries": n_in, "unique_voxels": n_u,
+                       "bricks": st.brick_count, "leaves": o.leaf_count, "node_words": o.node_words,
+                       "prims": o.prim_count, "sort_passes": st.sort_passes, "radix_bits": st.radix_bits,
+                       "l2": "flushed between steps (512 MiB write outside the timed events)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "hbm_gbs": hbm_gbs,
+            "roofline": {"bound": "hbm", "kernel": "k_sort_pass", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": sort_bytes, "mean_launch_ms": sort_ms},
+            "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 16 * n_in,
+                    "d2h_bytes_per_step": 4 * 160, "ms_per_step": 1e3 * float(e2e_s.item()) / e2e_steps},
+            "gpu_launches": launches_per_build * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

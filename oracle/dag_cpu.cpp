@@ -249,6 +249,30 @@ int orc_cpu_build_points(uint32_t log2_size, const uint32_t* points, uint64_t n,
     return 0;
 }
 
+// Edit overlay on the CPU path: the edits are merged into the voxel list with a hash
+// map (last entry wins, attribute 0 removes), then buildPoints runs on the result --
+// how the reference's tests build the CPU side of an edited scene
+// (tests/cpu_test.zig:829-838, tests/gpu_test.zig:686-700).
+int orc_cpu_build_overlay(uint32_t log2_size, const uint32_t* voxels, uint64_t n, const uint32_t* edits, uint64_t m,
+                          int store_attrs, orc_dag* out) {
+    std::memset(out, 0, sizeof(*out));
+    std::unordered_map<uint64_t, uint32_t> merged;
+    merged.reserve(size_t((n + m) * 1.3));
+    auto key = [](const uint32_t* p) { return uint64_t(p[0]) | (uint64_t(p[1]) << 21) | (uint64_t(p[2]) << 42); };
+    for (uint64_t i = 0; i < n; ++i) merged[key(voxels + 4 * i)] = voxels[4 * i + 3];
+    for (uint64_t i = 0; i < m; ++i) merged[key(edits + 4 * i)] = edits[4 * i + 3];
+    std::vector<uint32_t> pts;
+    pts.reserve(merged.size() * 4);
+    for (const auto& kv : merged) {
+        if (kv.second == 0) continue;
+        pts.push_back(uint32_t(kv.first & 0x1FFFFF));
+        pts.push_back(uint32_t((kv.first >> 21) & 0x1FFFFF));
+        pts.push_back(uint32_t(kv.first >> 42));
+        pts.push_back(kv.second);
+    }
+    return orc_cpu_build_points(log2_size, pts.data(), pts.size() / 4, store_attrs, out);
+}
+
 int orc_cpu_build_dense(uint32_t log2_size, const uint32_t* vox, int store_attrs, orc_dag* out) {  // :292-320
     std::memset(out, 0, sizeof(*out));
     if (log2_size < kMinLog2 || log2_size > kMaxLog2) return -1;

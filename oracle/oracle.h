@@ -75,6 +75,10 @@ typedef struct orc_dag {
 /* buildPoints (src/dag_builder.zig:325-368): points int32/uint32 [n][4], every point
  * inside the volume and attribute != 0, else -1 (InvalidArgument). */
 int orc_cpu_build_points(uint32_t log2_size, const uint32_t* points, uint64_t n, int store_attrs, orc_dag* out);
+/* Edit overlay merged by a host hash map (last wins, attribute 0 removes), then
+ * buildPoints (tests/cpu_test.zig:829-838). voxels [n][4], edits [m][4]. */
+int orc_cpu_build_overlay(uint32_t log2_size, const uint32_t* voxels, uint64_t n, const uint32_t* edits, uint64_t m,
+                          int store_attrs, orc_dag* out);
 /* buildDense (src/dag_builder.zig:292-320): voxels[x + N*(y + N*z)], 0 = empty. */
 int orc_cpu_build_dense(uint32_t log2_size, const uint32_t* voxels, int store_attrs, orc_dag* out);
 /* buildFn (src/dag_builder.zig:373-412) over a dense lookup table (same octree walk). */

@@ -55,6 +55,7 @@ def lib():
         L.orc_built_free.argtypes = [ctypes.POINTER(OrcBuilt)]
         L.orc_cpu_build_points.argtypes = [u32, p, u64, ctypes.c_int, ctypes.POINTER(OrcDag)]
         L.orc_cpu_build_dense.argtypes = [u32, p, ctypes.c_int, ctypes.POINTER(OrcDag)]
+        L.orc_cpu_build_overlay.argtypes = [u32, p, u64, p, u64, ctypes.c_int, ctypes.POINTER(OrcDag)]
         L.orc_cpu_build_fn_dense.argtypes = [u32, p, ctypes.c_int, ctypes.POINTER(OrcDag)]
         L.orc_dag_free.argtypes = [ctypes.POINTER(OrcDag)]
         L.orc_lookup.argtypes = [u32, p, p, p, u32, u32, u32, u32]
@@ -194,6 +195,17 @@ def cpu_build_points(log2_size, points, store_attrs=True) -> Dag:
     pts = np.ascontiguousarray(points, dtype=np.uint32)
     d = OrcDag()
     if lib().orc_cpu_build_points(log2_size, _ptr(pts.reshape(-1)), len(pts), int(store_attrs), ctypes.byref(d)) != 0:
+        raise ValueError("invalid argument")
+    return _take_dag(d)
+
+
+def cpu_build_overlay(log2_size, voxels, edits, store_attrs=True) -> Dag:
+    """Edits merged by a host hash map, then buildPoints (tests/cpu_test.zig:829-838)."""
+    v = np.ascontiguousarray(voxels, dtype=np.uint32)
+    e = np.ascontiguousarray(edits, dtype=np.uint32)
+    d = OrcDag()
+    if lib().orc_cpu_build_overlay(log2_size, _ptr(v.reshape(-1)), len(v), _ptr(e.reshape(-1)), len(e),
+                                   int(store_attrs), ctypes.byref(d)) != 0:
         raise ValueError("invalid argument")
     return _take_dag(d)
 
