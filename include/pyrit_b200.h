@@ -191,6 +191,27 @@ PYRB_API void pyrb_get_tuning(pyrb_tuning* t);
 PYRB_API void pyrb_profile_enable(int on);
 PYRB_API uint32_t pyrb_profile_read(float* ms, char* names, uint32_t name_len, uint32_t cap);
 
+/* A plain build that allocates no device memory (no counterpart in the reference).
+ * For callers that cannot allocate while they build: a render or frame loop that must
+ * not call cudaMalloc (it synchronises the whole device), code running while a stream
+ * is captured into a CUDA graph (allocation calls are illegal there), or engines whose
+ * device memory is fully budgeted up front. All scratch lives in a fixed 64 MiB
+ * device array inside the library (held by every GPU that loads the library until the
+ * process exits); the caller passes the input (device PyrVoxel[n_new]) and every
+ * output buffer (device memory) with its capacity in elements. Limits: log2_size in
+ * [3, 8], n_new <= 2^20; larger requests and too small outputs return
+ * PYRB_ERROR_INVALID_ARGUMENT with the sizes needed. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress), so make one call per device
+ * before any stream capture. All calls share the one array: calls whose work
+ * overlaps on the GPU (other streams, other threads) race and corrupt each other --
+ * serialise them. Output layout and values are identical to pyrb_build with
+ * n_old = 0. Synchronises `stream` once at the end to read the counts. */
+PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32_t rt_log2_req, uint64_t edits,
+                                        uint32_t n_new, uint64_t nodes, uint32_t node_capacity, uint64_t leaves,
+                                        uint32_t leaf_capacity, uint64_t keys, uint64_t attrs,
+                                        uint32_t voxel_capacity, uint64_t prims, uint64_t aabbs,
+                                        uint32_t prim_capacity, pyrb_built* out);
+
 /* Library version (major << 16 | minor). */
 PYRB_API uint32_t pyrb_version(void);
 

@@ -796,3 +796,271 @@ PYRB_API void pyrb_get_tuning(pyrb_tuning* t) {
 PYRB_API uint32_t pyrb_version(void) { return (0u << 16) | 1u; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Build without any device allocation (pyrb_build_noalloc).
+//
+// Some callers cannot allocate device memory while they build: a frame loop that
+// must not call cudaMalloc (it synchronises the device), code that runs while a
+// stream is being captured into a CUDA graph (allocation calls are illegal there),
+// or hosts whose memory is fully budgeted up front. For them all scratch of the
+// build lives in this fixed, file-scope device array; the caller brings input and
+// output buffers. Every GPU that loads the library keeps the array until exit.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kStaticScratchBytes = 64ull << 20;   // 64 MiB per device
+constexpr uint32_t kStaticMaxEntries = 1u << 20;        // input voxels per build
+constexpr uint32_t kStaticMaxLog2 = 8;                  // edge 256
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mu;
+void* g_static_addr[64] = {};
+
+// Device address of the array on the current device. The first call per device
+// resolves it with cudaGetSymbolAddress (the array's name is only a host stand-in).
+pyrb_result static_scratch(void** out) {
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(PYRB_ERROR_CUDA, "device index %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t err = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (err != cudaSuccess || !p)
+            return fail(PYRB_ERROR_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(err));
+        g_static_addr[dev] = p;
+    }
+    *out = g_static_addr[dev];
+    return PYRB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32_t rt_log2_req, uint64_t edits,
+                                        uint32_t n_new, uint64_t nodes, uint32_t node_capacity, uint64_t leaves,
+                                        uint32_t leaf_capacity, uint64_t keys, uint64_t attrs,
+                                        uint32_t voxel_capacity, uint64_t prims, uint64_t aabbs,
+                                        uint32_t prim_capacity, pyrb_built* out) {
+    if (!out) return fail(PYRB_ERROR_INVALID_ARGUMENT, "out is NULL");
+    std::memset(out, 0, sizeof(*out));
+    if (log2_size < 3 || log2_size > kStaticMaxLog2)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "pyrb_build_noalloc: log2_size must lie in [3, %u] (got %u)",
+                    kStaticMaxLog2, log2_size);
+    if (n_new > kStaticMaxEntries)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "pyrb_build_noalloc: %u voxels exceed the fixed limit of %u", n_new,
+                    kStaticMaxEntries);
+    if (n_new && !edits) return fail(PYRB_ERROR_INVALID_ARGUMENT, "edits is NULL");
+    if (!nodes || !leaves || !keys || !attrs || !prims || !aabbs)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "pyrb_build_noalloc: every output buffer is required");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t log2 = log2_size, lb = 3 * log2, K = 1;
+    const uint32_t rt = std::min(std::max(rt_log2_req, 3u), log2);
+    const uint32_t n = n_new, nmax = std::max(n, 1u);
+    const uint32_t rb = 8, tile_keys = 4096, lf = 50;
+
+    BuildDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.mode = kModePlain;
+    d.log2 = log2;
+    d.rt_log2 = rt;
+    d.lb = lb;
+    d.seg_count = K;
+    d.n_new = n;
+    d.n_total = n;
+    d.top = log2 - 1;
+    d.voxels = reinterpret_cast<const uint4*>(edits);
+    const uint32_t sort_bits = lb + 1, passes = (sort_bits + rb - 1) / rb;
+    d.passes = passes;
+    d.radix = 1u << rb;
+    {
+        uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 0;
+        for (uint32_t p = 0; p < passes; ++p) {
+            d.pass_shift[p] = sh;
+            d.pass_bits[p] = base + (p < extra ? 1 : 0);
+            sh += d.pass_bits[p];
+        }
+    }
+    d.tile_keys = tile_keys;
+    d.sort_tiles = std::max((n + tile_keys - 1) / tile_keys, 1u);
+    auto cells = [&](uint32_t edge_log2) -> uint64_t { return uint64_t(1) << (3 * (log2 - edge_log2)); };
+    const uint32_t B = uint32_t(std::max<uint64_t>(std::min<uint64_t>(nmax, cells(2)), 1));
+    uint32_t P[kMaxLevels + 2] = {};
+    uint64_t words = 2;
+    for (uint32_t lv = 2; lv < log2; ++lv) {
+        uint64_t prev = lv == 2 ? B : P[lv - 1];
+        P[lv] = uint32_t(std::max<uint64_t>(std::min<uint64_t>(prev, cells(lv + 1)), 1));
+        words += uint64_t(P[lv]) * kNodeStride;
+    }
+    d.brick_bound = B;
+    d.brick_tiles = std::max((nmax + kBrickTile - 1) / kBrickTile, 1u);
+    d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
+    d.leaf_cap = next_pow2(uint64_t(B) * 100 / lf + 1, 1024);
+    d.node_bound = uint32_t(words);
+    d.prim_bound = P[rt - 1];
+    if (node_capacity < d.node_bound || leaf_capacity < B || voxel_capacity < nmax || prim_capacity < std::max(d.prim_bound, 1u))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT,
+                    "pyrb_build_noalloc: output buffers too small (need nodes %u words, leaves %u, keys/attrs %u, "
+                    "prims %u)", d.node_bound, B, nmax, std::max(d.prim_bound, 1u));
+
+    // scratch layout inside the fixed array: zero region, 0xFF region, the rest
+    Layout zl;
+    const uint64_t o_counters = zl.take(kCtrCount * 4);
+    const uint64_t o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
+    const uint64_t o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
+    const uint64_t o_uniq_status = zl.take(uint64_t(d.sort_tiles) * 8);
+    const uint64_t o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
+    const uint64_t o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
+    const uint64_t o_leaf_table = zl.take(uint64_t(d.leaf_cap) * 16);
+    uint64_t o_table[kMaxLevels + 2], o_bstat[kMaxLevels + 2], o_ostat[kMaxLevels + 2];
+    uint32_t cap[kMaxLevels + 2], btiles[kMaxLevels + 2], otiles[kMaxLevels + 2];
+    for (uint32_t lv = 2; lv < log2; ++lv) {
+        cap[lv] = next_pow2(uint64_t(P[lv]) * 100 / lf + 1, 1024);
+        uint32_t child = lv == 2 ? B : P[lv - 1];
+        btiles[lv] = std::max((child + kNodeTile - 1) / kNodeTile, 1u);
+        otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
+        o_table[lv] = zl.take(uint64_t(cap[lv]) * 16);
+        o_bstat[lv] = zl.take(uint64_t(btiles[lv]) * 8);
+        o_ostat[lv] = zl.take(uint64_t(otiles[lv]) * 8);
+    }
+    const uint64_t zero_bytes = align_up(zl.size, 256);
+    Layout fl;
+    fl.size = zero_bytes;
+    const uint64_t o_chunk_first = fl.take(4), o_roots = fl.take(4), o_prim_start = fl.take(4);
+    const uint64_t ff_bytes = align_up(fl.size, 256) - zero_bytes;
+    Layout ol;
+    ol.size = zero_bytes + ff_bytes;
+    const uint64_t o_seg_entry = ol.take(8), o_seg_tile = ol.take(8);
+    const uint64_t o_k0 = ol.take(uint64_t(nmax) * 4), o_v0 = ol.take(uint64_t(nmax) * 4);
+    const uint64_t o_k1 = ol.take(uint64_t(nmax) * 4), o_v1 = ol.take(uint64_t(nmax) * 4);
+    const uint64_t o_bkey = ol.take(uint64_t(B) * 8), o_bmask = ol.take(uint64_t(B) * 8);
+    const uint64_t o_bfirst = ol.take(uint64_t(B) * 4), o_bslot = ol.take(uint64_t(B) * 4);
+    uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
+    uint64_t o_set[2][7];
+    for (int s = 0; s < 2; ++s) {
+        uint64_t m = std::max(setn[s], 1u);
+        o_set[s][0] = ol.take(m * 8);
+        o_set[s][1] = ol.take(m * 4);
+        o_set[s][2] = ol.take(m * 4);
+        o_set[s][3] = ol.take(m * 4);
+        o_set[s][4] = ol.take(m * 8);
+        o_set[s][5] = ol.take(m * 8);
+        o_set[s][6] = ol.take(m * kNodeStride * 4);
+    }
+    const uint64_t scratch_bytes = align_up(ol.size, 256);
+    if (scratch_bytes > kStaticScratchBytes)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT,
+                    "pyrb_build_noalloc: this build needs %llu bytes of scratch, the fixed array holds %llu",
+                    (unsigned long long)scratch_bytes, (unsigned long long)kStaticScratchBytes);
+
+    void* base = nullptr;
+    pyrb_result r = static_scratch(&base);
+    if (r != PYRB_OK) return r;
+    auto at = [&](uint64_t off) { return static_cast<void*>(static_cast<unsigned char*>(base) + off); };
+    d.counters = static_cast<uint32_t*>(at(o_counters));
+    d.hist = static_cast<uint32_t*>(at(o_hist));
+    d.sort_status = static_cast<uint64_t*>(at(o_sort_status));
+    d.uniq_status = static_cast<uint64_t*>(at(o_uniq_status));
+    d.brick_status = static_cast<uint64_t*>(at(o_brick_status));
+    d.leafown_status = static_cast<uint64_t*>(at(o_leafown_status));
+    d.leaf_table = static_cast<uint4*>(at(o_leaf_table));
+    d.chunk_first = static_cast<uint32_t*>(at(o_chunk_first));
+    d.roots = static_cast<uint32_t*>(at(o_roots));
+    d.prim_start = static_cast<uint32_t*>(at(o_prim_start));
+    d.seg_entry = static_cast<uint32_t*>(at(o_seg_entry));
+    d.seg_tile = static_cast<uint32_t*>(at(o_seg_tile));
+    d.kbuf[0] = static_cast<uint32_t*>(at(o_k0));
+    d.vbuf[0] = static_cast<uint32_t*>(at(o_v0));
+    d.kbuf[1] = static_cast<uint32_t*>(at(o_k1));
+    d.vbuf[1] = static_cast<uint32_t*>(at(o_v1));
+    d.bkey = static_cast<uint64_t*>(at(o_bkey));
+    d.bmask = static_cast<uint64_t*>(at(o_bmask));
+    d.bfirst = static_cast<uint32_t*>(at(o_bfirst));
+    d.bslot = static_cast<uint32_t*>(at(o_bslot));
+    d.ukey = reinterpret_cast<uint64_t*>(keys);
+    d.uval = reinterpret_cast<uint32_t*>(attrs);
+    d.leaves = reinterpret_cast<uint64_t*>(leaves);
+    d.nodes = reinterpret_cast<uint32_t*>(nodes);
+    d.prims = reinterpret_cast<uint8_t*>(prims);
+    d.aabbs = reinterpret_cast<float*>(aabbs);
+
+    std::vector<LevelDesc> levels;
+    for (uint32_t lv = 2; lv < log2; ++lv) {
+        LevelDesc L;
+        std::memset(&L, 0, sizeof(L));
+        L.lv = lv;
+        L.child_bound = lv == 2 ? B : P[lv - 1];
+        L.parent_bound = P[lv];
+        L.build_tiles = btiles[lv];
+        L.own_tiles = otiles[lv];
+        L.need_box = lv + 1 <= rt ? 1u : 0u;
+        L.pcap = cap[lv];
+        L.tile_ctr_build = 12 + 2 * (lv - 2);
+        L.tile_ctr_own = 13 + 2 * (lv - 2);
+        const int ps = (lv - 2) & 1;
+        L.pkey = static_cast<uint64_t*>(at(o_set[ps][0]));
+        L.pcnt = static_cast<uint32_t*>(at(o_set[ps][1]));
+        L.pfirst = static_cast<uint32_t*>(at(o_set[ps][2]));
+        L.pslot = static_cast<uint32_t*>(at(o_set[ps][3]));
+        L.plo = static_cast<uint64_t*>(at(o_set[ps][4]));
+        L.phi = static_cast<uint64_t*>(at(o_set[ps][5]));
+        L.pwords = static_cast<uint32_t*>(at(o_set[ps][6]));
+        L.ptable = static_cast<uint4*>(at(o_table[lv]));
+        L.build_status = static_cast<uint64_t*>(at(o_bstat[lv]));
+        L.own_status = static_cast<uint64_t*>(at(o_ostat[lv]));
+        if (lv == 2) {
+            L.ckey = d.bkey;
+            L.cmask = d.bmask;
+            L.cfirst = d.bfirst;
+            L.cslot = d.bslot;
+            L.ctable = d.leaf_table;
+        } else {
+            const LevelDesc& C = levels.back();
+            L.ckey = C.pkey;
+            L.ccnt = C.pcnt;
+            L.cfirst = C.pfirst;
+            L.cslot = C.pslot;
+            L.clo = C.plo;
+            L.chi = C.phi;
+            L.ctable = C.ptable;
+        }
+        levels.push_back(L);
+    }
+
+    // the array keeps the previous call's contents: clear everything that must start
+    // at zero (counters, histograms, look-back status, dedup tables) and the 0xFF part
+    CU(cudaMemsetAsync(at(0), 0, zero_bytes, st));
+    CU(cudaMemsetAsync(at(zero_bytes), 0xFF, ff_bytes, st));
+    Prof prof(st);
+    k_plan<<<1, 1024, 0, st>>>(d);
+    CU(cudaGetLastError());
+    CU((launch_sort<8, 16>(d, st, prof)));
+    k_brick<<<d.brick_tiles, kBlock, 0, st>>>(d);
+    k_leaf_own<<<d.leafown_tiles, kBlock, 0, st>>>(d);
+    for (const LevelDesc& L : levels) {
+        k_node_build<<<L.build_tiles, kBlock, 0, st>>>(d, L);
+        k_node_own<<<L.own_tiles, kBlock, 0, st>>>(d, L);
+        if (L.lv + 1 == rt) k_prims<<<std::max((L.parent_bound + kBlock - 1) / kBlock, 1u), kBlock, 0, st>>>(d, L);
+    }
+    k_finalize<<<1, kBlock, 0, st>>>(d, levels.back());
+    CU(cudaGetLastError());
+    uint32_t ctr[kCtrCount];
+    CU(cudaMemcpyAsync(ctr, d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (ctr[kCtrError]) return device_error(ctr[kCtrError]);
+    out->log2_size = log2;
+    out->rt_log2 = rt;
+    out->nodes = nodes;
+    out->leaves = leaves;
+    out->keys = keys;
+    out->attrs = attrs;
+    out->prims = prims;
+    out->aabbs = aabbs;
+    fill_counts(ctr, out);
+    return PYRB_OK;
+}
+
+}  // extern "C"

@@ -86,6 +86,8 @@ SIGNATURES = {
     "pyrb_set_tuning": (ctypes.c_int32, [ctypes.POINTER(Tuning)]),
     "pyrb_get_tuning": (None, [ctypes.POINTER(Tuning)]),
     "pyrb_version": (ctypes.c_uint32, []),
+    "pyrb_build_noalloc": (ctypes.c_int32, [_p, _u32, _u32, _u64, _u32, _u64, _u32, _u64, _u32, _u64, _u64, _u32,
+                                            _u64, _u64, _u32, ctypes.POINTER(BuiltC)]),
 }
 
 _lib = None
