@@ -171,7 +171,7 @@ PYRB_API void pyrb_last_stats(pyrb_stats* out);
 PYRB_API const char* pyrb_error_message(void);
 PYRB_API const char* pyrb_result_string(pyrb_result r);
 
-/* Tuning of the sort and the dedup tables (digit width 4, 8 or 11 bits; keys per
+/* Tuning of the sort and the dedup tables (digit width 4, 8, 9, 10 or 11 bits; keys per
  * sort tile 1024, 2048 or 4096; hash load factor in percent, 25..90). Applies to
  * builds started afterwards on any thread. Returns PYRB_ERROR_INVALID_ARGUMENT for
  * unsupported values. */

@@ -189,6 +189,66 @@ struct Prof {
     }
 };
 
+uint32_t leaf_insert_grid(const BuildDesc& d) {
+    return std::max(std::min((d.brick_bound + kBlock - 1) / kBlock, 148u * 8u), 1u);
+}
+
+// First level built by the single-CTA tail kernel (children bound <= kTailMaxChildren
+// from there on); log2 means no tail (the top level is too wide, e.g. many chunks).
+uint32_t tail_level(uint32_t log2, uint32_t B, const uint32_t* P) {
+    for (uint32_t lv = 2; lv < log2; ++lv) {
+        const uint32_t child = lv == 2 ? B : P[lv - 1];
+        if (child <= kTailMaxChildren) return lv;
+    }
+    return log2;
+}
+
+// Node levels, prims and the final counts. Levels below lv0 run as multi-CTA
+// kernels; the rest (and the finalisation) in k_tail.
+uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels, uint32_t lv0, const TailDesc& T,
+                       cudaStream_t st, Prof& prof) {
+    uint32_t launches = 0;
+    for (const LevelDesc& L : levels) {
+        if (L.lv >= lv0) break;
+        k_node_build<<<L.build_tiles, kBlock, node_build_smem_bytes(), st>>>(d, L);
+        prof.mark("node_build", L.lv);
+        k_node_own<<<L.own_tiles, kBlock, 0, st>>>(d, L);
+        prof.mark("node_own", L.lv);
+        launches += 2;
+        if (L.lv + 1 == d.rt_log2) {
+            k_prims<<<std::max((L.parent_bound + kBlock - 1) / kBlock, 1u), kBlock, 0, st>>>(d, L);
+            prof.mark("prims", L.lv);
+            ++launches;
+        }
+    }
+    if (lv0 < d.log2) {
+        static std::once_flag once;
+        std::call_once(once, [] {
+            cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tail_smem_bytes()));
+        });
+        k_tail<<<1, kTailThreads, tail_smem_bytes(), st>>>(d, T);
+        prof.mark("tail", lv0);
+    } else {
+        k_finalize<<<1, kBlock, 0, st>>>(d, levels.back());
+        prof.mark("finalize");
+    }
+    return launches + 1;
+}
+
+TailDesc make_tail(uint32_t lv0, const uint32_t* P, const std::vector<LevelDesc>& levels, const uint4* leaf_table) {
+    TailDesc T;
+    std::memset(&T, 0, sizeof(T));
+    T.lv0 = lv0;
+    for (int i = 0; i < kMaxLevels + 2; ++i) T.parent_bound[i] = P[i];
+    for (const LevelDesc& L : levels) {
+        const int ps = (L.lv - 2) & 1;
+        T.set[ps] = RecordSet{L.pkey, L.pcnt, L.pfirst, L.pslot, L.plo, L.phi, L.pwords};
+        if (L.lv + 1 == lv0) T.ctable0 = L.ptable;
+    }
+    if (lv0 == 2) T.ctable0 = leaf_table;
+    return T;
+}
+
 pyrb_result device_error(uint32_t bits) {
     return fail(PYRB_ERROR_CUDA, "device-side build error 0x%x (%s%s%s)", bits,
                 (bits & kErrSpin) ? "look-back wait limit " : "", (bits & kErrTable) ? "dedup table full " : "",
@@ -227,6 +287,7 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
     std::call_once(once, [&] {
         cudaFuncSetAttribute(k_encode_hist<RB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
         cudaFuncSetAttribute(k_sort_pass<RB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
+        cudaFuncSetAttribute(k_sort_pass<RB, IT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     });
     k_encode_hist<RB, IT><<<d.sort_tiles, kBlock, hist_smem, st>>>(d);
     prof.mark("encode_hist");
@@ -240,6 +301,12 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
 }
 
 cudaError_t launch_sort_any(uint32_t rb, uint32_t it, const BuildDesc& d, cudaStream_t st, Prof& prof) {
+    if (rb == 9 && it == 16) return launch_sort<9, 16>(d, st, prof);
+    if (rb == 9 && it == 8) return launch_sort<9, 8>(d, st, prof);
+    if (rb == 9 && it == 4) return launch_sort<9, 4>(d, st, prof);
+    if (rb == 10 && it == 16) return launch_sort<10, 16>(d, st, prof);
+    if (rb == 10 && it == 8) return launch_sort<10, 8>(d, st, prof);
+    if (rb == 10 && it == 4) return launch_sort<10, 4>(d, st, prof);
     if (rb == 8 && it == 16) return launch_sort<8, 16>(d, st, prof);
     if (rb == 8 && it == 8) return launch_sort<8, 8>(d, st, prof);
     if (rb == 8 && it == 4) return launch_sort<8, 4>(d, st, prof);
@@ -350,7 +417,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.brick_bound = B;
     d.brick_tiles = std::max((nmax + kBrickTile - 1) / kBrickTile, 1u);
     d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
-    d.leaf_cap = next_pow2(uint64_t(B) * 100 / lf + 1, 1024);
+    d.leaf_cap = next_pow2((uint64_t(B) * 100 + lf - 1) / lf, 1024);
     d.node_bound = uint32_t(words);
     d.prim_bound = P[rt - 1];
 
@@ -366,9 +433,9 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     uint64_t o_table[kMaxLevels + 2], o_bstat[kMaxLevels + 2], o_ostat[kMaxLevels + 2];
     uint32_t cap[kMaxLevels + 2], btiles[kMaxLevels + 2], otiles[kMaxLevels + 2];
     for (uint32_t lv = 2; lv < log2; ++lv) {
-        cap[lv] = next_pow2(uint64_t(P[lv]) * 100 / lf + 1, 1024);
+        cap[lv] = next_pow2((uint64_t(P[lv]) * 100 + lf - 1) / lf, 1024);
         uint32_t child = lv == 2 ? B : P[lv - 1];
-        btiles[lv] = std::max((child + kNodeTile - 1) / kNodeTile, 1u);
+        btiles[lv] = std::max((child + kNodeBuildTile - 1) / kNodeBuildTile, 1u);
         otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
         o_table[lv] = zl.take(uint64_t(cap[lv]) * 16);
         o_bstat[lv] = zl.take(uint64_t(btiles[lv]) * 8);
@@ -518,24 +585,13 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     launches += 2 + passes;
     k_brick<<<d.brick_tiles, kBlock, 0, st>>>(d);
     prof.mark("brick");
+    k_leaf_insert<<<leaf_insert_grid(d), kBlock, 0, st>>>(d);
+    prof.mark("leaf_insert");
     k_leaf_own<<<d.leafown_tiles, kBlock, 0, st>>>(d);
     prof.mark("leaf_own");
-    launches += 2;
-    for (const LevelDesc& L : levels) {
-        k_node_build<<<L.build_tiles, kBlock, 0, st>>>(d, L);
-        prof.mark("node_build", L.lv);
-        k_node_own<<<L.own_tiles, kBlock, 0, st>>>(d, L);
-        prof.mark("node_own", L.lv);
-        launches += 2;
-        if (L.lv + 1 == rt) {
-            k_prims<<<std::max((L.parent_bound + kBlock - 1) / kBlock, 1u), kBlock, 0, st>>>(d, L);
-            prof.mark("prims", L.lv);
-            ++launches;
-        }
-    }
-    k_finalize<<<1, kBlock, 0, st>>>(d, levels.back());
-    prof.mark("finalize");
-    ++launches;
+    launches += 3;
+    const uint32_t lv0 = tail_level(log2, B, P);
+    launches += launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
     CUL(cudaGetLastError());
 
     const uint64_t out_bytes = uint64_t(d.node_bound) * 4 + uint64_t(B) * 8 + uint64_t(nmax) * 12 +
@@ -773,8 +829,8 @@ PYRB_API const char* pyrb_result_string(pyrb_result r) {
 
 PYRB_API pyrb_result pyrb_set_tuning(const pyrb_tuning* t) {
     if (!t) return fail(PYRB_ERROR_INVALID_ARGUMENT, "tuning is NULL");
-    if (t->radix_bits != 4 && t->radix_bits != 8 && t->radix_bits != 11)
-        return fail(PYRB_ERROR_INVALID_ARGUMENT, "radix_bits must be 4, 8 or 11");
+    if (t->radix_bits != 4 && (t->radix_bits < 8 || t->radix_bits > 11))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "radix_bits must be 4, 8, 9, 10 or 11");
     if (t->tile_keys != 1024 && t->tile_keys != 2048 && t->tile_keys != 4096)
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "tile_keys must be 1024, 2048 or 4096");
     if (t->load_factor_pct < 25 || t->load_factor_pct > 90)
@@ -898,7 +954,7 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     d.brick_bound = B;
     d.brick_tiles = std::max((nmax + kBrickTile - 1) / kBrickTile, 1u);
     d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
-    d.leaf_cap = next_pow2(uint64_t(B) * 100 / lf + 1, 1024);
+    d.leaf_cap = next_pow2((uint64_t(B) * 100 + lf - 1) / lf, 1024);
     d.node_bound = uint32_t(words);
     d.prim_bound = P[rt - 1];
     if (node_capacity < d.node_bound || leaf_capacity < B || voxel_capacity < nmax || prim_capacity < std::max(d.prim_bound, 1u))
@@ -918,9 +974,9 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     uint64_t o_table[kMaxLevels + 2], o_bstat[kMaxLevels + 2], o_ostat[kMaxLevels + 2];
     uint32_t cap[kMaxLevels + 2], btiles[kMaxLevels + 2], otiles[kMaxLevels + 2];
     for (uint32_t lv = 2; lv < log2; ++lv) {
-        cap[lv] = next_pow2(uint64_t(P[lv]) * 100 / lf + 1, 1024);
+        cap[lv] = next_pow2((uint64_t(P[lv]) * 100 + lf - 1) / lf, 1024);
         uint32_t child = lv == 2 ? B : P[lv - 1];
-        btiles[lv] = std::max((child + kNodeTile - 1) / kNodeTile, 1u);
+        btiles[lv] = std::max((child + kNodeBuildTile - 1) / kNodeBuildTile, 1u);
         otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
         o_table[lv] = zl.take(uint64_t(cap[lv]) * 16);
         o_bstat[lv] = zl.take(uint64_t(btiles[lv]) * 8);
@@ -1039,13 +1095,10 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     CU(cudaGetLastError());
     CU((launch_sort<8, 16>(d, st, prof)));
     k_brick<<<d.brick_tiles, kBlock, 0, st>>>(d);
+    k_leaf_insert<<<leaf_insert_grid(d), kBlock, 0, st>>>(d);
     k_leaf_own<<<d.leafown_tiles, kBlock, 0, st>>>(d);
-    for (const LevelDesc& L : levels) {
-        k_node_build<<<L.build_tiles, kBlock, 0, st>>>(d, L);
-        k_node_own<<<L.own_tiles, kBlock, 0, st>>>(d, L);
-        if (L.lv + 1 == rt) k_prims<<<std::max((L.parent_bound + kBlock - 1) / kBlock, 1u), kBlock, 0, st>>>(d, L);
-    }
-    k_finalize<<<1, kBlock, 0, st>>>(d, levels.back());
+    const uint32_t lv0 = tail_level(log2, B, P);
+    launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
     CU(cudaGetLastError());
     uint32_t ctr[kCtrCount];
     CU(cudaMemcpyAsync(ctr, d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));

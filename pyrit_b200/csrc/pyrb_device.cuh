@@ -94,6 +94,20 @@ __device__ __forceinline__ uint32_t ld_relaxed32(const uint32_t* p) {
     return v;
 }
 
+__device__ __forceinline__ uint32_t ld_acquire32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// Compare-and-swap with acquire-release ordering at device scope: the caller's
+// earlier stores are visible to whoever observes the swapped value, and the value
+// returned on failure comes with the other writer's earlier stores.
+__device__ __forceinline__ uint32_t cas_acq_rel32(uint32_t* p, uint32_t cmp, uint32_t val) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.cas.b32 %0, [%1], %2, %3;" : "=r"(old) : "l"(p), "r"(cmp), "r"(val) : "memory");
+    return old;
+}
+
 // Look-back of one value by one thread (used per digit by the sort). Tiles
 // [first, tile) precede `tile`; status[first - 1] is never read. Returns the
 // exclusive prefix and publishes the inclusive one. A predecessor that never

@@ -144,4 +144,28 @@ struct LevelDesc {
 
 constexpr uint32_t kNodeStride = 10;
 
+// The upper levels, once a level has at most kTailMaxChildren children, are built by
+// one CTA (k_tail) that keeps each level's dedup table in shared memory.
+constexpr uint32_t kTailThreads = 1024;
+constexpr uint32_t kTailMaxChildren = 4096;
+constexpr uint32_t kTailSlots = 8192;
+
+// One record set of parents (levels alternate between two sets).
+struct RecordSet {
+    uint64_t* key;
+    uint32_t* cnt;
+    uint32_t* first;
+    uint32_t* slot;    // k_tail: node word offset of the parent (its reference)
+    uint64_t* lo;
+    uint64_t* hi;
+    uint32_t* words;   // [bound][kNodeStride]
+};
+
+struct TailDesc {
+    uint32_t lv0;                    // first level built by the tail (children <= kTailMaxChildren)
+    uint32_t parent_bound[kMaxLevels + 2];
+    RecordSet set[2];                // parents of level lv live in set[(lv - 2) & 1]
+    const uint4* ctable0;            // references of lv0's children: leaf table (lv0 == 2) or level lv0-1 table
+};
+
 }  // namespace pyrb

@@ -447,8 +447,7 @@ __device__ __forceinline__ uint32_t leaf_insert(uint4* table, uint32_t cap, uint
 // ---------------------------------------------------------------------------
 // Bricks: 4^3 runs of the sorted unique keys -> (brick key, mask, first voxel).
 // A warp owns 32*8 consecutive keys; a run is emitted by the warp that holds its
-// first key (reading at most 63 keys past its chunk). The emitting lanes insert
-// their masks into the leaf table, collapsing equal masks of a warp first.
+// first key (reading at most 63 keys past its chunk).
 // ---------------------------------------------------------------------------
 constexpr int kBrickIT = 8;
 constexpr int kBrickTile = kBlock * kBrickIT;
@@ -541,24 +540,33 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
         c_own = __shfl_sync(kFull, own ? 1 : 0, 31) != 0;
         c_first = __shfl_sync(kFull, first, 31);
         hcount += __popc(hbj);
-        unsigned em = __ballot_sync(kFull, emit);
         if (emit) {
-            unsigned same = __match_any_sync(em, v);
-            unsigned leader = __ffs(same) - 1;
-            uint32_t slot = 0;
-            if (lane == leader) {
-                if (idx < d.brick_bound) slot = leaf_insert(d.leaf_table, d.leaf_cap, v, idx, d.counters + kCtrError);
-            }
-            slot = __shfl_sync(em, slot, leader);
             if (idx < d.brick_bound) {
                 d.bkey[idx] = bk;
                 d.bmask[idx] = v;
                 d.bfirst[idx] = first;
-                d.bslot[idx] = slot;
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);
             }
         }
+    }
+}
+
+// Leaf dedup insert, one brick per thread. Equal masks of a warp are collapsed with
+// match_any first: only the lowest brick of each group touches the table.
+__global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
+    const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * kBlock; base < B; base += gridDim.x * kBlock) {
+        const uint32_t b = base + threadIdx.x;
+        const bool valid = b < B;
+        const uint64_t m = valid ? d.bmask[b] : 0;  // masks are never 0
+        const unsigned same = __match_any_sync(kFull, m);
+        const unsigned leader = __ffs(same) - 1;
+        uint32_t slot = 0;
+        if (valid && lane == leader) slot = leaf_insert(d.leaf_table, d.leaf_cap, m, b, d.counters + kCtrError);
+        slot = __shfl_sync(kFull, slot, leader);
+        if (valid) d.bslot[b] = slot;
     }
 }
 
@@ -620,36 +628,47 @@ __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
 // words [mask, saturating count, refs...] (gbuild.zig:484-520), inserted into
 // the level's table (equal words -> same slot, owner = minimum parent index).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t hash_words(const uint32_t* w, uint32_t len) {
-    uint64_t h = len;
-    for (uint32_t k = 0; k < len; ++k) h = mix64(h ^ w[k]);
+// Node words are [mask, count, ref_0 .. ref_{n-1}]; the hash only places table
+// slots (equality is decided by comparing all words).
+__device__ __forceinline__ uint64_t node_hash(uint32_t mask, uint32_t count, const uint32_t* refs, uint32_t n) {
+    uint64_t h = mix64(mix64(uint64_t(n + 2) ^ mask) ^ count);
+    for (uint32_t k = 0; k < n; ++k) h = mix64(h ^ refs[k]);
     return h;
 }
 
+// Insert parent `par` (words already stored and fenced) into the level table.
+// refs point to shared memory. Returns the slot; the minimum index owns it.
 __device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, const uint32_t* all_words, uint32_t par,
-                                                const uint32_t* w, uint32_t len, uint32_t* err) {
-    uint32_t h = uint32_t(hash_words(w, len)) & (cap - 1);
+                                                uint32_t mask, uint32_t count, const uint32_t* refs, uint32_t n,
+                                                uint32_t* err) {
+    uint32_t h = uint32_t(node_hash(mask, count, refs, n)) & (cap - 1);
     for (uint32_t probe = 0; probe < cap; ++probe) {
         uint32_t* kp = &table[h].x;
-        uint32_t cur = ld_relaxed32(kp);
+        uint32_t cur = ld_acquire32(kp);
         if (cur == 0) {
-            cur = atomicCAS(kp, 0u, par + 1);
+            // release: our words (stored before this call) are visible with the key
+            cur = cas_acq_rel32(kp, 0u, par + 1);
             if (cur == 0) {
                 claim_owner(table + h, par);
                 return h;
             }
         }
-        // compare with the resident node (its words were made visible before its CAS)
-        __threadfence();
+        // acquired above: the resident's words are visible
         const uint32_t* ow = all_words + uint64_t(cur - 1) * kNodeStride;
-        uint32_t omask = __ldcg(ow);
-        if (2u + __popc(omask & 0xFF) == len) {
-            bool same = omask == w[0];
-            for (uint32_t k = 1; k < len && same; ++k) same = __ldcg(ow + k) == w[k];
-            if (same) {
-                claim_owner(table + h, par);
-                return h;
-            }
+        uint32_t o[kNodeStride];
+#pragma unroll
+        for (int k = 0; k < int(kNodeStride); k += 2) {
+            uint2 v = __ldcg(reinterpret_cast<const uint2*>(ow + k));
+            o[k] = v.x;
+            o[k + 1] = v.y;
+        }
+        bool same = o[0] == mask && o[1] == count;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (uint32_t(k) < n) same = same && o[2 + k] == refs[k];
+        if (same) {
+            claim_owner(table + h, par);
+            return h;
         }
         h = (h + 1) & (cap - 1);
     }
@@ -657,32 +676,70 @@ __device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, cons
     return 0;
 }
 
+// Tile of the node build: kNodeBuildTile children staged in shared memory (plus
+// a halo of up to 7 children of the tile's last parent), heads found with warp
+// ballots, positions by a look-back scan, then every thread builds parents from
+// shared memory.
 constexpr int kNodeIT = 8;
-constexpr int kNodeTile = kBlock * kNodeIT;
+constexpr int kNodeTile = kBlock * kNodeIT;     // tile of the node-owner kernel
+constexpr int kNBIT = 4;
+constexpr int kNodeBuildTile = kBlock * kNBIT;  // children per node-build tile
+constexpr int kNodeHalo = 8;
+constexpr size_t node_build_smem_bytes() {
+    return size_t(kNodeBuildTile + kNodeHalo) * (8 + 8 + 8 + 4 + 4 + 4) + size_t(kNodeBuildTile) * 4 + 64;
+}
 
 __global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L) {
+    extern __shared__ uint64_t smem64[];
+    constexpr int N = kNodeBuildTile + kNodeHalo;
+    uint64_t* skey = smem64;
+    uint64_t* slo = skey + N;
+    uint64_t* shi = slo + N;
+    uint32_t* sref = reinterpret_cast<uint32_t*>(shi + N);
+    uint32_t* scnt = sref + N;
+    uint32_t* sfirst = scnt + N;
+    uint32_t* shead = sfirst + N;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
+    __shared__ uint64_t s_prev;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = dyn_tile(d.counters, L.tile_ctr_build, &s_tile);
     const uint32_t C = L.lv == 2 ? min(d.counters[kCtrBricks], d.brick_bound)
                                  : min(d.counters[kCtrParents + L.lv - 1], L.child_bound);
-    const uint32_t ntiles = (C + kNodeTile - 1) / kNodeTile;
+    const uint32_t ntiles = (C + kNodeBuildTile - 1) / kNodeBuildTile;
     if (tile >= ntiles) return;
-    const uint32_t wstart = tile * kNodeTile + warp * 32 * kNodeIT;
-    const uint64_t NONE = ~0ull;
-    unsigned hb[kNodeIT];
+    const uint32_t t0 = tile * kNodeBuildTile;
+    const uint32_t own_n = min(uint32_t(kNodeBuildTile), C - t0);
+    const uint32_t tn = min(uint32_t(N), C - t0);
+    // stage the children: independent coalesced loads, one gather per child for its reference
+    for (uint32_t i = threadIdx.x; i < tn; i += kBlock) {
+        const uint32_t c = t0 + i;
+        skey[i] = L.ckey[c];
+        sfirst[i] = L.cfirst[c];
+        sref[i] = __ldcg(&L.ctable[L.cslot[c]].w);
+        if (L.lv == 2) {
+            const uint64_t m = L.cmask[c];
+            scnt[i] = __popcll(m);
+            if (L.need_box) brick_box(m, slo[i], shi[i]);
+        } else {
+            scnt[i] = L.ccnt[c];
+            if (L.need_box) { slo[i] = L.clo[c]; shi[i] = L.chi[c]; }
+        }
+    }
+    if (threadIdx.x == 0) s_prev = t0 > 0 ? L.ckey[t0 - 1] : ~0ull;
+    __syncthreads();
+    // heads of this tile's own children (warp chunks of 32 * kNBIT)
+    unsigned hb[kNBIT];
     uint32_t wc = 0;
-    uint64_t prev = (wstart > 0 && wstart - 1 < C) ? L.ckey[wstart - 1] : NONE;
 #pragma unroll
-    for (int j = 0; j < kNodeIT; ++j) {
-        uint32_t e = wstart + j * 32 + lane;
-        uint64_t k = e < C ? L.ckey[e] : NONE;
-        uint64_t pk = __shfl_up_sync(kFull, k, 1);
-        if (lane == 0) pk = prev;
-        prev = __shfl_sync(kFull, k, 31);
-        bool head = e < C && (e == 0 || (k >> 3) != (pk >> 3));
+    for (int j = 0; j < kNBIT; ++j) {
+        const uint32_t i = warp * 32 * kNBIT + j * 32 + lane;
+        bool head = false;
+        if (i < own_n) {
+            const uint64_t pk = i == 0 ? s_prev : skey[i - 1];
+            head = (t0 + i == 0) || (skey[i] >> 3) != (pk >> 3);
+        }
         hb[j] = __ballot_sync(kFull, head);
         wc += __popc(hb[j]);
     }
@@ -694,61 +751,55 @@ __global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L)
         uint64_t ex = lookback_warp(L.build_status, tile, 0, total, d.counters + kCtrError);
         if (lane == 0) s_base = ex;
     }
+    uint32_t run = wexcl;
+#pragma unroll
+    for (int j = 0; j < kNBIT; ++j) {
+        const uint32_t i = warp * 32 * kNBIT + j * 32 + lane;
+        if ((hb[j] >> lane) & 1) shead[run + __popc(hb[j] & lanemask_lt())] = i;
+        run += __popc(hb[j]);
+    }
     __syncthreads();
     if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrParents + L.lv] = uint32_t(s_base + total);
-    uint32_t run = uint32_t(s_base) + wexcl;
+    const uint32_t base = uint32_t(s_base);
     const uint32_t child_size = 1u << L.lv;
-#pragma unroll 1
-    for (int j = 0; j < kNodeIT; ++j) {
-        uint32_t e = wstart + j * 32 + lane;
-        if ((hb[j] >> lane) & 1) {
-            uint32_t par = run + __popc(hb[j] & lanemask_lt());
-            uint64_t pkey = L.ckey[e] >> 3;
-            uint32_t w[kNodeStride];
-            uint32_t mask = 0, count = 0, n = 0;
-            uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
-            for (uint32_t c = e; c < C && n < 8; ++c) {
-                uint64_t ck = L.ckey[c];
-                if ((ck >> 3) != pkey) break;
-                uint32_t idx = uint32_t(ck & 7);
-                mask |= 1u << idx;
-                w[2 + n] = __ldcg(&L.ctable[L.cslot[c]].w);
-                ++n;
-                uint64_t clo, chi;
-                if (L.lv == 2) {
-                    uint64_t m = L.cmask[c];
-                    count = sat_add(count, __popcll(m));
-                    if (L.need_box) brick_box(m, clo, chi);
-                } else {
-                    count = sat_add(count, L.ccnt[c]);
-                    if (L.need_box) { clo = L.clo[c]; chi = L.chi[c]; }
-                }
-                if (L.need_box) {
-                    uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size, oz = (idx >> 2) * child_size;
-                    lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
-                    lo[1] = min(lo[1], cell_y(clo) + oy); hi[1] = max(hi[1], cell_y(chi) + oy);
-                    lo[2] = min(lo[2], cell_z(clo) + oz); hi[2] = max(hi[2], cell_z(chi) + oz);
-                }
+    for (uint32_t h = threadIdx.x; h < total; h += kBlock) {
+        const uint32_t i = shead[h];
+        const uint32_t par = base + h;
+        const uint64_t pkey = skey[i] >> 3;
+        uint32_t mask = 0, count = 0, n = 0;
+        uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
+        for (uint32_t j = i; j < tn && n < 8; ++j) {
+            const uint64_t ck = skey[j];
+            if ((ck >> 3) != pkey) break;
+            const uint32_t idx = uint32_t(ck & 7);
+            mask |= 1u << idx;
+            count = sat_add(count, scnt[j]);
+            if (L.need_box) {
+                const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
+                               oz = (idx >> 2) * child_size;
+                const uint64_t clo = slo[j], chi = shi[j];
+                lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
+                lo[1] = min(lo[1], cell_y(clo) + oy); hi[1] = max(hi[1], cell_y(chi) + oy);
+                lo[2] = min(lo[2], cell_z(clo) + oz); hi[2] = max(hi[2], cell_z(chi) + oz);
             }
-            w[0] = mask;
-            w[1] = count;
-            if (par < L.parent_bound) {
-                uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
-                for (uint32_t k = 0; k < 2 + n; ++k) pw[k] = w[k];
-                L.pkey[par] = pkey;
-                L.pcnt[par] = count;
-                L.pfirst[par] = L.cfirst[e];
-                if (L.need_box) {
-                    L.plo[par] = pack_cell(lo[0], lo[1], lo[2]);
-                    L.phi[par] = pack_cell(hi[0], hi[1], hi[2]);
-                }
-                __threadfence();
-                L.pslot[par] = node_insert(L.ptable, L.pcap, L.pwords, par, w, 2 + n, d.counters + kCtrError);
-            } else {
-                atomicOr(d.counters + kCtrError, kErrBound);
-            }
+            ++n;
         }
-        run += __popc(hb[j]);
+        if (par >= L.parent_bound) {
+            atomicOr(d.counters + kCtrError, kErrBound);
+            continue;
+        }
+        uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
+        pw[0] = mask;
+        pw[1] = count;
+        for (uint32_t k = 0; k < n; ++k) pw[2 + k] = sref[i + k];
+        L.pkey[par] = pkey;
+        L.pcnt[par] = count;
+        L.pfirst[par] = sfirst[i];
+        if (L.need_box) {
+            L.plo[par] = pack_cell(lo[0], lo[1], lo[2]);
+            L.phi[par] = pack_cell(hi[0], hi[1], hi[2]);
+        }
+        L.pslot[par] = node_insert(L.ptable, L.pcap, L.pwords, par, mask, count, sref + i, n, d.counters + kCtrError);
     }
 }
 
@@ -802,9 +853,18 @@ __global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
         uint32_t off = run + x - len[j];
         if (len[j]) {
             uint32_t dst = cursor + off;
-            const uint32_t* src = L.pwords + uint64_t(i) * kNodeStride;
+            const uint2* src = reinterpret_cast<const uint2*>(L.pwords + uint64_t(i) * kNodeStride);
+            uint32_t w[kNodeStride];
+#pragma unroll
+            for (int k = 0; k < int(kNodeStride) / 2; ++k) {
+                uint2 v = __ldg(src + k);
+                w[2 * k] = v.x;
+                w[2 * k + 1] = v.y;
+            }
             if (uint64_t(dst) + len[j] <= d.node_bound) {
-                for (uint32_t k = 0; k < len[j]; ++k) d.nodes[dst + k] = src[k];
+#pragma unroll
+                for (int k = 0; k < int(kNodeStride); ++k)
+                    if (uint32_t(k) < len[j]) d.nodes[dst + k] = w[k];
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);
             }
@@ -860,6 +920,256 @@ __global__ void __launch_bounds__(kBlock) k_prims(BuildDesc d, LevelDesc L) {
         if (d.chunked && (i == 0 || (L.pkey[i - 1] >> local_shift) != chunk)) d.prim_start[chunk] = i;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) d.counters[kCtrPrims] = P;
+}
+
+// ---------------------------------------------------------------------------
+// Upper levels in one CTA. Each level: stage the children in shared memory, find
+// heads (block scan), build the parents' words into global memory, dedup them in a
+// shared-memory table (owner = minimum parent index), give the owners word offsets
+// (block scan of their lengths), write their words, and turn every parent's slot
+// into its node offset, which the next level uses as the child reference. Prims
+// (level rt_log2 - 1), roots and the final counts are written here as well.
+// Same output as k_node_build/k_node_own/k_prims/k_finalize per level.
+// ---------------------------------------------------------------------------
+constexpr size_t tail_smem_bytes() {
+    return size_t(kTailMaxChildren) * (8 + 4 + 4) + size_t(kTailSlots) * (4 + 4 + 4) + size_t(kTailMaxChildren) * (4 + 4) +
+           64 * 8;
+}
+
+__device__ __forceinline__ uint32_t tail_scan(uint32_t v, uint32_t* sm, uint32_t* total) {
+    // exclusive scan over kTailThreads threads (32 warps)
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= unsigned(o)) x += y;
+    }
+    if (lane == 31) sm[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = sm[lane], s = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(kFull, s, o);
+            if (lane >= unsigned(o)) s += y;
+        }
+        sm[32 + lane] = s - w;
+        if (lane == 31) sm[64] = s;
+    }
+    __syncthreads();
+    uint32_t r = sm[32 + warp] + x - v;
+    *total = sm[64];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) {
+    extern __shared__ uint64_t tsm64[];
+    uint64_t* skey = tsm64;                                            // children keys
+    uint32_t* sref = reinterpret_cast<uint32_t*>(skey + kTailMaxChildren);
+    uint32_t* scnt = sref + kTailMaxChildren;
+    uint32_t* tkey = scnt + kTailMaxChildren;                          // table: parent index + 1
+    uint32_t* towner = tkey + kTailSlots;                              // table: minimum parent index
+    uint32_t* tval = towner + kTailSlots;                              // table: node offset
+    uint32_t* pslot = tval + kTailSlots;                               // parent -> slot
+    uint32_t* plen = pslot + kTailMaxChildren;                         // parent -> words (owners) / 0
+    uint32_t* scan = plen + kTailMaxChildren;                          // 65 words
+    __shared__ uint32_t s_cursor, s_children;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lv0 = T.lv0;
+    if (tid == 0) {
+        s_cursor = d.counters[kCtrCursor + lv0];
+        s_children = lv0 == 2 ? min(d.counters[kCtrBricks], d.brick_bound)
+                              : min(d.counters[kCtrParents + lv0 - 1], T.parent_bound[lv0 - 1]);
+    }
+    for (uint32_t i = tid; i < kTailSlots; i += kTailThreads) { tkey[i] = 0; towner[i] = 0xFFFFFFFFu; }
+    __syncthreads();
+    const uint32_t local_shift = 3 * (d.log2 - d.rt_log2);
+    for (uint32_t lv = lv0; lv < d.log2; ++lv) {
+        const uint32_t C = min(s_children, kTailMaxChildren);
+        const RecordSet& ps = T.set[(lv - 2) & 1];
+        const RecordSet& cs = T.set[(lv - 3) & 1];
+        const bool box = lv + 1 <= d.rt_log2;
+        const uint32_t child_size = 1u << lv;
+        // 1. stage children
+        for (uint32_t i = tid; i < C; i += kTailThreads) {
+            if (lv == 2) {
+                skey[i] = d.bkey[i];
+                sref[i] = __ldcg(&T.ctable0[d.bslot[i]].w);
+                scnt[i] = __popcll(d.bmask[i]);
+            } else {
+                skey[i] = cs.key[i];
+                sref[i] = lv == lv0 ? __ldcg(&T.ctable0[cs.slot[i]].w) : cs.slot[i];
+                scnt[i] = cs.cnt[i];
+            }
+        }
+        __syncthreads();
+        // 2. heads (4 consecutive children per thread) and parent indices
+        constexpr uint32_t PER = kTailMaxChildren / kTailThreads;
+        uint32_t hmask = 0, hc = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t i = tid * PER + k;
+            if (i < C && (i == 0 || (skey[i] >> 3) != (skey[i - 1] >> 3))) { hmask |= 1u << k; ++hc; }
+        }
+        uint32_t P;
+        uint32_t pbase = tail_scan(hc, scan, &P);
+        // 3. build parents (records and words in global memory)
+        uint32_t par = pbase;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            if (!((hmask >> k) & 1)) continue;
+            const uint32_t i = tid * PER + k;
+            const uint64_t pkey = skey[i] >> 3;
+            uint32_t mask = 0, count = 0, n = 0;
+            uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
+            uint32_t* pw = ps.words + uint64_t(par) * kNodeStride;
+            for (uint32_t j = i; j < C && n < 8; ++j) {
+                const uint64_t ck = skey[j];
+                if ((ck >> 3) != pkey) break;
+                const uint32_t idx = uint32_t(ck & 7);
+                mask |= 1u << idx;
+                count = sat_add(count, scnt[j]);
+                pw[2 + n] = sref[j];
+                if (box) {
+                    uint64_t clo, chi;
+                    if (lv == 2) brick_box(d.bmask[j], clo, chi);
+                    else { clo = cs.lo[j]; chi = cs.hi[j]; }
+                    const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
+                                   oz = (idx >> 2) * child_size;
+                    lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
+                    lo[1] = min(lo[1], cell_y(clo) + oy); hi[1] = max(hi[1], cell_y(chi) + oy);
+                    lo[2] = min(lo[2], cell_z(clo) + oz); hi[2] = max(hi[2], cell_z(chi) + oz);
+                }
+                ++n;
+            }
+            pw[0] = mask;
+            pw[1] = count;
+            ps.key[par] = pkey;
+            ps.cnt[par] = count;
+            ps.first[par] = lv == 2 ? d.bfirst[i] : cs.first[i];
+            if (box) {
+                ps.lo[par] = pack_cell(lo[0], lo[1], lo[2]);
+                ps.hi[par] = pack_cell(hi[0], hi[1], hi[2]);
+            }
+            plen[par] = 2 + n;
+            ++par;
+        }
+        __syncthreads();  // all words written (visible to the block)
+        // 4. dedup in the shared-memory table (owner = minimum parent index)
+        for (uint32_t q = tid; q < P; q += kTailThreads) {
+            const uint32_t* w = ps.words + uint64_t(q) * kNodeStride;
+            const uint32_t len = plen[q];
+            uint64_t h64 = len;
+            for (uint32_t k = 0; k < len; ++k) h64 = mix64(h64 ^ w[k]);
+            uint32_t h = uint32_t(h64) & (kTailSlots - 1);
+            uint32_t probes = 0;
+            for (; probes < kTailSlots; ++probes, h = (h + 1) & (kTailSlots - 1)) {
+                uint32_t cur = atomicCAS(tkey + h, 0u, q + 1);
+                if (cur == 0) break;
+                const uint32_t o = cur - 1;
+                if (plen[o] != len) continue;
+                const uint32_t* ow = ps.words + uint64_t(o) * kNodeStride;
+                bool same = true;
+                for (uint32_t k = 0; k < len && same; ++k) same = ow[k] == w[k];
+                if (same) break;
+            }
+            if (probes == kTailSlots) atomicOr(d.counters + kCtrError, kErrTable);
+            pslot[q] = h;
+            atomicMin(towner + h, q);
+        }
+        __syncthreads();
+        // 5. owners: word offsets in parent order, write words, slot value = offset
+        uint32_t wl = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t q = tid * PER + k;
+            if (q < P && towner[pslot[q]] == q) wl += plen[q];
+        }
+        uint32_t words;
+        uint32_t off = tail_scan(wl, scan, &words) + s_cursor;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t q = tid * PER + k;
+            if (q < P && towner[pslot[q]] == q) {
+                const uint32_t* w = ps.words + uint64_t(q) * kNodeStride;
+                if (uint64_t(off) + plen[q] <= d.node_bound) {
+                    for (uint32_t m = 0; m < plen[q]; ++m) d.nodes[off + m] = w[m];
+                } else {
+                    atomicOr(d.counters + kCtrError, kErrBound);
+                }
+                tval[pslot[q]] = off;
+                off += plen[q];
+            }
+        }
+        uint32_t owners = 0;
+        for (uint32_t q = tid; q < P; q += kTailThreads) owners += towner[pslot[q]] == q;
+        uint32_t utotal;
+        tail_scan(owners, scan, &utotal);  // includes a barrier: tval complete
+        // 6. references for the next level, prims, roots
+        for (uint32_t q = tid; q < P; q += kTailThreads) {
+            const uint32_t node = tval[pslot[q]];
+            ps.slot[q] = node;
+            if (lv + 1 == d.rt_log2 && q < d.prim_bound) {
+                const uint64_t full = ps.key[q];
+                const uint64_t key = full & ((1ull << local_shift) - 1);
+                const uint32_t chunk = uint32_t(full >> local_shift);
+                const uint32_t cx = compact3(key), cy = compact3(key >> 1), cz = compact3(key >> 2);
+                const uint32_t first = d.chunked ? d.chunk_first[chunk] : 0;
+                const uint32_t size = 1u << d.rt_log2;
+                uint4 rec;
+                rec.x = node;
+                rec.y = ps.first[q] - first;
+                const uint64_t pc = pack_cell(cx, cy, cz);
+                rec.z = uint32_t(pc);
+                rec.w = uint32_t(pc >> 32);
+                reinterpret_cast<uint4*>(d.prims)[q] = rec;
+                const uint64_t plo = ps.lo[q], phi = ps.hi[q];
+                const float eps = 1.0f / 256.0f;
+                float* b = d.aabbs + uint64_t(q) * 6;
+                b[0] = __fsub_rn(__fadd_rn(float(cx * size), float(cell_x(plo))), eps);
+                b[1] = __fsub_rn(__fadd_rn(float(cy * size), float(cell_y(plo))), eps);
+                b[2] = __fsub_rn(__fadd_rn(float(cz * size), float(cell_z(plo))), eps);
+                b[3] = __fadd_rn(__fadd_rn(float(cx * size), float(cell_x(phi))), eps);
+                b[4] = __fadd_rn(__fadd_rn(float(cy * size), float(cell_y(phi))), eps);
+                b[5] = __fadd_rn(__fadd_rn(float(cz * size), float(cell_z(phi))), eps);
+                if (d.chunked && (q == 0 || (ps.key[q - 1] >> local_shift) != chunk)) d.prim_start[chunk] = q;
+            }
+            if (lv + 1 == d.log2 && d.chunked) {
+                const uint32_t chunk = uint32_t(ps.key[q]);
+                if (chunk < d.seg_count) d.roots[chunk] = node;
+            }
+        }
+        // clear the table for the next level
+        for (uint32_t i = tid; i < kTailSlots; i += kTailThreads) { tkey[i] = 0; towner[i] = 0xFFFFFFFFu; }
+        if (tid == 0) {
+            d.counters[kCtrParents + lv] = P;
+            d.counters[kCtrUniqueLv + lv] = utotal;
+            s_cursor += words;
+            d.counters[kCtrCursor + lv + 1] = s_cursor;
+            s_children = P;
+            if (lv + 1 == d.rt_log2) d.counters[kCtrPrims] = P;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        // final counts and the empty geometry (gbuild.zig:607-624)
+        const uint32_t top_set = (d.log2 - 1 - 2) & 1;
+        uint32_t cursor = s_cursor;
+        uint32_t root = s_children > 0 ? T.set[top_set].slot[0] : 0;
+        if (d.counters[kCtrUnique] == 0) {
+            if (cursor + 2 <= d.node_bound) {
+                d.nodes[cursor] = 0;
+                d.nodes[cursor + 1] = 0;
+            }
+            root = cursor;
+            cursor += 2;
+            d.counters[kCtrPrims] = 0;
+        }
+        d.counters[kCtrRoot] = root;
+        d.counters[kCtrWords] = cursor;
+    }
 }
 
 // Root(s), node word count and the empty geometry (gbuild.zig:607-624).

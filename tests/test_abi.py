@@ -40,7 +40,7 @@ def test_host_only_calls():
     L = native.lib()
     assert L.pyrb_version() >= 1
     assert L.pyrb_result_string(-1) == b"invalid argument"
-    t = native.Tuning(radix_bits=5, tile_keys=4096, load_factor_pct=50)
+    t = native.Tuning(radix_bits=5, tile_keys=4096, load_factor_pct=50)  # 5 is not a supported width
     assert L.pyrb_set_tuning(ctypes.byref(t)) == -1
     assert b"radix_bits" in L.pyrb_error_message()
 

@@ -150,7 +150,7 @@ def test_noise256_with_edits_matches_oracle(gb):
 
 
 @pytest.mark.parametrize("radix_bits,tile_keys,lf", [(4, 1024, 50), (8, 2048, 70), (11, 4096, 50), (11, 1024, 90),
-                                                     (8, 4096, 25)])
+                                                     (8, 4096, 25), (9, 4096, 50), (10, 2048, 70), (9, 1024, 50)])
 def test_tuning_variants_are_bit_exact(gb, radix_bits, tile_keys, lf):
     """The autotuner's knobs (digit width, tile, load factor) never change the output."""
     _, pts = _scene_points(6)
