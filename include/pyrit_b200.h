@@ -147,6 +147,35 @@ PYRB_API pyrb_result pyrb_build_chunks_edits(const pyrb_exec* e, uint32_t log2_s
                                              uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim,
                                              pyrb_built* out);
 
+/* Batched build of many chunks of mixed edges in one pipeline run (the batched form
+ * beside the reference's buildChunks, which needs one edge for all chunks). Chunk c
+ * (edge 2^log2[c], log2 in [3, 10]) holds voxels[voxel_offsets[c] .. voxel_offsets[c+1])
+ * in chunk-local coordinates, optionally followed by its overlay edits
+ * edits[edit_offsets[c] .. edit_offsets[c+1]) (last entry wins, attribute 0 removes).
+ * All chunks share one node/leaf/attribute buffer (nodes are deduplicated across
+ * chunks). Keys carry the chunk number above 3 * max(log2) bits. Per chunk:
+ * roots[c] (node offset of its root, 0xFFFFFFFF = empty), first_voxel[c] (first
+ * attribute), first_prim[c] (first prim; prims are at edge 2^rt with
+ * rt = clamp(rt_log2_req, 3, min(log2))). A chunk's voxel count is nodes[root + 1]. */
+typedef struct pyrb_batch {
+    uint32_t count;
+    uint32_t reserved;
+    const uint32_t* log2_host;   /* host u32[count] (sizes the scratch) */
+    uint64_t log2;               /* device u32[count], same values */
+    uint64_t voxels;             /* device PyrVoxel[voxel_total] */
+    uint64_t voxel_offsets;      /* device u32[count+1] */
+    uint64_t edits;              /* device PyrVoxel[edit_total] or 0 */
+    uint64_t edit_offsets;       /* device u32[count+1] or 0 */
+    uint32_t voxel_total;        /* host copy of voxel_offsets[count] */
+    uint32_t edit_total;         /* host copy of edit_offsets[count] (0 = no edits) */
+} pyrb_batch;
+PYRB_API pyrb_result pyrb_build_batch(const pyrb_exec* e, const pyrb_batch* batch, uint32_t rt_log2_req,
+                                      uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim, pyrb_built* out);
+/* Asynchronous form (see pyrb_build_async); roots/first_voxel/first_prim should be pinned. */
+PYRB_API pyrb_result pyrb_build_batch_async(const pyrb_exec* e, const pyrb_batch* batch, uint32_t rt_log2_req,
+                                            uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim,
+                                            uint32_t* host_counts, pyrb_built* out);
+
 /* gpu_build.downsample (src/gpu_build.zig:128-131): LOD of edge 2^(log2_src - shift)
  * from the sorted voxels of an editable geometry; per coarse cell the source voxel
  * with the largest key wins. shift >= 1 and shift + 3 <= log2_src. */

@@ -134,6 +134,10 @@ struct Job {
     uint32_t edit_total = 0;
     uint64_t src_keys = 0, src_vals = 0;
     uint32_t shift = 0;
+    // kModeBatch
+    const uint32_t* chunk_log2_host = nullptr;
+    uint64_t chunk_log2 = 0, voxel_offsets = 0, edit_offsets2 = 0;
+    uint32_t voxel_total = 0;
     uint32_t* roots = nullptr;
     uint32_t* first_voxel = nullptr;
     uint32_t* first_prim = nullptr;
@@ -329,13 +333,26 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
         return fail(PYRB_ERROR_INVALID_ARGUMENT,
                     "log2_size %u needs 64-bit sort keys; this build sorts 32-bit keys (log2_size <= 10)", log2);
     const uint32_t K = job.K;
-    const bool chunked = job.mode == kModeChunks || job.mode == kModeChunksEdits;
+    const bool chunked = job.mode == kModeChunks || job.mode == kModeChunksEdits || job.mode == kModeBatch;
+    // chunks per edge (kModeBatch mixes edges; every other mode has K chunks of edge 2^log2)
+    uint64_t per_log2[24] = {};
+    uint32_t min_log2 = log2;
+    if (job.mode == kModeBatch) {
+        for (uint32_t c = 0; c < K; ++c) {
+            const uint32_t l = job.chunk_log2_host[c];
+            if (l < 3 || l > log2) return fail(PYRB_ERROR_INVALID_ARGUMENT, "chunk %u: log2 %u outside [3, %u]", c, l, log2);
+            ++per_log2[l];
+            min_log2 = std::min(min_log2, l);
+        }
+    } else {
+        per_log2[log2] = K;
+    }
     if (chunked) {
         uint32_t bits = 0;
         while ((uint64_t(1) << bits) < K) ++bits;
         if (lb + bits + 1 > 64) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many chunks for this chunk size");
     }
-    const uint32_t rt = std::min(std::max(job.rt_req, 3u), log2);
+    const uint32_t rt = std::min(std::max(job.rt_req, 3u), min_log2);
     cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
     Mem mem{e, st};
 
@@ -345,6 +362,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
         case kModePlain: n64 = uint64_t(job.n_old) + job.n_new; break;
         case kModeChunks: n64 = job.total; break;
         case kModeChunksEdits: n64 = uint64_t(K) * job.capacity + job.edit_total; break;
+        case kModeBatch: n64 = uint64_t(job.voxel_total) + job.edit_total; break;
         default: n64 = job.n_new; break;
     }
     if (n64 >= (uint64_t(1) << 31)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many entries for one build (%llu)", (unsigned long long)n64);
@@ -379,6 +397,9 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.edit_offsets = reinterpret_cast<const uint32_t*>(job.edit_offsets);
     d.src_keys = reinterpret_cast<const uint64_t*>(job.src_keys);
     d.src_vals = reinterpret_cast<const uint32_t*>(job.src_vals);
+    d.chunk_log2 = reinterpret_cast<const uint32_t*>(job.chunk_log2);
+    d.voxel_offsets = reinterpret_cast<const uint32_t*>(job.voxel_offsets);
+    d.edit_offsets2 = reinterpret_cast<const uint32_t*>(job.edit_offsets2);
     d.chunked = chunked ? 1u : 0u;
 
     // digit plan over lb + 1 bits (the invalid bit on top)
@@ -401,9 +422,14 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
 
     // per-level upper bounds
     auto cells = [&](uint32_t edge_log2) -> uint64_t {  // cells of edge 2^edge_log2 in all chunks
-        uint32_t e3 = 3 * (log2 - edge_log2);
-        if (e3 >= 40) return ~0ull >> 1;
-        return (uint64_t(1) << e3) * K;
+        uint64_t total = 0;
+        for (uint32_t l = 3; l <= log2; ++l) {
+            if (!per_log2[l]) continue;
+            const uint32_t e3 = l > edge_log2 ? 3 * (l - edge_log2) : 0;  // a smaller chunk: one cell
+            if (e3 >= 40) return ~0ull >> 1;
+            total += (uint64_t(1) << e3) * per_log2[l];
+        }
+        return total;
     };
     const uint32_t B = uint32_t(std::max<uint64_t>(std::min<uint64_t>(nmax, cells(2)), 1));
     uint32_t P[kMaxLevels + 2] = {};
@@ -592,6 +618,11 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     launches += 3;
     const uint32_t lv0 = tail_level(log2, B, P);
     launches += launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
+    if (job.mode == kModeBatch && min_log2 < log2) {
+        k_batch_roots<<<std::max(std::min((K + 255) / 256, 1024u), 1u), 256, 0, st>>>(d, log2);
+        prof.mark("batch_roots");
+        ++launches;
+    }
     CUL(cudaGetLastError());
 
     const uint64_t out_bytes = uint64_t(d.node_bound) * 4 + uint64_t(B) * 8 + uint64_t(nmax) * 12 +
@@ -694,6 +725,49 @@ PYRB_API pyrb_result pyrb_build_chunks(const pyrb_exec* e, uint32_t log2_size, u
     j.first_voxel = first_voxel;
     j.first_prim = first_prim;
     return run_build(e, j, out);
+}
+
+static pyrb_result batch_job(const pyrb_batch* b, uint32_t rt_log2_req, uint32_t* roots, uint32_t* first_voxel,
+                             uint32_t* first_prim, Job& j) {
+    if (!b || b->count == 0) return fail(PYRB_ERROR_INVALID_ARGUMENT, "empty batch");
+    if (!b->log2_host || !b->log2 || !b->voxel_offsets || (b->voxel_total && !b->voxels))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL batch buffers");
+    if (b->edit_total && (!b->edits || !b->edit_offsets))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "edit_total > 0 without edit buffers");
+    uint32_t lmax = 0;
+    for (uint32_t c = 0; c < b->count; ++c) lmax = std::max(lmax, b->log2_host[c]);
+    j.mode = kModeBatch;
+    j.log2 = lmax;
+    j.rt_req = rt_log2_req;
+    j.K = b->count;
+    j.voxels = b->voxels;
+    j.edits = b->edit_total ? b->edits : 0;
+    j.chunk_log2_host = b->log2_host;
+    j.chunk_log2 = b->log2;
+    j.voxel_offsets = b->voxel_offsets;
+    j.edit_offsets2 = b->edit_total ? b->edit_offsets : 0;
+    j.voxel_total = b->voxel_total;
+    j.edit_total = b->edit_total;
+    j.roots = roots;
+    j.first_voxel = first_voxel;
+    j.first_prim = first_prim;
+    return PYRB_OK;
+}
+
+PYRB_API pyrb_result pyrb_build_batch(const pyrb_exec* e, const pyrb_batch* batch, uint32_t rt_log2_req,
+                                      uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim, pyrb_built* out) {
+    Job j;
+    pyrb_result r = batch_job(batch, rt_log2_req, roots, first_voxel, first_prim, j);
+    return r != PYRB_OK ? r : run_build(e, j, out);
+}
+
+PYRB_API pyrb_result pyrb_build_batch_async(const pyrb_exec* e, const pyrb_batch* batch, uint32_t rt_log2_req,
+                                            uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim,
+                                            uint32_t* host_counts, pyrb_built* out) {
+    if (!host_counts) return fail(PYRB_ERROR_INVALID_ARGUMENT, "host_counts is NULL");
+    Job j;
+    pyrb_result r = batch_job(batch, rt_log2_req, roots, first_voxel, first_prim, j);
+    return r != PYRB_OK ? r : run_build(e, j, out, host_counts);
 }
 
 PYRB_API pyrb_result pyrb_build_chunks_edits(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,

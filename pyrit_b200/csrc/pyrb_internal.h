@@ -33,6 +33,7 @@ enum Mode : uint32_t {
     kModeChunks = 1,       // segments of `capacity` PyrVoxels, filled per offsets[]
     kModeChunksEdits = 2,  // generated voxels per counts[] followed by overlay edits per edit_offsets[]
     kModeDownsample = 3,   // coarse keys of sorted source keys
+    kModeBatch = 4,        // packed per-chunk voxel lists (+ edits) of mixed edges 2^log2[c]
 };
 
 // Everything a build's kernels need, passed by value (kernel parameter space).
@@ -60,6 +61,9 @@ struct BuildDesc {
     const uint32_t* edit_offsets; // kModeChunksEdits: u32[K+1]
     const uint64_t* src_keys;     // kModeDownsample
     const uint32_t* src_vals;
+    const uint32_t* chunk_log2;   // kModeBatch: u32[K] edge of every chunk
+    const uint32_t* voxel_offsets;  // kModeBatch: u32[K+1] into voxels
+    const uint32_t* edit_offsets2;  // kModeBatch: u32[K+1] into edits (NULL = no edits)
 
     // segment tiling of the sort / unique stages
     uint32_t* seg_entry;     // u32[K+1]: first raw entry of each segment

@@ -55,6 +55,10 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
                 case kModeChunksEdits:
                     size = min(__ldg(d.gen_counts + c), d.capacity) + (__ldg(d.edit_offsets + c + 1) - __ldg(d.edit_offsets + c));
                     break;
+                case kModeBatch:
+                    size = __ldg(d.voxel_offsets + c + 1) - __ldg(d.voxel_offsets + c);
+                    if (d.edit_offsets2) size += __ldg(d.edit_offsets2 + c + 1) - __ldg(d.edit_offsets2 + c);
+                    break;
                 default: size = d.n_total; break;
             }
         }
@@ -121,6 +125,12 @@ __device__ __forceinline__ void load_raw(const BuildDesc& d, uint32_t seg, uint3
             uint4 v = j < g ? __ldg(d.voxels + uint64_t(seg) * d.capacity + j)
                             : __ldg(d.edits + __ldg(d.edit_offsets + seg) + (j - g));
             encode_voxel(v, d.log2, d.lb, key, val);
+            break;
+        }
+        case kModeBatch: {
+            const uint32_t vb = __ldg(d.voxel_offsets + seg), vn = __ldg(d.voxel_offsets + seg + 1) - vb;
+            const uint4 v = j < vn ? __ldg(d.voxels + vb + j) : __ldg(d.edits + __ldg(d.edit_offsets2 + seg) + (j - vn));
+            encode_voxel(v, __ldg(d.chunk_log2 + seg), d.lb, key, val);
             break;
         }
         default: {  // downsample (gbuild.zig:262-274): coarse key of the source voxel
@@ -1169,6 +1179,19 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
         }
         d.counters[kCtrRoot] = root;
         d.counters[kCtrWords] = cursor;
+    }
+}
+
+// Mixed batch: chunk c of edge 2^log2[c] < 2^top_log2 sits in the low corner of its
+// cell, so above its own top level it hangs below single-child nodes (child index
+// 0). Its root is found by descending from the cell's top node.
+__global__ void k_batch_roots(BuildDesc d, uint32_t max_log2) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < d.seg_count; c += gridDim.x * blockDim.x) {
+        uint32_t node = d.roots[c];
+        if (node == 0xFFFFFFFFu) continue;
+        const uint32_t l = __ldg(d.chunk_log2 + c);
+        for (uint32_t lv = max_log2; lv > l; --lv) node = d.nodes[node + 2];
+        d.roots[c] = node;
     }
 }
 

@@ -176,6 +176,48 @@ def build_chunks_edits(log2_size: int, rt_log2_req: int, count: int, capacity: i
     return r
 
 
+def build_batch(log2s, rt_log2_req: int, voxels, voxel_offsets, edits=None, edit_offsets=None,
+                stream=None) -> Built:
+    """Batched build of chunks with mixed edges (host arrays are uploaded here).
+
+    log2s: host uint32[K]; voxels: uint32[N, 4] (chunk-local PyrVoxels, chunk c at
+    voxel_offsets[c]:voxel_offsets[c+1]); optional per-chunk overlay edits. Arrays may be
+    numpy (uploaded) or device tensors."""
+    import torch
+    stream = _current_stream() if stream is None else stream
+    log2s = np.ascontiguousarray(log2s, dtype=np.uint32)
+    K = len(log2s)
+    keep = []
+
+    def dev32(a):
+        if a is None:
+            return None
+        if isinstance(a, np.ndarray):
+            t = torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+            keep.append(t)
+            return t
+        return a
+
+    vo = np.asarray(voxel_offsets.cpu() if hasattr(voxel_offsets, "cpu") else voxel_offsets, dtype=np.uint32)
+    eo = None if edit_offsets is None else np.asarray(
+        edit_offsets.cpu() if hasattr(edit_offsets, "cpu") else edit_offsets, dtype=np.uint32)
+    b = native.Batch(count=K, log2_host=log2s.ctypes.data, log2=_addr(dev32(log2s)),
+                     voxels=_addr(dev32(voxels)) if int(vo[-1]) else 0, voxel_offsets=_addr(dev32(vo)),
+                     edits=_addr(dev32(edits)) if eo is not None and int(eo[-1]) else 0,
+                     edit_offsets=_addr(dev32(eo)) if eo is not None else 0,
+                     voxel_total=int(vo[-1]), edit_total=0 if eo is None else int(eo[-1]))
+    roots = np.zeros(K, np.uint32)
+    first = np.zeros(K, np.uint32)
+    prim = np.zeros(K, np.uint32)
+    out = native.BuiltC()
+    native.check(native.lib().pyrb_build_batch(ctypes.byref(_exec(stream)), ctypes.byref(b), rt_log2_req,
+                                               roots.ctypes.data, first.ctypes.data, prim.ctypes.data,
+                                               ctypes.byref(out)))
+    r = Built(out, stream)
+    r.roots, r.first_voxel, r.first_prim = roots, first, prim
+    return r
+
+
 def downsample(log2_src: int, rt_log2_req: int, src_keys, src_vals, n_src: int, shift: int, stream=None) -> Built:
     """gpu_build.downsample: LOD from the sorted voxels (keys/attrs) of a previous build."""
     stream = _current_stream() if stream is None else stream

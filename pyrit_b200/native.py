@@ -44,6 +44,13 @@ class ChunkBatch(ctypes.Structure):
                 ("offsets", ctypes.c_uint64), ("total", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
+class Batch(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("log2_host", ctypes.c_void_p),
+                ("log2", ctypes.c_uint64), ("voxels", ctypes.c_uint64), ("voxel_offsets", ctypes.c_uint64),
+                ("edits", ctypes.c_uint64), ("edit_offsets", ctypes.c_uint64), ("voxel_total", ctypes.c_uint32),
+                ("edit_total", ctypes.c_uint32)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("brick_count", ctypes.c_uint32), ("level_parents", ctypes.c_uint32 * 24),
                 ("level_unique", ctypes.c_uint32 * 24), ("sort_passes", ctypes.c_uint32),
@@ -79,6 +86,10 @@ SIGNATURES = {
     "pyrb_build_finish": (ctypes.c_int32, [_p, ctypes.POINTER(BuiltC)]),
     "pyrb_profile_enable": (None, [ctypes.c_int]),
     "pyrb_profile_read": (ctypes.c_uint32, [_p, _p, _u32, _u32]),
+    "pyrb_build_batch": (ctypes.c_int32, [ctypes.POINTER(Exec), ctypes.POINTER(Batch), _u32, _p, _p, _p,
+                                          ctypes.POINTER(BuiltC)]),
+    "pyrb_build_batch_async": (ctypes.c_int32, [ctypes.POINTER(Exec), ctypes.POINTER(Batch), _u32, _p, _p, _p, _p,
+                                                ctypes.POINTER(BuiltC)]),
     "pyrb_built_free": (None, [ctypes.POINTER(Exec), ctypes.POINTER(BuiltC)]),
     "pyrb_last_stats": (None, [ctypes.POINTER(Stats)]),
     "pyrb_error_message": (ctypes.c_char_p, []),

@@ -39,3 +39,47 @@ def assert_same_build(g, o, chunks: bool = False, label: str = ""):
         assert np.array_equal(g.roots, o.roots), f"{label} roots differ"
         assert np.array_equal(g.first_voxel, o.first_voxel), f"{label} first_voxel differ"
         assert np.array_equal(g.first_prim, o.first_prim), f"{label} first_prim differ"
+
+
+def subdag(log2, nodes, leaves, root):
+    """Canonical form of the DAG below `root`: nodes level by level (8^3 level first,
+    first visit in child-index order), leaves renumbered by first visit. Returns
+    (node words, leaf masks, root offset). Lets a chunk of a shared batch buffer be
+    compared with its own single build."""
+    top = log2 - 1
+    order = {lv: [] for lv in range(2, top + 1)}
+    seen = {lv: {} for lv in range(2, top + 1)}
+    leaf_ids, leaf_list = {}, []
+    seen[top][int(root)] = 0
+    order[top].append(int(root))
+    # iterative DFS with explicit child order
+    visit = [(int(root), top, 0)]
+    while visit:
+        off, lv, k = visit.pop()
+        n = bin(int(nodes[off]) & 0xFF).count("1")
+        if k >= n:
+            continue
+        visit.append((off, lv, k + 1))
+        ref = int(nodes[off + 2 + k])
+        if lv == 2:
+            if ref not in leaf_ids:
+                leaf_ids[ref] = len(leaf_list)
+                leaf_list.append(int(leaves[ref]))
+        elif ref not in seen[lv - 1]:
+            seen[lv - 1][ref] = len(order[lv - 1])
+            order[lv - 1].append(ref)
+            visit.append((ref, lv - 1, 0))
+    coff, w = {}, 0
+    for lv in range(2, top + 1):
+        for off in order[lv]:
+            coff[(lv, off)] = w
+            w += 2 + bin(int(nodes[off]) & 0xFF).count("1")
+    out = []
+    for lv in range(2, top + 1):
+        for off in order[lv]:
+            n = bin(int(nodes[off]) & 0xFF).count("1")
+            out += [int(nodes[off]), int(nodes[off + 1])]
+            for k in range(n):
+                ref = int(nodes[off + 2 + k])
+                out.append(leaf_ids[ref] if lv == 2 else coff[(lv - 1, ref)])
+    return out, leaf_list, coff[(top, int(root))]
