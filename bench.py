@@ -350,6 +350,99 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args, emit=True):
+    """1024 chunks of the mix (edges 32/64/128/256 with p .4/.3/.2/.1, heightfield tiled per
+    chunk and scaled to the edge, 0..20 spherical caves), generated on the device: one
+    batched build of all chunks (autotuned) vs the per-chunk loop of plain builds."""
+    import torch
+    from pyrit_b200 import autotune, gpu_build, native
+    from pyrit_b200 import workloads as wl
+
+    K = args.chunks
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    L = native.lib()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    ex = native.Exec()
+    ex.stream = ctypes.c_void_p(sptr)
+    log2s = wl.chunk_mix(K, 0)
+    vox, offs = wl.mix_chunks_device(log2s, 0, 0)
+    total = int(offs[-1])
+    d_log2 = torch.from_numpy(log2s.view(np.int32)).cuda()
+    d_offs = torch.from_numpy(offs.astype(np.uint32).view(np.int32)).cuda()
+    counts = torch.zeros(native.COUNTS_WORDS, dtype=torch.int32).pin_memory()
+    roots = torch.zeros(K, dtype=torch.int32).pin_memory()
+    first = torch.zeros(K, dtype=torch.int32).pin_memory()
+    fprim = torch.zeros(K, dtype=torch.int32).pin_memory()
+
+    def batch_desc(k):
+        return native.Batch(count=k, log2_host=log2s.ctypes.data, log2=d_log2.data_ptr(), voxels=vox.data_ptr(),
+                            voxel_offsets=d_offs.data_ptr(), edits=0, edit_offsets=0,
+                            voxel_total=int(offs[k]), edit_total=0)
+
+    def batched_once(k=K):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        bd = batch_desc(k)
+        out = native.BuiltC()
+        a.record(stream)
+        native.check(L.pyrb_build_batch_async(ctypes.byref(ex), ctypes.byref(bd), 5, roots.data_ptr(),
+                                              first.data_ptr(), fprim.data_ptr(), counts.data_ptr(),
+                                              ctypes.byref(out)))
+        b.record(stream)
+        L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(out))
+        return a, b
+
+    # autotune on the first 128 chunks, then measure the full batch
+    best, _ = autotune.sweep(lambda: batched_once(min(128, K)), reps=2, budget_s=args.tune_budget)
+    autotune.apply(best)
+    for _ in range(2):
+        batched_once()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.batched_reps):
+        a, b = batched_once()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    o = native.BuiltC()
+    native.check(L.pyrb_build_finish(counts.data_ptr(), ctypes.byref(o)))
+    n_u = o.voxel_count
+    t_batched = min(times)
+
+    # per-chunk loop of plain builds (asynchronous, one stream)
+    def loop_once():
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for c in range(K):
+            out = native.BuiltC()
+            n = int(offs[c + 1] - offs[c])
+            native.check(L.pyrb_build_async(ctypes.byref(ex), int(log2s[c]), 5, 0, 0, 0,
+                                            vox.data_ptr() + 16 * int(offs[c]), n, counts.data_ptr(),
+                                            ctypes.byref(out)))
+            L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(out))
+        b.record(stream)
+        return a, b
+
+    loop_once()
+    torch.cuda.synchronize()
+    a, b = loop_once()
+    torch.cuda.synchronize()
+    t_loop = a.elapsed_time(b)
+    res = {"chunks": K, "entries": total, "unique_voxels": n_u, "batched_ms": t_batched,
+           "batched_voxels_per_s": n_u / (t_batched / 1e3), "per_chunk_loop_ms": t_loop,
+           "per_chunk_loop_voxels_per_s": n_u / (t_loop / 1e3), "speedup_vs_per_chunk_loop": t_loop / t_batched,
+           "tuning": {k: best[k] for k in ("radix_bits", "tile_keys", "load_factor_pct")},
+           "edges": {str(1 << l): int((log2s == l).sum()) for l in (5, 6, 7, 8)}}
+    if emit:
+        print(json.dumps({"metric": METRIC + " (batched, 1024 mixed chunks)", "value": res["batched_voxels_per_s"],
+                          "unit": "voxels/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+                          "config": {"workload": "batched build of 1024 chunks of the mix, generated on the device"},
+                          "batched": res}), flush=True)
+    del vox
+    torch.cuda.empty_cache()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,11 +450,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["noise256", "batched"], default="noise256")
+    ap.add_argument("--chunks", type=int, default=1024)
+    ap.add_argument("--batched-reps", type=int, default=3)
+    ap.add_argument("--tune-budget", type=float, default=30.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        run_batched(args)
+        return 0
     return run_ours(args)
 
 

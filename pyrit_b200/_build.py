@@ -20,7 +20,7 @@ INCLUDE = os.path.join(ROOT, "include")
 
 CUDA_SOURCES = ["pyrb_build.cu"]
 CUDA_HEADERS = ["pyrb_device.cuh", "pyrb_internal.h", "pyrb_kernels.cuh"]
-WORKLOAD_SOURCES = ["workloads.cpp"]
+WORKLOAD_SOURCES = ["workloads.cpp", "workloads_gpu.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -65,12 +65,13 @@ def build_cuda(force: bool = False, verbose_ptxas: bool = False) -> str:
 
 
 def build_workloads(force: bool = False) -> str:
+    """Workload generators: host C++ (g++) plus the device-side chunk-mix generator (nvcc)."""
     out = os.path.join(HERE, "libpyrb_workloads.so")
     srcs = [os.path.join(CSRC, s) for s in WORKLOAD_SOURCES]
     deps = srcs + [os.path.join(CSRC, "workloads.h")]
     if force or _stale(out, deps):
-        cxx = os.environ.get("CXX", "g++")
-        _run([cxx, "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread", "-ffp-contract=off",
+        _run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-shared",
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread", "-Xcompiler", "-ffp-contract=off",
               "-I", CSRC, "-o", out, *srcs])
     return out
 

@@ -1,0 +1,73 @@
+"""Autotuner of the build's sort and dedup parameters.
+
+Sweeps the radix digit width (4, 8, 9, 10, 11 bits), the keys per sort tile (1024,
+2048, 4096) and the dedup hash-table load factor (50 %, 70 %) on a caller-supplied
+workload, times every setting with CUDA events, applies the fastest through
+pyrb_set_tuning and can persist it as JSON. None of the parameters changes the
+output (the build is bit-exact for all of them); they only change speed and memory.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+import time
+
+from . import gpu_build
+
+RADIX_BITS = (4, 8, 9, 10, 11)
+TILE_KEYS = (1024, 2048, 4096)
+LOAD_FACTORS = (50, 70)
+
+
+def default_path() -> str:
+    return os.path.join(os.path.expanduser("~"), ".cache", "pyrit_b200", "tuning.json")
+
+
+def sweep(run_once, reps: int = 3, radix_bits=RADIX_BITS, tile_keys=TILE_KEYS, load_factors=LOAD_FACTORS,
+          budget_s: float = 60.0):
+    """run_once() must enqueue one build on the current stream and return a pair of
+    (start, end) CUDA events around it. Returns (best setting, all results)."""
+    import torch
+    old = gpu_build.get_tuning()
+    results = []
+    t_start = time.time()
+    try:
+        for rb, tk, lf in itertools.product(radix_bits, tile_keys, load_factors):
+            if time.time() - t_start > budget_s:
+                break
+            gpu_build.set_tuning(rb, tk, lf)
+            run_once()  # warm-up of this setting
+            torch.cuda.synchronize()
+            times = []
+            for _ in range(reps):
+                a, b = run_once()
+                torch.cuda.synchronize()
+                times.append(a.elapsed_time(b))
+            results.append({"radix_bits": rb, "tile_keys": tk, "load_factor_pct": lf, "ms": min(times)})
+    finally:
+        gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+    best = min(results, key=lambda r: r["ms"])
+    return best, results
+
+
+def apply(setting: dict) -> None:
+    gpu_build.set_tuning(setting["radix_bits"], setting["tile_keys"], setting["load_factor_pct"])
+
+
+def save(setting: dict, path: str | None = None) -> str:
+    path = path or default_path()
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    with open(path, "w") as f:
+        json.dump(setting, f)
+    return path
+
+
+def load(path: str | None = None) -> dict | None:
+    path = path or default_path()
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        s = json.load(f)
+    apply(s)
+    return s

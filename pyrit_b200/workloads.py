@@ -46,6 +46,12 @@ def lib():
         L.wl_attr_of.restype = u32
         L.wl_poisson_arrivals.argtypes = [u64, ctypes.c_double, u32, p]
         L.wl_poisson_arrivals.restype = None
+        L.wlg_chunk_desc_bytes.restype = u64
+        L.wlg_describe.argtypes = [u32, p, u32, u32, p, p, p, ctypes.POINTER(u64), ctypes.POINTER(u64)]
+        L.wlg_describe.restype = None
+        L.wlg_heights.argtypes = [p, p, u32, u64, u32, p, p]
+        L.wlg_row_counts.argtypes = [p, p, u32, u64, p, p, p]
+        L.wlg_row_fill.argtypes = [p, p, u32, u64, p, p, p, p]
         _lib = L
     return _lib
 
@@ -129,3 +135,43 @@ def poisson_arrivals(n: int, rate: float, seed: int = 0) -> np.ndarray:
     out = np.empty(n, dtype=np.float64)
     lib().wl_poisson_arrivals(n, rate, seed, out.ctypes.data)
     return out
+
+
+def mix_chunks_device(log2s, first_index: int = 0, seed: int = 0):
+    """Chunk-mix content generated on the current CUDA device (same lists as mix_chunk).
+
+    Returns (voxels: int32 tensor [N, 4] in PyrVoxel layout, offsets: int64 numpy [K+1]).
+    Chunk c is the mix chunk number first_index + c with edge 2^log2s[c]."""
+    import torch
+    L = lib()
+    log2s = np.ascontiguousarray(log2s, dtype=np.uint32)
+    K = len(log2s)
+    desc = np.zeros(K * int(L.wlg_chunk_desc_bytes()), dtype=np.uint8)
+    cb = np.zeros(K, np.uint64)
+    rb = np.zeros(K, np.uint64)
+    tc, tr = ctypes.c_uint64(), ctypes.c_uint64()
+    L.wlg_describe(K, log2s.ctypes.data, first_index, seed, desc.ctypes.data, cb.ctypes.data, rb.ctypes.data,
+                   ctypes.byref(tc), ctypes.byref(tr))
+    dev = torch.device("cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    d_desc = torch.from_numpy(desc).to(dev)
+    d_cb = torch.from_numpy(cb.view(np.int64)).to(dev)
+    d_rb = torch.from_numpy(rb.view(np.int64)).to(dev)
+    heights = torch.empty(int(tc.value), dtype=torch.int32, device=dev)
+    rc = L.wlg_heights(d_desc.data_ptr(), d_cb.data_ptr(), K, tc.value, seed, heights.data_ptr(), stream)
+    assert rc == 0, rc
+    counts = torch.empty(int(tr.value), dtype=torch.int32, device=dev)
+    rc = L.wlg_row_counts(d_desc.data_ptr(), d_rb.data_ptr(), K, tr.value, heights.data_ptr(), counts.data_ptr(),
+                          stream)
+    assert rc == 0, rc
+    row_off = torch.cumsum(counts.to(torch.int64), 0)
+    total = int(row_off[-1].item()) if len(row_off) else 0
+    out = torch.empty((max(total, 1), 4), dtype=torch.int32, device=dev)
+    rc = L.wlg_row_fill(d_desc.data_ptr(), d_rb.data_ptr(), K, tr.value, heights.data_ptr(), row_off.data_ptr(),
+                        out.data_ptr(), stream)
+    assert rc == 0, rc
+    # chunk offsets: row offset at each chunk's first row
+    rows_end = np.concatenate([rb[1:], [tr.value]]).astype(np.int64)
+    ends = row_off[torch.from_numpy(rows_end - 1).to(dev)].cpu().numpy()
+    offsets = np.concatenate([[0], ends]).astype(np.int64)
+    return out[:total], offsets
