@@ -168,6 +168,9 @@ typedef struct pyrb_batch {
     uint64_t edit_offsets;       /* device u32[count+1] or 0 */
     uint32_t voxel_total;        /* host copy of voxel_offsets[count] */
     uint32_t edit_total;         /* host copy of edit_offsets[count] (0 = no edits) */
+    uint64_t voxel_starts;       /* device u64[count] or 0: chunk c's voxels start at voxels[voxel_starts[c]]
+                                    (its size stays voxel_offsets[c+1] - voxel_offsets[c]), so a batch can
+                                    reference chunks in a resident pool without packing them */
 } pyrb_batch;
 PYRB_API pyrb_result pyrb_build_batch(const pyrb_exec* e, const pyrb_batch* batch, uint32_t rt_log2_req,
                                       uint32_t* roots, uint32_t* first_voxel, uint32_t* first_prim, pyrb_built* out);

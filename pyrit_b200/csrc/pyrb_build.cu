@@ -136,7 +136,7 @@ struct Job {
     uint32_t shift = 0;
     // kModeBatch
     const uint32_t* chunk_log2_host = nullptr;
-    uint64_t chunk_log2 = 0, voxel_offsets = 0, edit_offsets2 = 0;
+    uint64_t chunk_log2 = 0, voxel_offsets = 0, edit_offsets2 = 0, voxel_starts = 0;
     uint32_t voxel_total = 0;
     uint32_t* roots = nullptr;
     uint32_t* first_voxel = nullptr;
@@ -400,6 +400,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.chunk_log2 = reinterpret_cast<const uint32_t*>(job.chunk_log2);
     d.voxel_offsets = reinterpret_cast<const uint32_t*>(job.voxel_offsets);
     d.edit_offsets2 = reinterpret_cast<const uint32_t*>(job.edit_offsets2);
+    d.voxel_starts = reinterpret_cast<const uint64_t*>(job.voxel_starts);
     d.chunked = chunked ? 1u : 0u;
 
     // digit plan over lb + 1 bits (the invalid bit on top)
@@ -746,6 +747,7 @@ static pyrb_result batch_job(const pyrb_batch* b, uint32_t rt_log2_req, uint32_t
     j.chunk_log2 = b->log2;
     j.voxel_offsets = b->voxel_offsets;
     j.edit_offsets2 = b->edit_total ? b->edit_offsets : 0;
+    j.voxel_starts = b->voxel_starts;
     j.voxel_total = b->voxel_total;
     j.edit_total = b->edit_total;
     j.roots = roots;

@@ -64,6 +64,7 @@ struct BuildDesc {
     const uint32_t* chunk_log2;   // kModeBatch: u32[K] edge of every chunk
     const uint32_t* voxel_offsets;  // kModeBatch: u32[K+1] into voxels
     const uint32_t* edit_offsets2;  // kModeBatch: u32[K+1] into edits (NULL = no edits)
+    const uint64_t* voxel_starts;   // kModeBatch: u64[K] start of chunk c in voxels (NULL = voxel_offsets[c])
 
     // segment tiling of the sort / unique stages
     uint32_t* seg_entry;     // u32[K+1]: first raw entry of each segment

@@ -128,7 +128,8 @@ __device__ __forceinline__ void load_raw(const BuildDesc& d, uint32_t seg, uint3
             break;
         }
         case kModeBatch: {
-            const uint32_t vb = __ldg(d.voxel_offsets + seg), vn = __ldg(d.voxel_offsets + seg + 1) - vb;
+            const uint32_t vo = __ldg(d.voxel_offsets + seg), vn = __ldg(d.voxel_offsets + seg + 1) - vo;
+            const uint64_t vb = d.voxel_starts ? __ldg(d.voxel_starts + seg) : uint64_t(vo);
             const uint4 v = j < vn ? __ldg(d.voxels + vb + j) : __ldg(d.edits + __ldg(d.edit_offsets2 + seg) + (j - vn));
             encode_voxel(v, __ldg(d.chunk_log2 + seg), d.lb, key, val);
             break;

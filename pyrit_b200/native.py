@@ -48,7 +48,7 @@ class Batch(ctypes.Structure):
     _fields_ = [("count", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("log2_host", ctypes.c_void_p),
                 ("log2", ctypes.c_uint64), ("voxels", ctypes.c_uint64), ("voxel_offsets", ctypes.c_uint64),
                 ("edits", ctypes.c_uint64), ("edit_offsets", ctypes.c_uint64), ("voxel_total", ctypes.c_uint32),
-                ("edit_total", ctypes.c_uint32)]
+                ("edit_total", ctypes.c_uint32), ("voxel_starts", ctypes.c_uint64)]
 
 
 class Stats(ctypes.Structure):
