@@ -443,6 +443,53 @@ def run_batched(args, emit=True):
     return res
 
 
+def run_served(args, emit=True):
+    """Poisson arrivals of chunk-build requests (a chunk of the 1024-chunk mix plus 0..64
+    random edits) at --rate per second for --duration seconds, served by continuous
+    batching with a 40 GB budget for dedup tables and the DAG arena."""
+    import torch
+    from pyrit_b200 import workloads as wl
+    from pyrit_b200.serve import ChunkPool, ChunkServer, Request
+
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    K = args.chunks
+    log2s = wl.chunk_mix(K, 0)
+    vox, offs = wl.mix_chunks_device(log2s, 0, 0)
+    pool = ChunkPool(vox, offs, log2s)
+    out = {}
+    for rate in args.rates:
+        n = int(rate * args.duration)
+        arr = wl.poisson_arrivals(n, rate, 7)
+        rng = np.random.default_rng(11)
+        chunks = rng.integers(0, K, n)
+        nedits = rng.integers(0, 65, n)
+        reqs = [Request(i, int(chunks[i]), wl.chunk_edits(int(log2s[chunks[i]]), int(nedits[i]), 5000 + i),
+                        float(arr[i])) for i in range(n)]
+        srv = ChunkServer(pool, budget_bytes=40 << 30, max_batch_voxels=args.max_batch_voxels, max_inflight=2,
+                          rt_log2=5)
+        srv.keep_results = False
+        # warm-up on a few requests (not timed)
+        srv.serve([Request(-1 - i, int(chunks[i]), reqs[i].edits, 0.0) for i in range(4)], realtime=False)
+        srv.release_all()
+        st = srv.serve(reqs, realtime=True)
+        srv.release_all()
+        s = st.summary()
+        s["offered_req_per_s"] = rate
+        s["offered_voxels_per_s"] = float(np.mean(pool.sizes[chunks]) * rate)
+        out[str(int(rate))] = s
+    if emit:
+        print(json.dumps({"metric": METRIC + " (served, Poisson arrivals)", "unit": "voxels/s", "n_gpus": 1,
+                          "higher_is_better": True, "data": "synthetic",
+                          "config": {"workload": "Poisson chunk requests from the 1024-chunk mix + 0..64 edits",
+                                     "duration_s": args.duration, "budget_gb": 40,
+                                     "max_batch_voxels": args.max_batch_voxels},
+                          "served": out}), flush=True)
+    del vox
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,7 +497,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["noise256", "batched"], default="noise256")
+    ap.add_argument("--workload", choices=["noise256", "batched", "served"], default="noise256")
+    ap.add_argument("--rates", type=float, nargs="+", default=[20000.0])
+    ap.add_argument("--duration", type=float, default=10.0)
+    ap.add_argument("--max-batch-voxels", type=int, default=64 << 20)
     ap.add_argument("--chunks", type=int, default=1024)
     ap.add_argument("--batched-reps", type=int, default=3)
     ap.add_argument("--tune-budget", type=float, default=30.0)
@@ -461,6 +511,9 @@ def main():
         return run_reference(args)
     if args.workload == "batched":
         run_batched(args)
+        return 0
+    if args.workload == "served":
+        run_served(args)
         return 0
     return run_ours(args)
 
