@@ -31,6 +31,10 @@ def sweep(run_once, reps: int = 3, radix_bits=RADIX_BITS, tile_keys=TILE_KEYS, l
     import torch
     old = gpu_build.get_tuning()
     results = []
+    if budget_s <= 0:   # no sweep: report the current setting
+        cur = {"radix_bits": old.radix_bits, "tile_keys": old.tile_keys, "load_factor_pct": old.load_factor_pct,
+               "ms": None}
+        return cur, [cur]
     t_start = time.time()
     try:
         for rb, tk, lf in itertools.product(radix_bits, tile_keys, load_factors):

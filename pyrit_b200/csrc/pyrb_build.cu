@@ -283,28 +283,30 @@ void fill_stats(const uint32_t* ctr, const uint32_t* meta) {
     g_stats = s;
 }
 
-template <int RB, int IT>
+template <int RB, int IT, typename KeyT = uint32_t>
 cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
     const size_t hist_smem = size_t(d.passes) * (1u << RB) * 4;
-    const size_t sort_smem = sort_smem_bytes<RB, IT>();
+    const size_t sort_smem = sort_smem_bytes<RB, IT, KeyT>();
     static std::once_flag once;
     std::call_once(once, [&] {
-        cudaFuncSetAttribute(k_encode_hist<RB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        cudaFuncSetAttribute(k_sort_pass<RB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
-        cudaFuncSetAttribute(k_sort_pass<RB, IT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_encode_hist<RB, IT, KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        cudaFuncSetAttribute(k_sort_pass<RB, IT, KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
+        cudaFuncSetAttribute(k_sort_pass<RB, IT, KeyT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     });
-    k_encode_hist<RB, IT><<<d.sort_tiles, kBlock, hist_smem, st>>>(d);
+    k_encode_hist<RB, IT, KeyT><<<d.sort_tiles, kBlock, hist_smem, st>>>(d);
     prof.mark("encode_hist");
     for (uint32_t p = 0; p < d.passes; ++p) {
-        k_sort_pass<RB, IT><<<d.sort_tiles, kBlock, sort_smem, st>>>(d, p, p & 1);
+        k_sort_pass<RB, IT, KeyT><<<d.sort_tiles, kBlock, sort_smem, st>>>(d, p, p & 1);
         prof.mark("sort_pass", p);
     }
-    k_unique<IT><<<d.sort_tiles, kBlock, 0, st>>>(d, d.passes & 1);
+    k_unique<IT, KeyT><<<d.sort_tiles, kBlock, 0, st>>>(d, d.passes & 1);
     prof.mark("unique");
     return cudaGetLastError();
 }
 
+// 64-bit sort keys (edges above 2^10): one digit width and tile, 8 bits x 2048 keys.
 cudaError_t launch_sort_any(uint32_t rb, uint32_t it, const BuildDesc& d, cudaStream_t st, Prof& prof) {
+    if (3 * d.log2 + 1 > 32) return launch_sort<8, 8, uint64_t>(d, st, prof);
     if (rb == 9 && it == 16) return launch_sort<9, 16>(d, st, prof);
     if (rb == 9 && it == 8) return launch_sort<9, 8>(d, st, prof);
     if (rb == 9 && it == 4) return launch_sort<9, 4>(d, st, prof);
@@ -329,9 +331,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     const uint32_t log2 = job.log2;
     if (log2 < 3 || log2 > 20) return fail(PYRB_ERROR_INVALID_ARGUMENT, "log2_size must lie in [3, 20] (got %u)", log2);
     const uint32_t lb = 3 * log2;
-    if (lb + 1 > 32)
-        return fail(PYRB_ERROR_INVALID_ARGUMENT,
-                    "log2_size %u needs 64-bit sort keys; this build sorts 32-bit keys (log2_size <= 10)", log2);
+    const bool key64 = lb + 1 > 32;
     const uint32_t K = job.K;
     const bool chunked = job.mode == kModeChunks || job.mode == kModeChunksEdits || job.mode == kModeBatch;
     // chunks per edge (kModeBatch mixes edges; every other mode has K chunks of edge 2^log2)
@@ -369,9 +369,9 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     const uint32_t n = uint32_t(n64);
     const uint32_t nmax = std::max(n, 1u);
 
-    // tuning
-    const uint32_t rb = g_radix_bits.load();
-    const uint32_t tile_keys = g_tile_keys.load();
+    // tuning (64-bit keys use 8-bit digits and 2048-key tiles)
+    const uint32_t rb = key64 ? 8u : g_radix_bits.load();
+    const uint32_t tile_keys = key64 ? 2048u : g_tile_keys.load();
     const uint32_t it = tile_keys / kBlock;
     const uint32_t lf = g_load_pct.load();
 
@@ -479,8 +479,9 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     ol.size = zero_bytes + ff_bytes;
     const uint64_t o_seg_entry = ol.take(uint64_t(K + 1) * 4);
     const uint64_t o_seg_tile = ol.take(uint64_t(K + 1) * 4);
-    const uint64_t o_k0 = ol.take(uint64_t(nmax) * 4), o_v0 = ol.take(uint64_t(nmax) * 4);
-    const uint64_t o_k1 = ol.take(uint64_t(nmax) * 4), o_v1 = ol.take(uint64_t(nmax) * 4);
+    const uint64_t kbytes = key64 ? 8 : 4;
+    const uint64_t o_k0 = ol.take(uint64_t(nmax) * kbytes), o_v0 = ol.take(uint64_t(nmax) * 4);
+    const uint64_t o_k1 = ol.take(uint64_t(nmax) * kbytes), o_v1 = ol.take(uint64_t(nmax) * 4);
     const uint64_t o_bkey = ol.take(uint64_t(B) * 8), o_bmask = ol.take(uint64_t(B) * 8);
     const uint64_t o_bfirst = ol.take(uint64_t(B) * 4), o_bslot = ol.take(uint64_t(B) * 4);
     // parent record sets: A for even offsets from level 2, B for odd
@@ -528,9 +529,9 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.prim_start = static_cast<uint32_t*>(at(o_prim_start));
     d.seg_entry = static_cast<uint32_t*>(at(o_seg_entry));
     d.seg_tile = static_cast<uint32_t*>(at(o_seg_tile));
-    d.kbuf[0] = static_cast<uint32_t*>(at(o_k0));
+    d.kbuf[0] = at(o_k0);
     d.vbuf[0] = static_cast<uint32_t*>(at(o_v0));
-    d.kbuf[1] = static_cast<uint32_t*>(at(o_k1));
+    d.kbuf[1] = at(o_k1);
     d.vbuf[1] = static_cast<uint32_t*>(at(o_v1));
     d.bkey = static_cast<uint64_t*>(at(o_bkey));
     d.bmask = static_cast<uint64_t*>(at(o_bmask));
@@ -1104,9 +1105,9 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     d.prim_start = static_cast<uint32_t*>(at(o_prim_start));
     d.seg_entry = static_cast<uint32_t*>(at(o_seg_entry));
     d.seg_tile = static_cast<uint32_t*>(at(o_seg_tile));
-    d.kbuf[0] = static_cast<uint32_t*>(at(o_k0));
+    d.kbuf[0] = at(o_k0);
     d.vbuf[0] = static_cast<uint32_t*>(at(o_v0));
-    d.kbuf[1] = static_cast<uint32_t*>(at(o_k1));
+    d.kbuf[1] = at(o_k1);
     d.vbuf[1] = static_cast<uint32_t*>(at(o_v1));
     d.bkey = static_cast<uint64_t*>(at(o_bkey));
     d.bmask = static_cast<uint64_t*>(at(o_bmask));

@@ -79,7 +79,7 @@ struct BuildDesc {
     uint32_t pass_bits[kMaxPasses];
     uint32_t* hist;          // [K][passes][radix]
     uint64_t* sort_status;   // [passes][sort_tiles][radix]
-    uint32_t* kbuf[2];
+    void* kbuf[2];           // sort keys: u32 when 3 * log2 + 1 <= 32 bits, else u64
     uint32_t* vbuf[2];
 
     // unique voxels (outputs)

@@ -94,23 +94,25 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
 // (bit lb), which sorts them behind every valid key of their segment; the
 // unique stage drops them (same rule as gbuild.encode / packChunks).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void encode_voxel(uint4 v, uint32_t log2, uint32_t lb, uint32_t& key, uint32_t& val) {
+template <typename KeyT>
+__device__ __forceinline__ void encode_voxel(uint4 v, uint32_t log2, uint32_t lb, KeyT& key, uint32_t& val) {
     const int32_t n = int32_t(1u << log2);
     int32_t x = int32_t(v.x), y = int32_t(v.y), z = int32_t(v.z);
     if (x < 0 || y < 0 || z < 0 || x >= n || y >= n || z >= n) {
-        key = 1u << lb;
+        key = KeyT(1) << lb;
         val = 0;
     } else {
-        key = uint32_t(voxel_key(uint32_t(x), uint32_t(y), uint32_t(z)));
+        key = KeyT(voxel_key(uint32_t(x), uint32_t(y), uint32_t(z)));
         val = v.w;
     }
 }
 
-__device__ __forceinline__ void load_raw(const BuildDesc& d, uint32_t seg, uint32_t j, uint32_t& key, uint32_t& val) {
+template <typename KeyT>
+__device__ __forceinline__ void load_raw(const BuildDesc& d, uint32_t seg, uint32_t j, KeyT& key, uint32_t& val) {
     switch (d.mode) {
         case kModePlain:
             if (j < d.n_old) {
-                key = uint32_t(__ldg(d.old_keys + j));
+                key = KeyT(__ldg(d.old_keys + j));
                 val = __ldg(d.old_vals + j);
             } else {
                 encode_voxel(__ldg(d.voxels + (j - d.n_old)), d.log2, d.lb, key, val);
@@ -118,7 +120,7 @@ __device__ __forceinline__ void load_raw(const BuildDesc& d, uint32_t seg, uint3
             break;
         case kModeChunks:
             if (j < d.capacity) encode_voxel(__ldg(d.voxels + uint64_t(seg) * d.capacity + j), d.log2, d.lb, key, val);
-            else { key = 1u << d.lb; val = 0; }
+            else { key = KeyT(1) << d.lb; val = 0; }
             break;
         case kModeChunksEdits: {
             uint32_t g = min(__ldg(d.gen_counts + seg), d.capacity);
@@ -141,7 +143,7 @@ __device__ __forceinline__ void load_raw(const BuildDesc& d, uint32_t seg, uint3
             uint32_t x = ((compact3(brick) << 2) | (bit & 3)) >> sh;
             uint32_t y = ((compact3(brick >> 1) << 2) | ((bit >> 2) & 3)) >> sh;
             uint32_t z = ((compact3(brick >> 2) << 2) | (bit >> 4)) >> sh;
-            key = uint32_t(voxel_key(x, y, z));
+            key = KeyT(voxel_key(x, y, z));
             val = __ldg(d.src_vals + j);
             break;
         }
@@ -165,7 +167,7 @@ __device__ __forceinline__ TileSpan tile_span(const BuildDesc& d, uint32_t tile)
 // ---------------------------------------------------------------------------
 // Encode + histogram of every pass ("onesweep" upfront histogram).
 // ---------------------------------------------------------------------------
-template <int RB, int IT>
+template <int RB, int IT, typename KeyT>
 __global__ void __launch_bounds__(kBlock) k_encode_hist(BuildDesc d) {
     constexpr int RADIX = 1 << RB;
     extern __shared__ uint32_t smem[];
@@ -176,23 +178,38 @@ __global__ void __launch_bounds__(kBlock) k_encode_hist(BuildDesc d) {
     for (uint32_t i = threadIdx.x; i < d.passes * RADIX; i += kBlock) hist[i] = 0;
     __syncthreads();
     const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
+    // Each lane counts runs of equal digits of its own items in registers and adds a
+    // run to the shared histogram only when the digit changes (inputs tend to be
+    // spatially coherent, so high digits change rarely).
+    uint32_t run_dig[kMaxPasses], run_cnt[kMaxPasses];
+#pragma unroll
+    for (int p = 0; p < kMaxPasses; ++p) { run_dig[p] = 0xFFFFFFFFu; run_cnt[p] = 0; }
 #pragma unroll 4
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = j * kBlock + threadIdx.x;
-        bool valid = idx < sp.count;
-        uint32_t key = 0, val = 0;
-        if (valid) {
+        if (idx < sp.count) {
+            KeyT key = 0;
+            uint32_t val = 0;
             uint32_t e = sp.start + idx;
             load_raw(d, sp.seg, e - seg_begin, key, val);
-            d.kbuf[0][e] = key;
+            static_cast<KeyT*>(d.kbuf[0])[e] = key;
             d.vbuf[0][e] = val;
-        }
-        for (uint32_t p = 0; p < d.passes; ++p) {
-            uint32_t dig = valid ? (key >> d.pass_shift[p]) & ((1u << d.pass_bits[p]) - 1) : 0xFFFFFFFFu;
-            unsigned peers = __match_any_sync(kFull, dig);
-            if (valid && (threadIdx.x & 31) == unsigned(__ffs(peers) - 1)) atomicAdd(hist + p * RADIX + dig, __popc(peers));
+#pragma unroll
+            for (int p = 0; p < kMaxPasses; ++p) {
+                if (uint32_t(p) >= d.passes) break;
+                const uint32_t dig = uint32_t(key >> d.pass_shift[p]) & ((1u << d.pass_bits[p]) - 1);
+                if (dig != run_dig[p]) {
+                    if (run_cnt[p]) atomicAdd(hist + p * RADIX + run_dig[p], run_cnt[p]);
+                    run_dig[p] = dig;
+                    run_cnt[p] = 0;
+                }
+                ++run_cnt[p];
+            }
         }
     }
+#pragma unroll
+    for (int p = 0; p < kMaxPasses; ++p)
+        if (run_cnt[p]) atomicAdd(hist + p * RADIX + run_dig[p], run_cnt[p]);
     __syncthreads();
     uint32_t* gh = d.hist + uint64_t(sp.seg) * d.passes * RADIX;
     for (uint32_t i = threadIdx.x; i < d.passes * RADIX; i += kBlock) {
@@ -229,17 +246,19 @@ __device__ __forceinline__ void scan_digits(const uint32_t* in, uint32_t* out, u
 // tiles of the segment, staged in shared memory so that the global writes of a
 // digit run are contiguous.
 // ---------------------------------------------------------------------------
-template <int RB, int IT>
+template <int RB, int IT, typename KeyT>
 constexpr size_t sort_smem_bytes() {
     constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
-    constexpr int U = (kWarps * RADIX > 2 * TILE) ? kWarps * RADIX : 2 * TILE;
+    constexpr int KW = int(sizeof(KeyT) / 4);  // words per key
+    constexpr int U = (kWarps * RADIX > (KW + 1) * TILE) ? kWarps * RADIX : (KW + 1) * TILE;
     return size_t(U + 3 * RADIX + 2 * kWarps + 8) * 4;
 }
 
-template <int RB, int IT>
+template <int RB, int IT, typename KeyT>
 __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass, uint32_t src) {
     constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
-    constexpr int U = (kWarps * RADIX > 2 * TILE) ? kWarps * RADIX : 2 * TILE;
+    constexpr int KW = int(sizeof(KeyT) / 4);
+    constexpr int U = (kWarps * RADIX > (KW + 1) * TILE) ? kWarps * RADIX : (KW + 1) * TILE;
     constexpr int DPT = (RADIX + kBlock - 1) / kBlock;
     extern __shared__ uint32_t smem[];
     uint32_t* whist = smem;               // [kWarps][RADIX], later staging keys|vals
@@ -254,9 +273,9 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
     if (tile >= d.seg_tile[d.seg_count]) return;
     const TileSpan sp = tile_span(d, tile);
     const uint32_t shift = d.pass_shift[pass], dmask = (1u << d.pass_bits[pass]) - 1;
-    const uint32_t* kin = d.kbuf[src];
+    const KeyT* kin = static_cast<const KeyT*>(d.kbuf[src]);
     const uint32_t* vin = d.vbuf[src];
-    uint32_t* kout = d.kbuf[src ^ 1];
+    KeyT* kout = static_cast<KeyT*>(d.kbuf[src ^ 1]);
     uint32_t* vout = d.vbuf[src ^ 1];
 
     for (uint32_t i = threadIdx.x; i < uint32_t(kWarps * RADIX); i += kBlock) whist[i] = 0;
@@ -266,7 +285,8 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
     __syncthreads();
     scan_digits<RADIX>(tcnt, gofs, scratch);
 
-    uint32_t keys[IT], vals[IT], rank[IT];
+    KeyT keys[IT];
+    uint32_t vals[IT], rank[IT];
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
@@ -284,7 +304,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
         bool valid = idx < sp.count;
-        uint32_t dig = valid ? (keys[j] >> shift) & dmask : 0xFFFFFFFFu;
+        uint32_t dig = valid ? uint32_t(keys[j] >> shift) & dmask : 0xFFFFFFFFu;
         unsigned peers = __match_any_sync(kFull, dig);
         uint32_t cnt = valid ? wh[dig] : 0;
         rank[j] = cnt + __popc(peers & lt);
@@ -325,13 +345,13 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
         if (idx < sp.count) {
-            uint32_t dig = (keys[j] >> shift) & dmask;
+            uint32_t dig = uint32_t(keys[j] >> shift) & dmask;
             rank[j] += texcl[dig] + wh[dig];
         }
     }
     __syncthreads();
-    uint32_t* sk = whist;
-    uint32_t* sv = whist + TILE;
+    KeyT* sk = reinterpret_cast<KeyT*>(whist);
+    uint32_t* sv = whist + KW * TILE;
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
@@ -344,8 +364,8 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
     const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
     bool oob = false;
     for (uint32_t i = threadIdx.x; i < sp.count; i += kBlock) {
-        uint32_t k = sk[i];
-        uint32_t pos = gofs[(k >> shift) & dmask] + i;
+        KeyT k = sk[i];
+        uint32_t pos = gofs[uint32_t(k >> shift) & dmask] + i;
         if (pos >= seg_begin && pos < seg_end) {
             kout[pos] = k;
             vout[pos] = sv[i];
@@ -362,7 +382,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
 // look-back scan in global (segment-major) order; keys get the segment (chunk)
 // number above bit lb, like packChunks.
 // ---------------------------------------------------------------------------
-template <int IT>
+template <int IT, typename KeyT>
 __global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
@@ -373,12 +393,13 @@ __global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
     if (tile >= ntiles) return;
     const TileSpan sp = tile_span(d, tile);
     const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
-    const uint32_t* keys = d.kbuf[fin];
+    const KeyT* keys = static_cast<const KeyT*>(d.kbuf[fin]);
     const uint32_t* vals = d.vbuf[fin];
-    const uint32_t inv = 1u << d.lb;
+    const KeyT inv = KeyT(1) << d.lb;
     const uint32_t wbase = warp * 32 * IT;
 
-    uint32_t k[IT], v[IT];
+    KeyT k[IT];
+    uint32_t v[IT];
     unsigned keepb[IT];
     uint32_t wcount = 0;
 #pragma unroll
@@ -388,8 +409,8 @@ __global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
         uint32_t e = sp.start + idx;
         k[j] = in ? keys[e] : inv;
         v[j] = in ? vals[e] : 0;
-        uint32_t nk = __shfl_down_sync(kFull, k[j], 1);
-        if (lane == 31 || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~0u;
+        KeyT nk = __shfl_down_sync(kFull, k[j], 1);
+        if (lane == 31 || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~KeyT(0);
         bool last = !in ? false : (e + 1 == seg_end || nk != k[j]);
         bool keep = in && last && !(k[j] & inv) && v[j] != 0;
         keepb[j] = __ballot_sync(kFull, keep);
@@ -413,7 +434,7 @@ __global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
         if ((keepb[j] >> lane) & 1) {
             uint64_t pos = base + run + __popc(keepb[j] & lanemask_lt());
             if (pos < d.n_total) {
-                d.ukey[pos] = segbits | k[j];
+                d.ukey[pos] = segbits | uint64_t(k[j]);
                 d.uval[pos] = v[j];
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);

@@ -174,3 +174,20 @@ def test_invalid_arguments(gb):
     with pytest.raises(PyrbError) as ei:
         gb.downsample(6, 3, 0, 0, 0, 4)
     assert ei.value.code == -1
+
+
+@pytest.mark.parametrize("log2,rt,n", [(11, 7, 60000), (12, 9, 40000), (16, 12, 20000), (20, 3, 3000), (20, 20, 500)])
+def test_large_edges_64bit_keys_match_oracle(gb, log2, rt, n):
+    """Edges 2^11 .. 2^20 need 64-bit sort keys (3*log2 + 1 > 32 bits): sparse clustered
+    points plus outliers and duplicates, bit-exact with the oracle."""
+    rng = np.random.default_rng(log2)
+    side = 1 << log2
+    centers = rng.integers(0, side, (8, 3))
+    pts = (centers[rng.integers(0, 8, n)] + rng.integers(-20, 21, (n, 3))) % side
+    attrs = rng.integers(0, 5, (n, 1))
+    v = np.concatenate([pts, attrs], 1).astype(np.uint32)
+    v = np.concatenate([v, v[:50], np.array([[side, 0, 0, 1], [0xFFFFFFFF, 1, 1, 1], [side - 1, side - 1, side - 1, 7]],
+                                            np.uint32)])
+    g = gb.build(log2, rt, dev(v)).download()
+    o = orc.gb_build(log2, rt, v)
+    assert_same_build(g, o, label=f"log2={log2}")
