@@ -191,3 +191,38 @@ def test_large_edges_64bit_keys_match_oracle(gb, log2, rt, n):
     g = gb.build(log2, rt, dev(v)).download()
     o = orc.gb_build(log2, rt, v)
     assert_same_build(g, o, label=f"log2={log2}")
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_world_edit_overlay_matches_worldedit_then_build_chunks(gb, seed):
+    """World path: generated chunk voxels with each chunk's overlay edits merged by the
+    build (sort-merge, last entry wins) == the reference's worldedit apply/compact/append
+    (src/device/worldedit.zig:26-90) followed by buildChunks, byte for byte. Edit lists
+    name every coordinate at most once per chunk, as World.prepareEdits produces them."""
+    rng = np.random.default_rng(seed)
+    K, log2, cap = 6, 5, 12000
+    n = 1 << log2
+    vox = np.zeros((K * cap, 4), np.uint32)
+    counts = np.zeros(K, np.uint32)
+    edits, eoff = [], [0]
+    for c in range(K):
+        g = wl.mix_chunk(100 + c, log2, seed) if c != 2 else np.zeros((0, 4), np.uint32)
+        g = g[:cap // 2]
+        vox[c * cap:c * cap + len(g)] = g
+        counts[c] = len(g)
+        m = int(rng.integers(0, 400))
+        pos = rng.choice(n ** 3, m, replace=False)
+        for p in pos:
+            a = 0 if rng.integers(2) else int(rng.integers(1, 9))
+            edits.append([p % n, (p // n) % n, p // (n * n), a])
+        eoff.append(len(edits))
+    edits = np.array(edits, np.uint32).reshape(-1, 4)
+    eoff = np.array(eoff, np.uint32)
+    g = gb.build_chunks_edits(log2, 4, K, cap, dev(vox), dev(counts), dev(edits), dev(eoff), int(eoff[-1])).download()
+    ov, oc = orc.we_apply_all(K, cap, vox, counts, edits, eoff)
+    offs = np.concatenate([[0], np.cumsum(oc)]).astype(np.uint32)
+    packed = np.zeros_like(ov)
+    for c in range(K):  # buildChunks reads segment c from voxels[c * cap], filled to oc[c]
+        packed[c * cap:c * cap + oc[c]] = ov[c * cap:c * cap + oc[c]]
+    o = orc.gb_build_chunks(log2, 4, cap, packed, offs)
+    assert_same_build(g, o, chunks=True, label="world overlay")
