@@ -50,10 +50,23 @@ def _env_int(name, default):
         return default
 
 
-def make_input():
+WORKLOAD_BERNOULLI = ("worst-case dedup single build: 1024^3 i.i.d. Bernoulli(0.15) occupancy, material "
+                      "uniform 1..255, +10^6 uniform set/remove edits")
+# name -> (edge log2, rt_log2, description, CPU-baseline sample octant log2 or None for the whole grid)
+SPECS = {
+    "noise256": (8, 7, WORKLOAD, None),
+    "bernoulli1024": (10, 7, WORKLOAD_BERNOULLI, 8),
+}
+
+
+def make_input(name="noise256"):
     from pyrit_b200 import workloads as wl
-    vox = wl.noise_grid(8, 0)
-    ed = wl.noise_edits(8, 0)
+    if name == "bernoulli1024":
+        vox = wl.bernoulli_grid(10, 0)
+        ed = wl.uniform_edits(10, 1_000_000, 0)
+    else:
+        vox = wl.noise_grid(8, 0)
+        ed = wl.noise_edits(8, 0)
     return vox, ed, np.concatenate([vox, ed])
 
 
@@ -66,14 +79,14 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+def committed_traffic(kernel: str, workload: str):
+    """Per-launch DRAM bytes of `kernel` on `workload` from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
         parts = line.strip().strip("|").split("|")
-        if len(parts) >= 3 and parts[0].strip() == kernel:
+        if len(parts) >= 3 and parts[0].strip() == kernel and parts[1].strip().startswith(workload + ":"):
             try:
                 return int(parts[2].strip())
             except ValueError:
@@ -139,13 +152,13 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def cpu_builder_time(vox, ed, reps=1):
+def cpu_builder_time(vox, ed, reps=1, log2=8):
     """Reference CPU builder (oracle restatement) on one core: seconds per build, voxels."""
     from oracle import oracle as orc
     best, n = None, 0
     for _ in range(reps):
         t = time.perf_counter()
-        d = orc.cpu_build_overlay(8, vox, ed)
+        d = orc.cpu_build_overlay(log2, vox, ed)
         dt = time.perf_counter() - t
         best = dt if best is None else min(best, dt)
         n = d.voxel_count
@@ -162,18 +175,31 @@ def run_reference(args):
     rank = _env_int("RANK", 0)
     if rank != 0:
         return 0
-    vox, ed, _ = make_input()
-    # one full build takes ~2-3 s on one core: shrink the per-step sample for long runs
+    full, _, desc, _ = SPECS[args.workload]
+    vox, ed, _ = make_input(args.workload)
+    # one full 256^3 build takes ~1-3 s on one core: shrink the per-step sample for long runs
     runs = args.steps + args.warmup
     log2 = 8 if runs <= 50 else (7 if runs <= 400 else 6)
-    if log2 < 8:
+    log2 = min(log2, full)
+    if log2 < full:
         vox, ed = sub_volume(vox, log2), sub_volume(ed, log2)
+    from concurrent.futures import ThreadPoolExecutor
+
     from oracle import oracle as orc
+
+    # The reference builder is single-threaded; the host's cores each build their own
+    # copy of the sample at once (ctypes releases the GIL), the way independent chunk
+    # builds spread over a CPU.
+    threads = max(1, min(os.cpu_count() or 1, 32))
+    pool = ThreadPoolExecutor(threads)
+
+    def build_one(_):
+        return orc.cpu_build_overlay(log2, vox, ed).voxel_count
 
     def one():
         t = time.perf_counter()
-        d = orc.cpu_build_overlay(log2, vox, ed)
-        return time.perf_counter() - t, d.voxel_count
+        counts = list(pool.map(build_one, range(threads)))
+        return time.perf_counter() - t, counts[0]
 
     for _ in range(args.warmup):
         one()
@@ -181,18 +207,20 @@ def run_reference(args):
     for _ in range(args.steps):
         dt, n = one()
         times.append(dt)
+    pool.shutdown()
     total = sum(times)
-    value = n * len(times) / total
-    sample = ("one full build of the workload per step" if log2 == 8 else
-              "per step the %d^3 octant of the workload (same voxels and edits inside it)" % (1 << log2))
+    value = threads * n * len(times) / total
+    sample = ("per step %d concurrent builds of the whole workload" % threads if log2 == full else
+              "per step %d concurrent builds of the %d^3 octant of the workload (same voxels and edits inside it)"
+              % (threads, 1 << log2))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "log2_size": 8, "sample_log2": log2, "unique_voxels_per_sample": n},
-        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": 1, "kind": "port",
+        "config": {"workload": desc, "log2_size": full, "sample_log2": log2, "unique_voxels_per_sample": n},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": threads, "kind": "port",
                          "sample": sample + ": hash-map edit merge + buildPoints "
-                                   "(src/dag_builder.zig restated in oracle/dag_cpu.cpp), single thread"},
+                                   "(src/dag_builder.zig restated in oracle/dag_cpu.cpp), one build per thread"},
         "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -215,7 +243,8 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
 
-    vox, ed, pts = make_input()
+    LOG2, RT, desc, cpu_sample_log2 = SPECS[args.workload]
+    vox, ed, pts = make_input(args.workload)
     n_in = len(pts)
     dpts = torch.from_numpy(pts.view(np.int32)).cuda()
     host = torch.from_numpy(pts.view(np.int32)).pin_memory()
@@ -227,7 +256,7 @@ def run_ours(args):
 
     def build_async():
         out = native.BuiltC()
-        native.check(L.pyrb_build_async(ctypes.byref(ex), 8, 7, 0, 0, 0, dpts.data_ptr(), n_in,
+        native.check(L.pyrb_build_async(ctypes.byref(ex), LOG2, RT, 0, 0, 0, dpts.data_ptr(), n_in,
                                         ctypes.c_void_p(counts_ptr), ctypes.byref(out)))
         return out
 
@@ -277,7 +306,7 @@ def run_ours(args):
     prof_steps = min(args.steps, 20)
     for s in range(prof_steps):
         flush.fill_(s & 0xFF)
-        b = gpu_build.build(8, 7, dpts, stream=sptr)
+        b = gpu_build.build(LOG2, RT, dpts, stream=sptr)
         ms = (ctypes.c_float * 256)()
         names = ctypes.create_string_buffer(256 * 32)
         k = L.pyrb_profile_read(ms, names, 32, 256)
@@ -289,10 +318,11 @@ def run_ours(args):
     stage_ms = {k: statistics.mean(v) for k, v in stage.items()}
     sort_keys = [k for k in stage_ms if k.startswith("sort_pass")]
     sort_ms = statistics.mean(stage_ms[k] for k in sort_keys)
-    sort_bytes = 16 * n_in
+    key_bytes = 4 if 3 * LOG2 + 1 <= 32 else 8
+    sort_bytes = 2 * (key_bytes + 4) * n_in
     peak, peak_kind = load_peaks()
     achieved = sort_bytes / (sort_ms / 1e3) / 1e9
-    traffic = committed_traffic("k_sort_pass")
+    traffic = committed_traffic("k_sort_pass", args.workload)
 
     # whole-build algorithmic bytes (read input once; write keys+attrs, leaves, nodes, prims)
     alg_bytes = 16 * n_in + 12 * n_u + 8 * o.leaf_count + 4 * o.node_words + 40 * o.prim_count
@@ -306,7 +336,7 @@ def run_ours(args):
     for s in range(e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        b = gpu_build.geometry_build(8, 7, host.numpy().view(np.uint32), stream=sptr)
+        b = gpu_build.geometry_build(LOG2, RT, host.numpy().view(np.uint32), stream=sptr)
         e2e_times.append(time.perf_counter() - t0)
         assert b.voxel_count == n_u
         b.free()
@@ -317,20 +347,32 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        dt, n = cpu_builder_time(vox, ed, reps=1)
+        if cpu_sample_log2 is None:
+            dt, n = cpu_builder_time(vox, ed, reps=1, log2=LOG2)
+            what = "one full build of the same workload"
+        else:
+            dt, n = cpu_builder_time(sub_volume(vox, cpu_sample_log2), sub_volume(ed, cpu_sample_log2), reps=1,
+                                     log2=cpu_sample_log2)
+            what = "one build of the %d^3 octant of the same workload (its voxels and edits)" % (1 << cpu_sample_log2)
         cpu = {"value": n / dt, "unit": "voxels/s", "cores": 1, "kind": "port",
-               "sample": "one full build of the same workload: hash-map edit merge + buildPoints "
+               "sample": what + ": hash-map edit merge + buildPoints "
                          "(src/dag_builder.zig restated in oracle/dag_cpu.cpp), single thread, %.2f s" % dt}
+
+    # dedup ratio per node level: parents formed / unique nodes kept (level 2 = nodes over bricks)
+    dedup = {str(lv): {"parents": int(st.level_parents[lv]), "unique": int(st.level_unique[lv]),
+                       "ratio": (st.level_parents[lv] / st.level_unique[lv]) if st.level_unique[lv] else None}
+             for lv in range(2, LOG2)}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded value noise + edit overlay)",
-            "config": {"workload": WORKLOAD, "log2_size": 8, "entries": n_in, "unique_voxels": n_u,
+            "config": {"workload": desc, "log2_size": LOG2, "rt_log2": RT, "entries": n_in, "unique_voxels": n_u,
                        "bricks": st.brick_count, "leaves": o.leaf_count, "node_words": o.node_words,
                        "prims": o.prim_count, "sort_passes": st.sort_passes, "radix_bits": st.radix_bits,
                        "l2": "flushed between steps (512 MiB write outside the timed events)",
+                       "key_bits": 8 * key_bytes, "dedup_per_level": dedup,
                        "parallelism": "replicas" if world > 1 else "single"},
             "hbm_gbs": hbm_gbs,
             "roofline": {"bound": "hbm", "kernel": "k_sort_pass", "achieved": achieved, "peak": peak,
@@ -497,7 +539,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["noise256", "batched", "served"], default="noise256")
+    ap.add_argument("--workload", choices=["noise256", "bernoulli1024", "batched", "served"], default="noise256")
     ap.add_argument("--rates", type=float, nargs="+", default=[20000.0])
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--max-batch-voxels", type=int, default=64 << 20)

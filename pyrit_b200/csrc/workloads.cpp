@@ -148,6 +148,13 @@ uint64_t wl_bernoulli_grid(uint32_t log2_size, uint32_t seed, uint32_t* out, uin
     return emit_dense(n, cell, out, cap);
 }
 
+void wl_bernoulli_at(uint64_t n, const uint32_t* pts, uint32_t seed, uint32_t* out) {
+    for (uint64_t i = 0; i < n; ++i) {
+        uint64_t h = wl_hash4(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], seed);
+        out[i] = uint32_t(h >> 32) >= 644245094u ? 0u : 1u + uint32_t(uint32_t(h) % 255);
+    }
+}
+
 uint64_t wl_uniform_edits(uint32_t log2_size, uint64_t count, uint32_t seed, uint32_t* out) {
     if (!out) return count;
     uint64_t mask = (uint64_t(1) << log2_size) - 1;

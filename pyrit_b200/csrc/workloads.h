@@ -99,6 +99,8 @@ uint64_t wl_noise_grid(uint32_t log2_size, uint32_t seed, uint32_t* out, uint64_
 uint64_t wl_noise_edits(uint32_t log2_size, uint32_t seed, uint32_t* out, uint64_t cap);
 /* Bernoulli(0.15) grid, material 1..255 */
 uint64_t wl_bernoulli_grid(uint32_t log2_size, uint32_t seed, uint32_t* out, uint64_t cap);
+/* attribute of the Bernoulli grid at pts[n][3] (0 = empty) */
+void wl_bernoulli_at(uint64_t n, const uint32_t* pts, uint32_t seed, uint32_t* out);
 /* n uniform random set/remove edits, material 1..255 (positions may repeat) */
 uint64_t wl_uniform_edits(uint32_t log2_size, uint64_t n, uint32_t seed, uint32_t* out);
 /* chunk edges for the mix: out_log2[k] in {5,6,7,8} */

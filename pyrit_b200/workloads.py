@@ -46,6 +46,8 @@ def lib():
         L.wl_attr_of.restype = u32
         L.wl_poisson_arrivals.argtypes = [u64, ctypes.c_double, u32, p]
         L.wl_poisson_arrivals.restype = None
+        L.wl_bernoulli_at.argtypes = [u64, p, u32, p]
+        L.wl_bernoulli_at.restype = None
         L.wlg_chunk_desc_bytes.restype = u64
         L.wlg_describe.argtypes = [u32, p, u32, u32, p, p, p, ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L.wlg_describe.restype = None
@@ -89,6 +91,15 @@ def noise_edits(log2_size: int = 8, seed: int = 0) -> np.ndarray:
 def bernoulli_grid(log2_size: int = 10, seed: int = 0) -> np.ndarray:
     """Bernoulli(0.15) occupancy, material 1..255 (the 1024^3 worst-case dedup workload)."""
     return _two_phase(lib().wl_bernoulli_grid, log2_size, seed)
+
+
+def bernoulli_at(pts: np.ndarray, seed: int = 0) -> np.ndarray:
+    """Attribute of the Bernoulli grid at cells pts[n, 3] (0 = empty)."""
+    pts = np.ascontiguousarray(pts, dtype=np.uint32)
+    out = np.empty(len(pts), dtype=np.uint32)
+    if len(pts):
+        lib().wl_bernoulli_at(len(pts), pts.ctypes.data, seed, out.ctypes.data)
+    return out
 
 
 def uniform_edits(log2_size: int, count: int, seed: int = 0) -> np.ndarray:
