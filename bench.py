@@ -400,16 +400,26 @@ def run_batched(args, emit=True):
     from pyrit_b200 import autotune, gpu_build, native
     from pyrit_b200 import workloads as wl
 
+    from pyrit_b200 import shard
+
     K = args.chunks
-    local = _env_int("LOCAL_RANK", 0)
+    rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     L = native.lib()
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
     ex = native.Exec()
     ex.stream = ctypes.c_void_p(sptr)
-    log2s = wl.chunk_mix(K, 0)
-    vox, offs = wl.mix_chunks_device(log2s, 0, 0)
+    # weak scaling: a world of world*K chunks, each rank builds its contiguous K
+    lo, hi = shard.chunk_range(world * K, rank, world)
+    log2s = np.ascontiguousarray(wl.chunk_mix(world * K, 0)[lo:hi])
+    vox, offs = wl.mix_chunks_device(log2s, lo, 0)
     total = int(offs[-1])
     d_log2 = torch.from_numpy(log2s.view(np.int32)).cuda()
     d_offs = torch.from_numpy(offs.astype(np.uint32).view(np.int32)).cuda()
@@ -441,6 +451,8 @@ def run_batched(args, emit=True):
     for _ in range(2):
         batched_once()
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     times = []
     for _ in range(args.batched_reps):
         a, b = batched_once()
@@ -470,14 +482,20 @@ def run_batched(args, emit=True):
     a, b = loop_once()
     torch.cuda.synchronize()
     t_loop = a.elapsed_time(b)
-    res = {"chunks": K, "entries": total, "unique_voxels": n_u, "batched_ms": t_batched,
+    comb = shard.combine({"voxels": n_u, "entries": total, "chunks": K, "batched_ms": t_batched, "loop_ms": t_loop})
+    n_u, total, t_batched, t_loop = int(comb["voxels"]), int(comb["entries"]), comb["batched_ms"], comb["loop_ms"]
+    res = {"chunks": int(comb["chunks"]), "entries": total, "unique_voxels": n_u, "batched_ms": t_batched,
            "batched_voxels_per_s": n_u / (t_batched / 1e3), "per_chunk_loop_ms": t_loop,
            "per_chunk_loop_voxels_per_s": n_u / (t_loop / 1e3), "speedup_vs_per_chunk_loop": t_loop / t_batched,
+           "n_gpus": world, "scaling": "weak", "chunks_per_gpu": K,
            "tuning": {k: best[k] for k in ("radix_bits", "tile_keys", "load_factor_pct")},
            "edges": {str(1 << l): int((log2s == l).sum()) for l in (5, 6, 7, 8)}}
-    if emit:
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if emit and rank == 0:
         print(json.dumps({"metric": METRIC + " (batched, 1024 mixed chunks)", "value": res["batched_voxels_per_s"],
-                          "unit": "voxels/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+                          "unit": "voxels/s", "n_gpus": world, "higher_is_better": True, "data": "synthetic",
                           "config": {"workload": "batched build of 1024 chunks of the mix, generated on the device"},
                           "batched": res}), flush=True)
     del vox

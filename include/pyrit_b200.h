@@ -244,6 +244,24 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
                                         uint32_t voxel_capacity, uint64_t prims, uint64_t aabbs,
                                         uint32_t prim_capacity, pyrb_built* out);
 
+/* PYRD v1 bytes of a built DAG: the download + save pair pyr_geometry_download /
+ * pyr_dag_save (src/context.zig:1009-1031, src/root.zig:221-233, format src/io.zig:88-129).
+ * Layout (little-endian): "PYRD", u32 version 1, log2_size, root, flags (bit 0:
+ * attributes), u64 voxel_count (= nodes[root + 1], the root's saturated voxel count,
+ * as the reference's download reads it), node_words, leaf_count, attr_count, then
+ * nodes u32[], leaves u64[], attributes u32[]. Like pyr_dag_save, out == NULL only
+ * sets *size; a buffer smaller than needed returns PYRB_ERROR_INVALID_ARGUMENT.
+ * Copies on the exec's stream and synchronises it. */
+PYRB_API pyrb_result pyrb_pyrd_save(const pyrb_exec* e, const pyrb_built* b, void* out, uint64_t* size);
+
+/* pyr_dag_load (src/root.zig:235-244, io.load src/io.zig:131-160) onto the device: the
+ * header is checked like the reference does (magic, version 1, log2_size in [3, 20],
+ * sizes within `len`, root < node_words, attr_count == voxel_count when attributes are
+ * present; otherwise PYRB_ERROR_INVALID_ARGUMENT "no valid DAG data"), then nodes, leaves
+ * and attributes go into new device buffers of `out` (free with pyrb_built_free);
+ * keys, prims and aabbs stay 0, voxel_count is the header's. */
+PYRB_API pyrb_result pyrb_pyrd_load(const pyrb_exec* e, const void* data, uint64_t len, pyrb_built* out);
+
 /* Library version (major << 16 | minor). */
 PYRB_API uint32_t pyrb_version(void);
 

@@ -926,6 +926,90 @@ PYRB_API void pyrb_get_tuning(pyrb_tuning* t) {
     t->reserved = 0;
 }
 
+// PYRD v1 (src/io.zig:88-129): 52-byte header, then nodes, leaves, attributes.
+constexpr uint64_t kPyrdHeader = 4 + 4 * 4 + 8 * 4;
+
+PYRB_API pyrb_result pyrb_pyrd_save(const pyrb_exec* e, const pyrb_built* b, void* out, uint64_t* size) {
+    if (!b) return fail(PYRB_ERROR_INVALID_ARGUMENT, "built is NULL");
+    if (!size) return fail(PYRB_ERROR_INVALID_ARGUMENT, "size is NULL");
+    if (b->node_words == 0 || b->root + 1 >= b->node_words)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "built has no root node (node_words %u, root %u)", b->node_words, b->root);
+    const uint64_t nw = b->node_words, nl = b->leaf_count, na = b->voxel_count;
+    const uint64_t need = kPyrdHeader + nw * 4 + nl * 8 + na * 4;
+    if (out) {
+        if (*size < need) return fail(PYRB_ERROR_INVALID_ARGUMENT, "buffer too small: %llu bytes needed",
+                                      static_cast<unsigned long long>(need));
+        cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+        uint8_t* o = static_cast<uint8_t*>(out);
+        uint8_t* body = o + kPyrdHeader;
+        CU(cudaMemcpyAsync(body, reinterpret_cast<const void*>(b->nodes), nw * 4, cudaMemcpyDeviceToHost, st));
+        if (nl) CU(cudaMemcpyAsync(body + nw * 4, reinterpret_cast<const void*>(b->leaves), nl * 8, cudaMemcpyDeviceToHost, st));
+        if (na) CU(cudaMemcpyAsync(body + nw * 4 + nl * 8, reinterpret_cast<const void*>(b->attrs), na * 4,
+                                   cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        uint32_t root_count = 0;
+        std::memcpy(&root_count, body + (uint64_t(b->root) + 1) * 4, 4);
+        std::memcpy(o, "PYRD", 4);
+        const uint32_t h32[4] = {1u, b->log2_size, b->root, 1u};
+        const uint64_t h64[4] = {root_count, nw, nl, na};
+        std::memcpy(o + 4, h32, sizeof(h32));
+        std::memcpy(o + 20, h64, sizeof(h64));
+    }
+    *size = need;
+    return PYRB_OK;
+}
+
+PYRB_API pyrb_result pyrb_pyrd_load(const pyrb_exec* e, const void* data, uint64_t len, pyrb_built* out) {
+    if (!out) return fail(PYRB_ERROR_INVALID_ARGUMENT, "out is NULL");
+    std::memset(out, 0, sizeof(*out));
+    if (!data) return fail(PYRB_ERROR_INVALID_ARGUMENT, "data is NULL");
+    const uint8_t* d = static_cast<const uint8_t*>(data);
+    if (len < kPyrdHeader || std::memcmp(d, "PYRD", 4) != 0) return fail(PYRB_ERROR_INVALID_ARGUMENT, "no valid DAG data");
+    uint32_t h32[4];
+    uint64_t h64[4];
+    std::memcpy(h32, d + 4, sizeof(h32));
+    std::memcpy(h64, d + 20, sizeof(h64));
+    const uint32_t version = h32[0], log2 = h32[1], root = h32[2];
+    const bool has_attrs = (h32[3] & 1) != 0;
+    const uint64_t voxel_count = h64[0], nw = h64[1], nl = h64[2], na = h64[3];
+    if (version != 1 || log2 < 3 || log2 > 20) return fail(PYRB_ERROR_INVALID_ARGUMENT, "no valid DAG data");
+    // 32-bit counts in pyrb_built; the overflow-safe size check of io.load
+    if (nw > 0xFFFFFFFFull || nl > 0xFFFFFFFFull || na > 0xFFFFFFFFull)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "no valid DAG data");
+    const uint64_t need = kPyrdHeader + nw * 4 + nl * 8 + na * 4;
+    if (need > len || root >= nw || (has_attrs && na != voxel_count))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "no valid DAG data");
+    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+    Mem mem{e, st};
+    pyrb_built r = {};
+    r.log2_size = log2;
+    r.root = root;
+    r.node_words = uint32_t(nw);
+    r.leaf_count = uint32_t(nl);
+    r.voxel_count = uint32_t(has_attrs ? na : std::min<uint64_t>(voxel_count, 0xFFFFFFFFull));
+    r.nodes = mem.get(nw * 4);
+    r.leaves = nl ? mem.get(nl * 8) : 0;
+    r.attrs = (has_attrs && na) ? mem.get(na * 4) : 0;
+    if (!r.nodes || (nl && !r.leaves) || (has_attrs && na && !r.attrs)) {
+        pyrb_built_free(e, &r);
+        return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for a loaded DAG (%llu bytes)",
+                    static_cast<unsigned long long>(need));
+    }
+    const uint8_t* body = d + kPyrdHeader;
+    cudaError_t err = cudaMemcpyAsync(reinterpret_cast<void*>(r.nodes), body, nw * 4, cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess && nl)
+        err = cudaMemcpyAsync(reinterpret_cast<void*>(r.leaves), body + nw * 4, nl * 8, cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess && r.attrs)
+        err = cudaMemcpyAsync(reinterpret_cast<void*>(r.attrs), body + nw * 4 + nl * 8, na * 4, cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess) {
+        pyrb_built_free(e, &r);
+        return fail(PYRB_ERROR_CUDA, "upload of a loaded DAG: %s", cudaGetErrorString(err));
+    }
+    *out = r;
+    return PYRB_OK;
+}
+
 PYRB_API uint32_t pyrb_version(void) { return (0u << 16) | 1u; }
 
 }  // extern "C"

@@ -66,6 +66,16 @@ class Built:
         except Exception:
             pass
 
+    def save_pyrd(self) -> bytes:
+        """PYRD v1 bytes (pyr_geometry_download + pyr_dag_save; src/io.zig:88-129)."""
+        L = native.lib()
+        ex = _exec(self._stream)
+        size = ctypes.c_uint64(0)
+        native.check(L.pyrb_pyrd_save(ctypes.byref(ex), ctypes.byref(self._c), None, ctypes.byref(size)))
+        buf = np.empty(size.value, dtype=np.uint8)
+        native.check(L.pyrb_pyrd_save(ctypes.byref(ex), ctypes.byref(self._c), buf.ctypes.data, ctypes.byref(size)))
+        return buf.tobytes()
+
     def download(self) -> "HostBuilt":
         """Copies the result to host arrays (synchronous)."""
         from . import _cudart
@@ -86,6 +96,17 @@ class Built:
             aabbs=fetch(c.aabbs, c.prim_count * 6, np.float32),
             roots=self.roots, first_voxel=self.first_voxel, first_prim=self.first_prim,
         )
+
+
+def load_pyrd(data: bytes, stream=None) -> Built:
+    """PYRD v1 bytes onto the device (pyr_dag_load, src/io.zig:131-160): nodes, leaves and
+    attributes in new device buffers. Invalid data raises PyrbError (-1)."""
+    stream = _current_stream() if stream is None else stream
+    buf = np.frombuffer(data, dtype=np.uint8)
+    out = native.BuiltC()
+    native.check(native.lib().pyrb_pyrd_load(ctypes.byref(_exec(stream)), buf.ctypes.data if len(buf) else None,
+                                             len(buf), ctypes.byref(out)))
+    return Built(out, stream)
 
 
 @dataclass

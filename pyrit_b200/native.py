@@ -97,6 +97,9 @@ SIGNATURES = {
     "pyrb_set_tuning": (ctypes.c_int32, [ctypes.POINTER(Tuning)]),
     "pyrb_get_tuning": (None, [ctypes.POINTER(Tuning)]),
     "pyrb_version": (ctypes.c_uint32, []),
+    "pyrb_pyrd_save": (ctypes.c_int32, [ctypes.POINTER(Exec), ctypes.POINTER(BuiltC), _p,
+                                        ctypes.POINTER(ctypes.c_uint64)]),
+    "pyrb_pyrd_load": (ctypes.c_int32, [ctypes.POINTER(Exec), _p, _u64, ctypes.POINTER(BuiltC)]),
     "pyrb_build_noalloc": (ctypes.c_int32, [_p, _u32, _u32, _u64, _u32, _u64, _u32, _u64, _u32, _u64, _u64, _u32,
                                             _u64, _u64, _u32, ctypes.POINTER(BuiltC)]),
 }
