@@ -56,6 +56,8 @@ WORKLOAD_BERNOULLI = ("worst-case dedup single build: 1024^3 i.i.d. Bernoulli(0.
 SPECS = {
     "noise256": (8, 7, WORKLOAD, None),
     "bernoulli1024": (10, 7, WORKLOAD_BERNOULLI, 8),
+    # the same generator at edge 512 (2^17 edits): a case small enough for ncu captures
+    "bernoulli512": (9, 7, WORKLOAD_BERNOULLI.replace("1024^3", "512^3").replace("10^6", "2^17"), 8),
 }
 
 
@@ -64,6 +66,9 @@ def make_input(name="noise256"):
     if name == "bernoulli1024":
         vox = wl.bernoulli_grid(10, 0)
         ed = wl.uniform_edits(10, 1_000_000, 0)
+    elif name == "bernoulli512":
+        vox = wl.bernoulli_grid(9, 0)
+        ed = wl.uniform_edits(9, 1 << 17, 0)
     else:
         vox = wl.noise_grid(8, 0)
         ed = wl.noise_edits(8, 0)
@@ -373,6 +378,7 @@ def run_ours(args):
                        "prims": o.prim_count, "sort_passes": st.sort_passes, "radix_bits": st.radix_bits,
                        "l2": "flushed between steps (512 MiB write outside the timed events)",
                        "key_bits": 8 * key_bytes, "dedup_per_level": dedup,
+                       "scratch_bytes": int(st.scratch_bytes), "output_bytes_bound": int(st.output_bytes),
                        "parallelism": "replicas" if world > 1 else "single"},
             "hbm_gbs": hbm_gbs,
             "roofline": {"bound": "hbm", "kernel": "k_sort_pass", "achieved": achieved, "peak": peak,
@@ -557,7 +563,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["noise256", "bernoulli1024", "batched", "served"], default="noise256")
+    ap.add_argument("--workload", choices=["noise256", "bernoulli1024", "bernoulli512", "batched", "served"], default="noise256")
     ap.add_argument("--rates", type=float, nargs="+", default=[20000.0])
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--max-batch-voxels", type=int, default=64 << 20)

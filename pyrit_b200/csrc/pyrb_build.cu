@@ -295,6 +295,8 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
     });
     k_encode_hist<RB, IT, KeyT><<<d.sort_tiles, kBlock, hist_smem, st>>>(d);
     prof.mark("encode_hist");
+    k_digit_base<RB><<<d.seg_count * d.passes, kBlock, 0, st>>>(d);
+    prof.mark("digit_base");
     for (uint32_t p = 0; p < d.passes; ++p) {
         k_sort_pass<RB, IT, KeyT><<<d.sort_tiles, kBlock, sort_smem, st>>>(d, p, p & 1);
         prof.mark("sort_pass", p);
@@ -610,7 +612,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     prof.mark("plan");
     CUL(cudaGetLastError());
     CUL(launch_sort_any(rb, it, d, st, prof));
-    launches += 2 + passes;
+    launches += 3 + passes;
     k_brick<<<d.brick_tiles, kBlock, 0, st>>>(d);
     prof.mark("brick");
     k_leaf_insert<<<leaf_insert_grid(d), kBlock, 0, st>>>(d);

@@ -241,11 +241,23 @@ __device__ __forceinline__ void scan_digits(const uint32_t* in, uint32_t* out, u
 }
 
 // ---------------------------------------------------------------------------
-// One LSD pass of the onesweep radix sort: stable within the tile (warp-striped
-// items ranked in order with match_any), decoupled look-back per digit across the
-// tiles of the segment, staged in shared memory so that the global writes of a
-// digit run are contiguous.
+// Onesweep radix sort passes.
 // ---------------------------------------------------------------------------
+// Digit bases: the histogram of every (segment, pass) becomes its exclusive prefix
+// in place, once, so that the tiles of the sort passes read their segment's digit
+// starts instead of each scanning the histogram again.
+template <int RB>
+__global__ void __launch_bounds__(kBlock) k_digit_base(BuildDesc d) {
+    constexpr int RADIX = 1 << RB;
+    __shared__ uint32_t s_in[RADIX], s_out[RADIX], s_scratch[2 * kWarps + 4];
+    uint32_t* h = d.hist + uint64_t(blockIdx.x) * RADIX;  // blockIdx.x = seg * passes + pass
+    for (uint32_t i = threadIdx.x; i < uint32_t(RADIX); i += kBlock) s_in[i] = h[i];
+    __syncthreads();
+    scan_digits<RADIX>(s_in, s_out, s_scratch);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < uint32_t(RADIX); i += kBlock) h[i] = s_out[i];
+}
+
 template <int RB, int IT, typename KeyT>
 constexpr size_t sort_smem_bytes() {
     constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
@@ -254,17 +266,32 @@ constexpr size_t sort_smem_bytes() {
     return size_t(U + 3 * RADIX + 2 * kWarps + 8) * 4;
 }
 
+// One LSD pass of the onesweep radix sort over a tile of kBlock * IT entries:
+//  1. keys are loaded warp-striped (a warp owns 32 * IT consecutive entries) and
+//     ranked in input order with match_any against per-warp digit counters;
+//  2. the tile's digit counts are published at once as aggregates for the
+//     decoupled look-back of later tiles, and their exclusive scan gives the
+//     tile-local position of every key, so the keys go to shared memory in digit
+//     order while their registers free up;
+//  3. the values are loaded only now (fewer live registers during ranking, so more
+//     tiles per SM) and their loads overlap the look-back of this tile's digits;
+//  4. each digit's run is written contiguously from shared memory at the segment's
+//     digit base (k_digit_base) + the look-back prefix.
+// 4 resident tiles per SM: caps the pass at 64 registers (the 16-key tiles spill a
+// few words, cheaper than the lost occupancy)
+#ifndef PYRB_SORT_MIN_BLOCKS
+#define PYRB_SORT_MIN_BLOCKS 4
+#endif
 template <int RB, int IT, typename KeyT>
-__global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass, uint32_t src) {
+__global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(BuildDesc d, uint32_t pass, uint32_t src) {
     constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
     constexpr int KW = int(sizeof(KeyT) / 4);
     constexpr int U = (kWarps * RADIX > (KW + 1) * TILE) ? kWarps * RADIX : (KW + 1) * TILE;
-    constexpr int DPT = (RADIX + kBlock - 1) / kBlock;
     extern __shared__ uint32_t smem[];
     uint32_t* whist = smem;               // [kWarps][RADIX], later staging keys|vals
     uint32_t* tcnt = smem + U;            // tile count per digit
     uint32_t* texcl = tcnt + RADIX;       // tile-exclusive digit offsets
-    uint32_t* gofs = texcl + RADIX;       // segment digit start, then global write offset
+    uint32_t* gofs = texcl + RADIX;       // global write offset per digit
     uint32_t* scratch = gofs + RADIX;     // 2*kWarps + 1 words
     uint32_t* s_tile = scratch + 2 * kWarps + 4;
 
@@ -277,27 +304,17 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
     const uint32_t* vin = d.vbuf[src];
     KeyT* kout = static_cast<KeyT*>(d.kbuf[src ^ 1]);
     uint32_t* vout = d.vbuf[src ^ 1];
+    const uint32_t* gbase = d.hist + (uint64_t(sp.seg) * d.passes + pass) * RADIX;
 
     for (uint32_t i = threadIdx.x; i < uint32_t(kWarps * RADIX); i += kBlock) whist[i] = 0;
-    // segment digit starts (exclusive scan of the segment histogram of this pass)
-    const uint32_t* gh = d.hist + (uint64_t(sp.seg) * d.passes + pass) * RADIX;
-    for (uint32_t i = threadIdx.x; i < uint32_t(RADIX); i += kBlock) tcnt[i] = __ldg(gh + i);
-    __syncthreads();
-    scan_digits<RADIX>(tcnt, gofs, scratch);
-
     KeyT keys[IT];
-    uint32_t vals[IT], rank[IT];
+    uint32_t rank[IT];
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
-        if (idx < sp.count) {
-            keys[j] = kin[sp.start + idx];
-            vals[j] = vin[sp.start + idx];
-        } else {
-            keys[j] = 0;
-            vals[j] = 0;
-        }
+        keys[j] = idx < sp.count ? kin[sp.start + idx] : KeyT(0);
     }
+    __syncthreads();
     const unsigned lt = lanemask_lt();
     uint32_t* wh = whist + warp * RADIX;
 #pragma unroll
@@ -313,7 +330,8 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
         __syncwarp();
     }
     __syncthreads();
-    // cross-warp exclusive offsets per digit, tile totals
+    // cross-warp exclusive offsets per digit, tile totals, published at once
+    uint64_t* status = d.sort_status + uint64_t(pass) * d.sort_tiles * RADIX;
     for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
         uint32_t run = 0;
 #pragma unroll
@@ -323,24 +341,12 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
             run += c;
         }
         tcnt[dg] = run;
+        if (tile != sp.first_tile) st_relaxed(status + uint64_t(tile) * RADIX + dg, kFlagAgg | run);
     }
     __syncthreads();
-    // publish the tile's digit counts as early as possible
-    uint64_t* status = d.sort_status + uint64_t(pass) * d.sort_tiles * RADIX;
-    if (tile != sp.first_tile) {
-        for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock)
-            st_relaxed(status + uint64_t(tile) * RADIX + dg, kFlagAgg | tcnt[dg]);
-    }
     scan_digits<RADIX>(tcnt, texcl, scratch);
     __syncthreads();
-    // look-back per digit
-    const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
-    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
-        uint64_t excl = lookback_serial(status + dg, RADIX, tile, sp.first_tile, tcnt[dg], d.counters + kCtrError);
-        gofs[dg] = seg_begin + gofs[dg] + uint32_t(excl) - texcl[dg];
-    }
-    (void)DPT;
-    // final tile-local ranks
+    // tile-local ranks; then keys to shared memory in digit order
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
@@ -355,10 +361,24 @@ __global__ void __launch_bounds__(kBlock) k_sort_pass(BuildDesc d, uint32_t pass
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
-        if (idx < sp.count) {
-            sk[rank[j]] = keys[j];
-            sv[rank[j]] = vals[j];
-        }
+        if (idx < sp.count) sk[rank[j]] = keys[j];
+    }
+    uint32_t vals[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        vals[j] = idx < sp.count ? vin[sp.start + idx] : 0u;
+    }
+    // look-back per digit
+    const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
+    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
+        uint64_t excl = lookback_serial(status + dg, RADIX, tile, sp.first_tile, tcnt[dg], d.counters + kCtrError);
+        gofs[dg] = seg_begin + __ldg(gbase + dg) + uint32_t(excl) - texcl[dg];
+    }
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        if (idx < sp.count) sv[rank[j]] = vals[j];
     }
     __syncthreads();
     const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
