@@ -277,6 +277,8 @@ constexpr size_t sort_smem_bytes() {
 //     tiles per SM) and their loads overlap the look-back of this tile's digits;
 //  4. each digit's run is written contiguously from shared memory at the segment's
 //     digit base (k_digit_base) + the look-back prefix.
+constexpr int kMatchMaxGroups = 16;  // distinct digits per warp above which ballots are cheaper
+
 // 4 resident tiles per SM: caps the pass at 64 registers (the 16-key tiles spill a
 // few words, cheaper than the lost occupancy)
 #ifndef PYRB_SORT_MIN_BLOCKS
@@ -317,12 +319,37 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
     __syncthreads();
     const unsigned lt = lanemask_lt();
     uint32_t* wh = whist + warp * RADIX;
+    // Peer masks first (independent of each other), then the counter chain. match_any
+    // costs grow with the number of distinct digits in the warp; once a warp sees
+    // more than kMatchMaxGroups of them, it switches to RB ballots (one per digit bit),
+    // whose cost is fixed. Both give the same masks.
+    unsigned pm[IT];
+    bool by_bits = false;  // warp-uniform
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        const bool valid = idx < sp.count;
+        const uint32_t dig = valid ? uint32_t(keys[j] >> shift) & dmask : 0xFFFFFFFFu;
+        if (!by_bits) {
+            pm[j] = __match_any_sync(kFull, dig);
+            const unsigned heads = __ballot_sync(kFull, lane == unsigned(__ffs(pm[j]) - 1));
+            by_bits = __popc(heads) > kMatchMaxGroups;
+        } else {
+            unsigned peers = __ballot_sync(kFull, valid);
+#pragma unroll
+            for (int b = 0; b < RB; ++b) {
+                const unsigned bb = __ballot_sync(kFull, (dig >> b) & 1u);
+                peers &= ((dig >> b) & 1u) ? bb : ~bb;
+            }
+            pm[j] = peers;
+        }
+    }
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
         bool valid = idx < sp.count;
         uint32_t dig = valid ? uint32_t(keys[j] >> shift) & dmask : 0xFFFFFFFFu;
-        unsigned peers = __match_any_sync(kFull, dig);
+        const unsigned peers = pm[j];
         uint32_t cnt = valid ? wh[dig] : 0;
         rank[j] = cnt + __popc(peers & lt);
         __syncwarp();
@@ -484,7 +511,11 @@ __device__ __forceinline__ uint32_t leaf_insert(uint4* table, uint32_t cap, uint
         unsigned long long cur = ld_relaxed(reinterpret_cast<const uint64_t*>(kp));
         if (cur == 0) {
             cur = atomicCAS(kp, 0ull, (unsigned long long)mask);
-            if (cur == 0) cur = mask;
+            if (cur == 0) {
+                // first of its mask: claim without waiting (the result is not needed)
+                atomicMax(&table[h].z, ~idx);
+                return h;
+            }
         }
         if (cur == mask) {
             claim_owner(table + h, idx);
@@ -504,10 +535,17 @@ __device__ __forceinline__ uint32_t leaf_insert(uint4* table, uint32_t cap, uint
 constexpr int kBrickIT = 8;
 constexpr int kBrickTile = kBlock * kBrickIT;
 
+// Records of the bricks whose heads lie in a tile are staged in shared memory at
+// tile-local indices, so the look-back for the tile's global brick offset (by warp
+// 0, first) overlaps the mask assembly of the other warps, and the records leave
+// with coalesced stores.
 __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
+    __shared__ uint64_t s_bkey[kBrickTile];
+    __shared__ uint64_t s_bmask[kBrickTile];
+    __shared__ uint32_t s_bfirst[kBrickTile];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = dyn_tile(d.counters, 9, &s_tile);
     const uint32_t U = min(d.counters[kCtrUnique], d.n_total);
@@ -540,9 +578,6 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
         uint64_t ex = lookback_warp(d.brick_status, tile, 0, total, d.counters + kCtrError);
         if (lane == 0) s_base = ex;
     }
-    __syncthreads();
-    const uint32_t wbase = uint32_t(s_base) + wexcl;
-    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrBricks] = uint32_t(s_base + total);
 
     bool c_on = false, c_own = false;
     uint64_t c_brick = 0, c_mask = 0;
@@ -574,7 +609,8 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
             if (lane >= gstart + o) v |= y;
         }
         bool ghead = (hbj >> gstart) & 1;
-        uint32_t idx = ghead ? wbase + hcount + __popc(hbj & ((2u << gstart) - 1)) - 1 : c_idx;
+        // tile-local brick index
+        uint32_t idx = ghead ? wexcl + hcount + __popc(hbj & ((2u << gstart) - 1)) - 1 : c_idx;
         bool own = ghead ? (j < kBrickIT) : (cont && c_own);
         uint32_t first = ghead ? wstart + j * 32 + gstart : c_first;
         const uint64_t next_in_warp = __shfl_down_sync(kFull, bk, 1);  // every lane takes part
@@ -593,13 +629,26 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
         c_first = __shfl_sync(kFull, first, 31);
         hcount += __popc(hbj);
         if (emit) {
-            if (idx < d.brick_bound) {
-                d.bkey[idx] = bk;
-                d.bmask[idx] = v;
-                d.bfirst[idx] = first;
+            if (idx < uint32_t(kBrickTile)) {
+                s_bkey[idx] = bk;
+                s_bmask[idx] = v;
+                s_bfirst[idx] = first;
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);
             }
+        }
+    }
+    __syncthreads();
+    const uint64_t base = s_base;
+    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrBricks] = uint32_t(base + total);
+    for (uint32_t i = threadIdx.x; i < total; i += kBlock) {
+        const uint64_t g = base + i;
+        if (g < d.brick_bound) {
+            d.bkey[g] = s_bkey[i];
+            d.bmask[g] = s_bmask[i];
+            d.bfirst[g] = s_bfirst[i];
+        } else {
+            atomicOr(d.counters + kCtrError, kErrBound);
         }
     }
 }
@@ -701,7 +750,7 @@ __device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, cons
             // release: our words (stored before this call) are visible with the key
             cur = cas_acq_rel32(kp, 0u, par + 1);
             if (cur == 0) {
-                claim_owner(table + h, par);
+                atomicMax(&table[h].z, ~par);  // first of its words: claim without waiting
                 return h;
             }
         }
