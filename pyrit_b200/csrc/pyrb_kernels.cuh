@@ -449,6 +449,7 @@ __global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
     uint32_t v[IT];
     unsigned keepb[IT];
     uint32_t wcount = 0;
+    // all loads first (no shuffle between them), then the run-end tests
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = wbase + j * 32 + lane;
@@ -456,8 +457,17 @@ __global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
         uint32_t e = sp.start + idx;
         k[j] = in ? keys[e] : inv;
         v[j] = in ? vals[e] : 0;
-        KeyT nk = __shfl_down_sync(kFull, k[j], 1);
-        if (lane == 31 || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~KeyT(0);
+    }
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = wbase + j * 32 + lane;
+        bool in = idx < sp.count;
+        uint32_t e = sp.start + idx;
+        // successor key: lane + 1 of this row, lane 0 of the next row (every lane shuffles)
+        const KeyT down = __shfl_down_sync(kFull, k[j], 1);
+        const KeyT row_next = __shfl_sync(kFull, k[j + 1 < IT ? j + 1 : j], 0);
+        KeyT nk = lane < 31 ? down : row_next;
+        if ((lane == 31 && j + 1 == IT) || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~KeyT(0);
         bool last = !in ? false : (e + 1 == seg_end || nk != k[j]);
         bool keep = in && last && !(k[j] & inv) && v[j] != 0;
         keepb[j] = __ballot_sync(kFull, keep);
