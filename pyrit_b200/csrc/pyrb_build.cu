@@ -486,6 +486,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     const uint64_t o_k1 = ol.take(uint64_t(nmax) * kbytes), o_v1 = ol.take(uint64_t(nmax) * 4);
     const uint64_t o_bkey = ol.take(uint64_t(B) * 8), o_bmask = ol.take(uint64_t(B) * 8);
     const uint64_t o_bfirst = ol.take(uint64_t(B) * 4), o_bslot = ol.take(uint64_t(B) * 4);
+    const uint64_t o_bref = ol.take(uint64_t(B) * 4);
     // parent record sets: A for even offsets from level 2, B for odd
     uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
     uint64_t o_set[2][7];
@@ -539,6 +540,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.bmask = static_cast<uint64_t*>(at(o_bmask));
     d.bfirst = static_cast<uint32_t*>(at(o_bfirst));
     d.bslot = static_cast<uint32_t*>(at(o_bslot));
+    d.bref = static_cast<uint32_t*>(at(o_bref));
     d.ukey = reinterpret_cast<uint64_t*>(o_ukey);
     d.uval = reinterpret_cast<uint32_t*>(o_uval);
     d.leaves = reinterpret_cast<uint64_t*>(o_leaves);
@@ -1157,6 +1159,7 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     const uint64_t o_k1 = ol.take(uint64_t(nmax) * 4), o_v1 = ol.take(uint64_t(nmax) * 4);
     const uint64_t o_bkey = ol.take(uint64_t(B) * 8), o_bmask = ol.take(uint64_t(B) * 8);
     const uint64_t o_bfirst = ol.take(uint64_t(B) * 4), o_bslot = ol.take(uint64_t(B) * 4);
+    const uint64_t o_bref = ol.take(uint64_t(B) * 4);
     uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
     uint64_t o_set[2][7];
     for (int s = 0; s < 2; ++s) {
@@ -1199,6 +1202,7 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     d.bmask = static_cast<uint64_t*>(at(o_bmask));
     d.bfirst = static_cast<uint32_t*>(at(o_bfirst));
     d.bslot = static_cast<uint32_t*>(at(o_bslot));
+    d.bref = static_cast<uint32_t*>(at(o_bref));
     d.ukey = reinterpret_cast<uint64_t*>(keys);
     d.uval = reinterpret_cast<uint32_t*>(attrs);
     d.leaves = reinterpret_cast<uint64_t*>(leaves);

@@ -96,6 +96,7 @@ struct BuildDesc {
     uint64_t* bmask;
     uint32_t* bfirst;
     uint32_t* bslot;
+    uint32_t* bref;          // [B] leaf index of an owner brick, kNoRef for the others
     uint4* leaf_table;       // {mask lo, mask hi, ~owner, leaf index}
     uint32_t leaf_cap;
     uint32_t leafown_tiles;
@@ -148,6 +149,7 @@ struct LevelDesc {
 };
 
 constexpr uint32_t kNodeStride = 10;
+constexpr uint32_t kNoRef = 0xFFFFFFFFu;
 
 // The upper levels, once a level has at most kTailMaxChildren children, are built by
 // one CTA (k_tail) that keeps each level's dedup table in shared memory.

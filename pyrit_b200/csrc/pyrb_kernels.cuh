@@ -570,9 +570,13 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
     uint32_t wheads = 0;
     uint64_t prev_last = (wstart > 0 && wstart - 1 < U) ? ukey[wstart - 1] : NONE;
 #pragma unroll
-    for (int j = 0; j < kBrickIT; ++j) {
+    for (int j = 0; j < kBrickIT; ++j) {  // all loads first
         uint32_t e = wstart + j * 32 + lane;
         key[j] = e < U ? ukey[e] : NONE;
+    }
+#pragma unroll
+    for (int j = 0; j < kBrickIT; ++j) {
+        uint32_t e = wstart + j * 32 + lane;
         uint64_t pk = __shfl_up_sync(kFull, key[j], 1);
         if (lane == 0) pk = prev_last;
         prev_last = __shfl_sync(kFull, key[j], 31);
@@ -696,17 +700,23 @@ __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
     if (tile >= ntiles) return;
     const uint32_t wstart = tile * kBrickTile + warp * 32 * kBrickIT;
     unsigned ob[kBrickIT];
-    uint32_t slot[kBrickIT];
+    uint32_t slot[kBrickIT], inv_owner[kBrickIT];
     uint32_t wc = 0;
+    // slots, then all owner words, then the ballots (loads in flight together)
 #pragma unroll
     for (int j = 0; j < kBrickIT; ++j) {
         uint32_t b = wstart + j * 32 + lane;
-        bool own = false;
-        slot[j] = 0;
-        if (b < B) {
-            slot[j] = d.bslot[b];
-            own = ~ld_relaxed32(&d.leaf_table[slot[j]].z) == b;
-        }
+        slot[j] = b < B ? d.bslot[b] : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < kBrickIT; ++j) {
+        uint32_t b = wstart + j * 32 + lane;
+        inv_owner[j] = b < B ? ld_relaxed32(&d.leaf_table[slot[j]].z) : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < kBrickIT; ++j) {
+        uint32_t b = wstart + j * 32 + lane;
+        const bool own = b < B && ~inv_owner[j] == b;
         ob[j] = __ballot_sync(kFull, own);
         wc += __popc(ob[j]);
     }
@@ -723,12 +733,14 @@ __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
 #pragma unroll
     for (int j = 0; j < kBrickIT; ++j) {
         uint32_t b = wstart + j * 32 + lane;
+        uint32_t ref = kNoRef;
         if ((ob[j] >> lane) & 1) {
             uint32_t pos = run + __popc(ob[j] & lanemask_lt());
             if (pos < d.brick_bound) d.leaves[pos] = d.bmask[b];
             else atomicOr(d.counters + kCtrError, kErrBound);
-            d.leaf_table[slot[j]].w = pos;
+            ref = pos;
         }
+        if (b < B) d.bref[b] = ref;
         run += __popc(ob[j]);
     }
     if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrLeaves] = uint32_t(s_base + total);
@@ -787,6 +799,13 @@ __device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, cons
     return 0;
 }
 
+// Leaf index of brick b: its own (it owns its mask) or its mask's owner's, found
+// through the table's owner word (only bricks that repeat a mask take this gather).
+__device__ __forceinline__ uint32_t brick_ref(const BuildDesc& d, uint32_t b) {
+    const uint32_t r = __ldcg(d.bref + b);
+    return r != kNoRef ? r : __ldcg(d.bref + ~__ldcg(&d.leaf_table[__ldcg(d.bslot + b)].z));
+}
+
 // Tile of the node build: kNodeBuildTile children staged in shared memory (plus
 // a halo of up to 7 children of the tile's last parent), heads found with warp
 // ballots, positions by a look-back scan, then every thread builds parents from
@@ -823,12 +842,29 @@ __global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L)
     const uint32_t t0 = tile * kNodeBuildTile;
     const uint32_t own_n = min(uint32_t(kNodeBuildTile), C - t0);
     const uint32_t tn = min(uint32_t(N), C - t0);
-    // stage the children: independent coalesced loads, one gather per child for its reference
+    // stage the children: coalesced loads; references of bricks from the dense
+    // leaf-reference array, of nodes by one gather per child from the level's table
+    // (every slot index loaded before the gathers, so that they are all in flight)
+    constexpr int SPT = (N + kBlock - 1) / kBlock;
+    if (L.lv == 2) {
+        for (uint32_t i = threadIdx.x; i < tn; i += kBlock) sref[i] = brick_ref(d, t0 + i);
+    } else {
+        uint32_t cs[SPT];
+#pragma unroll
+        for (int r = 0; r < SPT; ++r) {
+            const uint32_t i = threadIdx.x + r * kBlock;
+            cs[r] = i < tn ? L.cslot[t0 + i] : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < SPT; ++r) {
+            const uint32_t i = threadIdx.x + r * kBlock;
+            if (i < tn) sref[i] = __ldcg(&L.ctable[cs[r]].w);
+        }
+    }
     for (uint32_t i = threadIdx.x; i < tn; i += kBlock) {
         const uint32_t c = t0 + i;
         skey[i] = L.ckey[c];
         sfirst[i] = L.cfirst[c];
-        sref[i] = __ldcg(&L.ctable[L.cslot[c]].w);
         if (L.lv == 2) {
             const uint64_t m = L.cmask[c];
             scnt[i] = __popcll(m);
@@ -1107,7 +1143,7 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
         for (uint32_t i = tid; i < C; i += kTailThreads) {
             if (lv == 2) {
                 skey[i] = d.bkey[i];
-                sref[i] = __ldcg(&T.ctable0[d.bslot[i]].w);
+                sref[i] = brick_ref(d, i);
                 scnt[i] = __popcll(d.bmask[i]);
             } else {
                 skey[i] = cs.key[i];
