@@ -42,6 +42,25 @@ pyrb_result fail(pyrb_result r, const char* fmt, ...) {
         if (err_ != cudaSuccess) return fail(PYRB_ERROR_CUDA, "%s: %s", #call, cudaGetErrorString(err_)); \
     } while (0)
 
+// Every kernel is launched with programmatic stream serialisation: its blocks may be
+// dispatched while the previous kernel of the stream drains, and each kernel's first
+// statement (grid_dep_wait) holds them until that kernel is complete. This hides the
+// launch gap between the ~16 dependent kernels of a build.
+template <typename... KArgs, typename... Args>
+cudaError_t launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // ---------------------------------------------------------------------------
 // tuning
 // ---------------------------------------------------------------------------
@@ -214,13 +233,13 @@ uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels,
     uint32_t launches = 0;
     for (const LevelDesc& L : levels) {
         if (L.lv >= lv0) break;
-        k_node_build<<<L.build_tiles, kBlock, node_build_smem_bytes(), st>>>(d, L);
+        launch(k_node_build, L.build_tiles, kBlock, node_build_smem_bytes(), st, d, L);
         prof.mark("node_build", L.lv);
-        k_node_own<<<L.own_tiles, kBlock, 0, st>>>(d, L);
+        launch(k_node_own, L.own_tiles, kBlock, 0, st, d, L);
         prof.mark("node_own", L.lv);
         launches += 2;
         if (L.lv + 1 == d.rt_log2) {
-            k_prims<<<std::max((L.parent_bound + kBlock - 1) / kBlock, 1u), kBlock, 0, st>>>(d, L);
+            launch(k_prims, std::max((L.parent_bound + kBlock - 1) / kBlock, 1u), kBlock, 0, st, d, L);
             prof.mark("prims", L.lv);
             ++launches;
         }
@@ -230,10 +249,10 @@ uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels,
         std::call_once(once, [] {
             cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tail_smem_bytes()));
         });
-        k_tail<<<1, kTailThreads, tail_smem_bytes(), st>>>(d, T);
+        launch(k_tail, 1, kTailThreads, tail_smem_bytes(), st, d, T);
         prof.mark("tail", lv0);
     } else {
-        k_finalize<<<1, kBlock, 0, st>>>(d, levels.back());
+        launch(k_finalize, 1, kBlock, 0, st, d, levels.back());
         prof.mark("finalize");
     }
     return launches + 1;
@@ -293,15 +312,15 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
         cudaFuncSetAttribute(k_sort_pass<RB, IT, KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
         cudaFuncSetAttribute(k_sort_pass<RB, IT, KeyT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     });
-    k_encode_hist<RB, IT, KeyT><<<d.sort_tiles, kBlock, hist_smem, st>>>(d);
+    launch(k_encode_hist<RB, IT, KeyT>, d.sort_tiles, kBlock, hist_smem, st, d);
     prof.mark("encode_hist");
-    k_digit_base<RB><<<d.seg_count * d.passes, kBlock, 0, st>>>(d);
+    launch(k_digit_base<RB>, d.seg_count * d.passes, kBlock, 0, st, d);
     prof.mark("digit_base");
     for (uint32_t p = 0; p < d.passes; ++p) {
-        k_sort_pass<RB, IT, KeyT><<<d.sort_tiles, kBlock, sort_smem, st>>>(d, p, p & 1);
+        launch(k_sort_pass<RB, IT, KeyT>, d.sort_tiles, kBlock, sort_smem, st, d, p, p & 1);
         prof.mark("sort_pass", p);
     }
-    k_unique<IT, KeyT><<<d.sort_tiles, kBlock, 0, st>>>(d, d.passes & 1);
+    launch(k_unique<IT, KeyT>, d.sort_tiles, kBlock, 0, st, d, d.passes & 1);
     prof.mark("unique");
     return cudaGetLastError();
 }
@@ -609,23 +628,23 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     CUL(cudaMemsetAsync(at(zero_bytes), 0xFF, ff_bytes, st));
     prof.mark("memset");
     uint32_t launches = 0;
-    k_plan<<<1, 1024, 0, st>>>(d);
+    launch(k_plan, 1, 1024, 0, st, d);
     ++launches;
     prof.mark("plan");
     CUL(cudaGetLastError());
     CUL(launch_sort_any(rb, it, d, st, prof));
     launches += 3 + passes;
-    k_brick<<<d.brick_tiles, kBlock, 0, st>>>(d);
+    launch(k_brick, d.brick_tiles, kBlock, 0, st, d);
     prof.mark("brick");
-    k_leaf_insert<<<leaf_insert_grid(d), kBlock, 0, st>>>(d);
+    launch(k_leaf_insert, leaf_insert_grid(d), kBlock, 0, st, d);
     prof.mark("leaf_insert");
-    k_leaf_own<<<d.leafown_tiles, kBlock, 0, st>>>(d);
+    launch(k_leaf_own, d.leafown_tiles, kBlock, 0, st, d);
     prof.mark("leaf_own");
     launches += 3;
     const uint32_t lv0 = tail_level(log2, B, P);
     launches += launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
     if (job.mode == kModeBatch && min_log2 < log2) {
-        k_batch_roots<<<std::max(std::min((K + 255) / 256, 1024u), 1u), 256, 0, st>>>(d, log2);
+        launch(k_batch_roots, std::max(std::min((K + 255) / 256, 1024u), 1u), 256, 0, st, d, log2);
         prof.mark("batch_roots");
         ++launches;
     }
@@ -1258,12 +1277,12 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     CU(cudaMemsetAsync(at(0), 0, zero_bytes, st));
     CU(cudaMemsetAsync(at(zero_bytes), 0xFF, ff_bytes, st));
     Prof prof(st);
-    k_plan<<<1, 1024, 0, st>>>(d);
+    launch(k_plan, 1, 1024, 0, st, d);
     CU(cudaGetLastError());
     CU((launch_sort<8, 16>(d, st, prof)));
-    k_brick<<<d.brick_tiles, kBlock, 0, st>>>(d);
-    k_leaf_insert<<<leaf_insert_grid(d), kBlock, 0, st>>>(d);
-    k_leaf_own<<<d.leafown_tiles, kBlock, 0, st>>>(d);
+    launch(k_brick, d.brick_tiles, kBlock, 0, st, d);
+    launch(k_leaf_insert, leaf_insert_grid(d), kBlock, 0, st, d);
+    launch(k_leaf_own, d.leafown_tiles, kBlock, 0, st, d);
     const uint32_t lv0 = tail_level(log2, B, P);
     launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
     CU(cudaGetLastError());

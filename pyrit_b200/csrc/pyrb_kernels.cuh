@@ -13,6 +13,11 @@
 
 namespace pyrb {
 
+// Programmatic dependent launch: kernels are launched so that they may start while
+// the previous kernel of the stream drains; this wait (first statement of every
+// kernel) returns once that kernel has completed and its memory is visible.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -41,6 +46,7 @@ __device__ __forceinline__ uint32_t dyn_tile(uint32_t* counters, uint32_t ctr, u
 // Segment plan: first entry and first sort tile of every segment.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
+    grid_dep_wait();
     __shared__ uint32_t s_scan[2][1024];
     __shared__ uint32_t s_carry[2];
     const uint32_t K = d.seg_count;
@@ -169,6 +175,7 @@ __device__ __forceinline__ TileSpan tile_span(const BuildDesc& d, uint32_t tile)
 // ---------------------------------------------------------------------------
 template <int RB, int IT, typename KeyT>
 __global__ void __launch_bounds__(kBlock) k_encode_hist(BuildDesc d) {
+    grid_dep_wait();
     constexpr int RADIX = 1 << RB;
     extern __shared__ uint32_t smem[];
     uint32_t* hist = smem;  // [passes][RADIX]
@@ -248,6 +255,7 @@ __device__ __forceinline__ void scan_digits(const uint32_t* in, uint32_t* out, u
 // starts instead of each scanning the histogram again.
 template <int RB>
 __global__ void __launch_bounds__(kBlock) k_digit_base(BuildDesc d) {
+    grid_dep_wait();
     constexpr int RADIX = 1 << RB;
     __shared__ uint32_t s_in[RADIX], s_out[RADIX], s_scratch[2 * kWarps + 4];
     uint32_t* h = d.hist + uint64_t(blockIdx.x) * RADIX;  // blockIdx.x = seg * passes + pass
@@ -286,6 +294,7 @@ constexpr int kMatchMaxGroups = 16;  // distinct digits per warp above which bal
 #endif
 template <int RB, int IT, typename KeyT>
 __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(BuildDesc d, uint32_t pass, uint32_t src) {
+    grid_dep_wait();
     constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
     constexpr int KW = int(sizeof(KeyT) / 4);
     constexpr int U = (kWarps * RADIX > (KW + 1) * TILE) ? kWarps * RADIX : (KW + 1) * TILE;
@@ -431,6 +440,7 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
 // ---------------------------------------------------------------------------
 template <int IT, typename KeyT>
 __global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
+    grid_dep_wait();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
@@ -550,6 +560,7 @@ constexpr int kBrickTile = kBlock * kBrickIT;
 // 0, first) overlaps the mask assembly of the other warps, and the records leave
 // with coalesced stores.
 __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
+    grid_dep_wait();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
@@ -670,6 +681,7 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
 // Leaf dedup insert, one brick per thread. Equal masks of a warp are collapsed with
 // match_any first: only the lowest brick of each group touches the table.
 __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
+    grid_dep_wait();
     const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
     const unsigned lane = threadIdx.x & 31;
     for (uint32_t base = blockIdx.x * kBlock; base < B; base += gridDim.x * kBlock) {
@@ -690,6 +702,7 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
 // (= first occurrence in Morton order); the table slot records the leaf index.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
+    grid_dep_wait();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
@@ -820,6 +833,7 @@ constexpr size_t node_build_smem_bytes() {
 }
 
 __global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L) {
+    grid_dep_wait();
     extern __shared__ uint64_t smem64[];
     constexpr int N = kNodeBuildTile + kNodeHalo;
     uint64_t* skey = smem64;
@@ -952,6 +966,7 @@ __global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L)
 
 // Owners of level lv get word offsets (scan of their lengths) and write their words.
 __global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
+    grid_dep_wait();
     __shared__ uint32_t s_tile;
     __shared__ uint64_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
@@ -1028,6 +1043,7 @@ __global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
 
 // Empty levels still have to pass the cursor on.
 __global__ void k_level_cursor(BuildDesc d, uint32_t lv) {
+    grid_dep_wait();
     if (threadIdx.x == 0 && d.counters[kCtrParents + lv] == 0) d.counters[kCtrCursor + lv + 1] = d.counters[kCtrCursor + lv];
 }
 
@@ -1037,6 +1053,7 @@ __global__ void k_level_cursor(BuildDesc d, uint32_t lv) {
 // base + hi + 1/256 in f32 (adds in the reference's order, no FMA possible).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_prims(BuildDesc d, LevelDesc L) {
+    grid_dep_wait();
     const uint32_t P = min(d.counters[kCtrParents + L.lv], L.parent_bound);
     const uint32_t local_shift = 3 * (d.log2 - d.rt_log2);
     const uint32_t size = 1u << d.rt_log2;
@@ -1112,6 +1129,7 @@ __device__ __forceinline__ uint32_t tail_scan(uint32_t v, uint32_t* sm, uint32_t
 }
 
 __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) {
+    grid_dep_wait();
     extern __shared__ uint64_t tsm64[];
     uint64_t* skey = tsm64;                                            // children keys
     uint32_t* sref = reinterpret_cast<uint32_t*>(skey + kTailMaxChildren);
@@ -1323,6 +1341,7 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
 // cell, so above its own top level it hangs below single-child nodes (child index
 // 0). Its root is found by descending from the cell's top node.
 __global__ void k_batch_roots(BuildDesc d, uint32_t max_log2) {
+    grid_dep_wait();
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < d.seg_count; c += gridDim.x * blockDim.x) {
         uint32_t node = d.roots[c];
         if (node == 0xFFFFFFFFu) continue;
@@ -1334,6 +1353,7 @@ __global__ void k_batch_roots(BuildDesc d, uint32_t max_log2) {
 
 // Root(s), node word count and the empty geometry (gbuild.zig:607-624).
 __global__ void __launch_bounds__(kBlock) k_finalize(BuildDesc d, LevelDesc top) {
+    grid_dep_wait();
     const uint32_t P = min(d.counters[kCtrParents + top.lv], top.parent_bound);
     if (d.chunked) {
         for (uint32_t i = threadIdx.x; i < P; i += kBlock) {
