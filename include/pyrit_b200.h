@@ -262,6 +262,27 @@ PYRB_API pyrb_result pyrb_pyrd_save(const pyrb_exec* e, const pyrb_built* b, voi
  * keys, prims and aabbs stay 0, voxel_count is the header's. */
 PYRB_API pyrb_result pyrb_pyrd_load(const pyrb_exec* e, const void* data, uint64_t len, pyrb_built* out);
 
+/* Chunk attribute palettes, the chunk-install step after a batch build
+ * (src/device/palette.zig, src/context.zig:1311-1360): chunk c owns the attributes
+ * attrs[first[c] .. first[c+1]) (device u32; first is a host u32[count+1], e.g. the
+ * batch's first_voxel of its non-empty chunks followed by voxel_count).
+ * pyrb_palette_scan: palettes (device u32[count][16]) receives up to 16 distinct
+ * values per chunk in the reference's table order (64 slots, hash v * 0x9E3779B1 ^
+ * h >> 15, linear probing, values inserted in order of first occurrence), padded with
+ * the first value (0 for an empty chunk); counts (host u32[count]) the number of
+ * distinct values, or 0xFFFFFFFF when there are more than 16 (the chunk keeps 32-bit
+ * attributes). The value 0xFFFFFFFF never enters a palette (the reference's table
+ * uses it as its empty marker). Synchronises the exec's stream. */
+PYRB_API pyrb_result pyrb_palette_scan(const pyrb_exec* e, uint64_t attrs, const uint32_t* first, uint32_t count,
+                                       uint64_t palettes, uint32_t* counts);
+/* pyrb_palette_pack: writes chunk c at pool[dst[c] ..] (device u32 pool, host word
+ * offsets dst[count]): for palette chunks the 16 palette words then one 4-bit index
+ * per voxel (the first palette entry equal to its value), 8 per word, low nibble
+ * first; for the others the attributes unchanged. The pool words of chunk c are
+ * 16 + ceil(n/8) or n (context.zig:1345-1352). Synchronises the exec's stream. */
+PYRB_API pyrb_result pyrb_palette_pack(const pyrb_exec* e, uint64_t attrs, const uint32_t* first, uint32_t count,
+                                       uint64_t palettes, const uint32_t* counts, const uint32_t* dst, uint64_t pool);
+
 /* Library version (major << 16 | minor). */
 PYRB_API uint32_t pyrb_version(void);
 

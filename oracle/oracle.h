@@ -119,6 +119,13 @@ uint64_t orc_pyrd_save(uint32_t log2_size, uint32_t root, uint64_t voxel_count, 
 
 void orc_free(void* p);
 
+/* Chunk attribute palettes (src/device/palette.zig), restated in palette_ref.cpp. */
+void orc_palette_scan(const uint32_t* attrs, const uint32_t* first, uint32_t count, uint32_t* palettes,
+                      uint32_t* counts);
+uint64_t orc_palette_words(const uint32_t* first, uint32_t count, const uint32_t* counts, uint32_t* dst);
+void orc_palette_pack(const uint32_t* attrs, const uint32_t* first, uint32_t count, const uint32_t* palettes,
+                      const uint32_t* counts, const uint32_t* dst, uint32_t* pool);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,10 @@ def lib():
         L.orc_pyrd_save.argtypes = [u32, u32, u64, p, u64, p, u64, p, u64, p]
         L.orc_pyrd_save.restype = u64
         L.orc_free.argtypes = [p]
+        L.orc_palette_scan.argtypes = [p, p, u32, p, p]
+        L.orc_palette_words.argtypes = [p, u32, p, p]
+        L.orc_palette_words.restype = u64
+        L.orc_palette_pack.argtypes = [p, p, u32, p, p, p, p]
         _lib = L
     return _lib
 
@@ -313,3 +317,35 @@ def morton(x, y, z) -> int:
 def local_key(x, y, z) -> int:
     """Voxel key: (brick Morton << 6) | x&3 + 4(y&3) + 16(z&3) (src/device/gbuild.zig:98-101)."""
     return (morton(x >> 2, y >> 2, z >> 2) << 6) | ((x & 3) + 4 * (y & 3) + 16 * (z & 3))
+
+
+def palette_scan(attrs, first):
+    """palette.zig scan (src/device/palette.zig:55-104), chunks one after the other:
+    returns (palettes uint32[count, 16], counts uint32[count]; 0xFFFFFFFF = overflow)."""
+    attrs = np.ascontiguousarray(attrs, dtype=np.uint32)
+    first = np.ascontiguousarray(first, dtype=np.uint32)
+    count = len(first) - 1
+    pal = np.zeros((max(count, 1), 16), dtype=np.uint32)
+    counts = np.zeros(max(count, 1), dtype=np.uint32)
+    lib().orc_palette_scan(_ptr(attrs), first.ctypes.data, count, pal.ctypes.data, counts.ctypes.data)
+    return pal[:count], counts[:count]
+
+
+def palette_layout(first, counts):
+    """Word offset of every chunk in the attribute pool and the total (src/context.zig:1345-1352)."""
+    first = np.ascontiguousarray(first, dtype=np.uint32)
+    counts = np.ascontiguousarray(counts, dtype=np.uint32)
+    dst = np.zeros(max(len(counts), 1), dtype=np.uint32)
+    total = int(lib().orc_palette_words(first.ctypes.data, len(counts), counts.ctypes.data, dst.ctypes.data))
+    return dst[:len(counts)], total
+
+
+def palette_pack(attrs, first, palettes, counts, dst, total_words):
+    """palette.zig pack (src/device/palette.zig:107-152) into a fresh pool of total_words."""
+    attrs = np.ascontiguousarray(attrs, dtype=np.uint32)
+    first = np.ascontiguousarray(first, dtype=np.uint32)
+    pool = np.zeros(max(total_words, 1), dtype=np.uint32)
+    lib().orc_palette_pack(_ptr(attrs), first.ctypes.data, len(counts), np.ascontiguousarray(palettes).ctypes.data,
+                           np.ascontiguousarray(counts, dtype=np.uint32).ctypes.data,
+                           np.ascontiguousarray(dst, dtype=np.uint32).ctypes.data, pool.ctypes.data)
+    return pool[:total_words]

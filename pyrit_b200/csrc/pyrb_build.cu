@@ -1033,6 +1033,103 @@ PYRB_API pyrb_result pyrb_pyrd_load(const pyrb_exec* e, const void* data, uint64
     return PYRB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Chunk attribute palettes (src/device/palette.zig, src/context.zig:1311-1360)
+// ---------------------------------------------------------------------------
+namespace {
+// Device copies of the per-chunk host arrays plus the tile plan; freed stream-ordered.
+struct PaletteJob {
+    Mem mem;
+    PaletteDesc p = {};
+    uint64_t blocks[4] = {};
+    uint32_t tiles = 0;
+    pyrb_result setup(const uint32_t* first, uint32_t count) {
+        std::vector<uint32_t> tile_of(count + 1);
+        uint64_t t = 0;
+        for (uint32_t c = 0; c < count; ++c) {
+            if (first[c + 1] < first[c]) return fail(PYRB_ERROR_INVALID_ARGUMENT, "first[%u] > first[%u]", c, c + 1);
+            tile_of[c] = uint32_t(t);
+            // at least one tile: a chunk without voxels still gets its palette words
+            t += std::max<uint64_t>((uint64_t(first[c + 1] - first[c]) + kPalTile - 1) / kPalTile, 1);
+            if (t >= (uint64_t(1) << 31)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many voxels");
+        }
+        tile_of[count] = uint32_t(t);
+        tiles = uint32_t(t);
+        blocks[0] = mem.get(uint64_t(count + 1) * 8);
+        if (!blocks[0]) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the palette plan");
+        uint32_t* dfirst = reinterpret_cast<uint32_t*>(blocks[0]);
+        CU(cudaMemcpyAsync(dfirst, first, uint64_t(count + 1) * 4, cudaMemcpyHostToDevice, mem.st));
+        CU(cudaMemcpyAsync(dfirst + count + 1, tile_of.data(), uint64_t(count + 1) * 4, cudaMemcpyHostToDevice,
+                           mem.st));
+        CU(cudaStreamSynchronize(mem.st));  // the host vector goes out of scope
+        p.first = dfirst;
+        p.tile_of = dfirst + count + 1;
+        p.count = count;
+        return PYRB_OK;
+    }
+    uint32_t* take(int k, uint64_t bytes) {
+        blocks[k] = mem.get(bytes);
+        return reinterpret_cast<uint32_t*>(blocks[k]);
+    }
+    ~PaletteJob() {
+        for (uint64_t b : blocks) mem.put(b);
+    }
+};
+}  // namespace
+
+PYRB_API pyrb_result pyrb_palette_scan(const pyrb_exec* e, uint64_t attrs, const uint32_t* first, uint32_t count,
+                                       uint64_t palettes, uint32_t* counts) {
+    if (!first || !counts || (count && !palettes)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL pointer");
+    if (count == 0) return PYRB_OK;
+    if (first[count] > first[0] && !attrs) return fail(PYRB_ERROR_INVALID_ARGUMENT, "attrs is NULL");
+    PaletteJob j{Mem{e, e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr}};
+    pyrb_result r = j.setup(first, count);
+    if (r != PYRB_OK) return r;
+    const cudaStream_t st = j.mem.st;
+    j.p.attrs = reinterpret_cast<const uint32_t*>(attrs);
+    uint32_t* tab = j.take(1, uint64_t(count) * kPalSlots * 8);
+    uint32_t* small = j.take(2, uint64_t(count) * 8);
+    if (!tab || !small) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the palette tables");
+    j.p.gval = tab;
+    j.p.gfirst = tab + uint64_t(count) * kPalSlots;
+    j.p.gflag = small;
+    j.p.counts = small + count;
+    j.p.palettes = reinterpret_cast<uint32_t*>(palettes);
+    CU(cudaMemsetAsync(tab, 0xFF, uint64_t(count) * kPalSlots * 8, st));
+    CU(cudaMemsetAsync(small, 0, uint64_t(count) * 4, st));
+    launch(k_pal_collect, j.tiles, kBlock, 0, st, j.p);
+    launch(k_pal_layout, (count + kBlock - 1) / kBlock, kBlock, 0, st, j.p);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(counts, j.p.counts, uint64_t(count) * 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    return PYRB_OK;
+}
+
+PYRB_API pyrb_result pyrb_palette_pack(const pyrb_exec* e, uint64_t attrs, const uint32_t* first, uint32_t count,
+                                       uint64_t palettes, const uint32_t* counts, const uint32_t* dst, uint64_t pool) {
+    if (!first || !counts || !dst || (count && (!palettes || !pool)))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL pointer");
+    if (count == 0) return PYRB_OK;
+    if (first[count] > first[0] && !attrs) return fail(PYRB_ERROR_INVALID_ARGUMENT, "attrs is NULL");
+    PaletteJob j{Mem{e, e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr}};
+    pyrb_result r = j.setup(first, count);
+    if (r != PYRB_OK) return r;
+    const cudaStream_t st = j.mem.st;
+    uint32_t* small = j.take(1, uint64_t(count) * 8);
+    if (!small) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the palette plan");
+    CU(cudaMemcpyAsync(small, counts, uint64_t(count) * 4, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(small + count, dst, uint64_t(count) * 4, cudaMemcpyHostToDevice, st));
+    j.p.attrs = reinterpret_cast<const uint32_t*>(attrs);
+    j.p.palettes = reinterpret_cast<uint32_t*>(palettes);
+    j.p.counts = small;
+    j.p.dst = small + count;
+    j.p.pool = reinterpret_cast<uint32_t*>(pool);
+    launch(k_pal_pack, j.tiles, kBlock, 0, st, j.p);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(st));
+    return PYRB_OK;
+}
+
 PYRB_API uint32_t pyrb_version(void) { return (0u << 16) | 1u; }
 
 }  // extern "C"

@@ -1378,4 +1378,179 @@ __global__ void __launch_bounds__(kBlock) k_finalize(BuildDesc d, LevelDesc top)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Chunk attribute palettes (src/device/palette.zig): up to 16 distinct attribute
+// values per chunk and a 4-bit index per voxel instead of 32 bits.
+//
+// The reference runs one CTA per chunk and inserts values into a 64-slot shared
+// table in whatever order its threads arrive; the palette is the table's slot order.
+// Here chunks are cut into tiles of kPalTile voxels over the whole GPU: each tile
+// collects its distinct values with the first voxel index of each (warp match_any,
+// then a shared table), merges them into the chunk's global table (value, first
+// index by atomicMin), and one thread per chunk then inserts the values in order of
+// first occurrence into the reference's 64-slot table (same hash, linear probing)
+// to lay out the palette: the order the reference produces when its inserts arrive
+// in voxel order, which is every order when no two values share a home slot.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kPalSlots = 64, kPalMax = 16, kPalEmpty = 0xFFFFFFFFu, kPalOverflow = 0xFFFFFFFFu;
+constexpr uint32_t kPalTile = 4096;
+
+struct PaletteDesc {
+    const uint32_t* attrs;
+    const uint32_t* first;      // [count + 1]
+    const uint32_t* tile_of;    // [count + 1] first tile of each chunk
+    uint32_t count;
+    uint32_t* gval;             // [count][kPalSlots] values, kPalEmpty = free
+    uint32_t* gfirst;           // [count][kPalSlots] first voxel index (atomicMin)
+    uint32_t* gflag;            // [count] 1 = more than kPalSlots values seen
+    uint32_t* palettes;         // [count][kPalMax]
+    uint32_t* counts;           // [count]
+    const uint32_t* dst;        // [count] word offset in pool
+    uint32_t* pool;
+    uint32_t* err;
+};
+
+__device__ __forceinline__ uint32_t pal_hash(uint32_t v) {  // palette.zig:34-38
+    uint32_t h = v * 0x9E3779B1u;
+    return h ^ (h >> 15);
+}
+
+// Insert (v, idx) into a kPalSlots table (shared or global); returns false when full.
+__device__ __forceinline__ bool pal_insert(uint32_t* vals, uint32_t* firsts, uint32_t v, uint32_t idx) {
+    uint32_t s = pal_hash(v) & (kPalSlots - 1);
+    for (uint32_t probes = 0; probes < kPalSlots; ++probes) {
+        uint32_t cur = atomicAdd(vals + s, 0u);
+        if (cur == kPalEmpty) {
+            cur = atomicCAS(vals + s, kPalEmpty, v);
+            if (cur == kPalEmpty) cur = v;
+        }
+        if (cur == v) {
+            atomicMin(firsts + s, idx);
+            return true;
+        }
+        s = (s + 1) & (kPalSlots - 1);
+    }
+    return false;
+}
+
+__device__ __forceinline__ uint32_t pal_chunk_of(const PaletteDesc& p, uint32_t tile) {
+    return upper_index(p.tile_of, p.count + 1, tile);
+}
+
+__global__ void __launch_bounds__(kBlock) k_pal_collect(PaletteDesc p) {
+    grid_dep_wait();
+    __shared__ uint32_t s_val[kPalSlots], s_first[kPalSlots];
+    __shared__ uint32_t s_full;
+    const uint32_t tile = blockIdx.x;
+    if (tile >= p.tile_of[p.count]) return;
+    const uint32_t c = pal_chunk_of(p, tile);
+    const uint32_t lo = p.first[c] + (tile - p.tile_of[c]) * kPalTile;
+    const uint32_t hi = min(p.first[c + 1], lo + kPalTile);
+    if (threadIdx.x < kPalSlots) {
+        s_val[threadIdx.x] = kPalEmpty;
+        s_first[threadIdx.x] = 0xFFFFFFFFu;
+    }
+    if (threadIdx.x == 0) s_full = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t base = lo; base < hi; base += kBlock) {
+        const uint32_t i = base + threadIdx.x;
+        const bool in = i < hi;
+        const uint32_t v = in ? __ldg(p.attrs + i) : 0u;
+        // one insert per distinct value of the warp, by its lowest lane (smallest index)
+        const unsigned peers = __match_any_sync(kFull, in ? v : kPalEmpty);
+        // (0xFFFFFFFF is the table's empty marker and never enters a palette, as in the reference)
+        if (in && v != kPalEmpty && lane == unsigned(__ffs(peers) - 1)) {
+            if (!pal_insert(s_val, s_first, v, i)) s_full = 1;
+        }
+    }
+    __syncthreads();
+    if (s_full) {
+        if (threadIdx.x == 0) atomicOr(p.gflag + c, 1u);
+        return;
+    }
+    if (threadIdx.x < kPalSlots && s_val[threadIdx.x] != kPalEmpty) {
+        if (!pal_insert(p.gval + uint64_t(c) * kPalSlots, p.gfirst + uint64_t(c) * kPalSlots, s_val[threadIdx.x],
+                        s_first[threadIdx.x]))
+            atomicOr(p.gflag + c, 1u);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_pal_layout(PaletteDesc p) {
+    grid_dep_wait();
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    if (c >= p.count) return;
+    const uint32_t* gv = p.gval + uint64_t(c) * kPalSlots;
+    const uint32_t* gf = p.gfirst + uint64_t(c) * kPalSlots;
+    uint32_t v[kPalMax + 1], f[kPalMax + 1], n = 0;
+    bool over = p.gflag[c] != 0;
+    for (uint32_t s = 0; s < kPalSlots && !over; ++s) {
+        if (gv[s] == kPalEmpty) continue;
+        if (n == kPalMax) { over = true; break; }
+        // insertion by first occurrence
+        uint32_t k = n++;
+        while (k > 0 && f[k - 1] > gf[s]) { v[k] = v[k - 1]; f[k] = f[k - 1]; --k; }
+        v[k] = gv[s];
+        f[k] = gf[s];
+    }
+    if (over) {
+        p.counts[c] = kPalOverflow;
+        return;
+    }
+    // the reference's table with the values inserted in that order
+    uint32_t keys[kPalSlots];
+    for (uint32_t s = 0; s < kPalSlots; ++s) keys[s] = kPalEmpty;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t s = pal_hash(v[k]) & (kPalSlots - 1);
+        while (keys[s] != kPalEmpty) s = (s + 1) & (kPalSlots - 1);
+        keys[s] = v[k];
+    }
+    uint32_t* pal = p.palettes + uint64_t(c) * kPalMax;
+    uint32_t m = 0, p0 = 0;
+    for (uint32_t s = 0; s < kPalSlots; ++s) {
+        if (keys[s] == kPalEmpty) continue;
+        if (m == 0) p0 = keys[s];
+        pal[m++] = keys[s];
+    }
+    for (; m < kPalMax; ++m) pal[m] = n > 0 ? p0 : 0u;
+    p.counts[c] = n;
+}
+
+// palette.zig pack: per tile of a chunk, one thread per output word (8 voxels).
+__global__ void __launch_bounds__(kBlock) k_pal_pack(PaletteDesc p) {
+    grid_dep_wait();
+    __shared__ uint32_t s_pal[kPalMax];
+    const uint32_t tile = blockIdx.x;
+    if (tile >= p.tile_of[p.count]) return;
+    const uint32_t c = pal_chunk_of(p, tile);
+    const uint32_t lo = p.first[c], n = p.first[c + 1] - lo;
+    const uint32_t t0 = (tile - p.tile_of[c]) * kPalTile;  // first voxel of the tile within the chunk
+    const uint32_t t1 = min(n, t0 + kPalTile);
+    uint32_t* out = p.pool + p.dst[c];
+    if (p.counts[c] == kPalOverflow) {
+        for (uint32_t i = t0 + threadIdx.x; i < t1; i += kBlock) out[i] = __ldg(p.attrs + lo + i);
+        return;
+    }
+    if (threadIdx.x < kPalMax) {
+        s_pal[threadIdx.x] = p.palettes[uint64_t(c) * kPalMax + threadIdx.x];
+        if (t0 == 0) out[threadIdx.x] = s_pal[threadIdx.x];
+    }
+    __syncthreads();
+    for (uint32_t w = t0 / 8 + threadIdx.x; w < (t1 + 7) / 8; w += kBlock) {
+        uint32_t word = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < 8; ++j) {
+            const uint32_t i = w * 8 + j;
+            if (i >= n) break;
+            const uint32_t v = __ldg(p.attrs + lo + i);
+            uint32_t idx = 0;
+#pragma unroll
+            for (int q = kPalMax - 1; q >= 0; --q)
+                if (s_pal[q] == v) idx = uint32_t(q);  // the first equal entry
+            word |= idx << (j * 4);
+        }
+        out[kPalMax + w] = word;
+    }
+}
+
 }  // namespace pyrb

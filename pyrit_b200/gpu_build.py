@@ -109,6 +109,45 @@ def load_pyrd(data: bytes, stream=None) -> Built:
     return Built(out, stream)
 
 
+PALETTE_OVERFLOW = 0xFFFFFFFF
+
+
+def palette_scan(attrs, first, stream=None):
+    """Chunk palettes (src/device/palette.zig scan): attrs a device u32 buffer (tensor or
+    address), first host uint32[count+1]. Returns (palettes: int32 CUDA tensor [count, 16]
+    with the u32 values, counts: numpy uint32[count], 0xFFFFFFFF = more than 16 values)."""
+    import torch
+    stream = _current_stream() if stream is None else stream
+    first = np.ascontiguousarray(first, dtype=np.uint32)
+    count = len(first) - 1
+    pal = torch.empty((max(count, 1), 16), dtype=torch.int32, device="cuda")
+    counts = np.zeros(max(count, 1), dtype=np.uint32)
+    native.check(native.lib().pyrb_palette_scan(ctypes.byref(_exec(stream)), _addr(attrs), first.ctypes.data, count,
+                                                pal.data_ptr(), counts.ctypes.data))
+    return pal[:count], counts[:count]
+
+
+def palette_layout(first, counts):
+    """Word offset of every chunk in the attribute pool and the pool words needed
+    (palette chunks: 16 + ceil(n/8), others n; src/context.zig:1345-1352)."""
+    first = np.asarray(first, dtype=np.int64)
+    n = first[1:] - first[:-1]
+    words = np.where(np.asarray(counts) != PALETTE_OVERFLOW, 16 + (n + 7) // 8, n)
+    dst = np.concatenate([[0], np.cumsum(words)[:-1]]).astype(np.uint32) if len(words) else np.zeros(0, np.uint32)
+    return dst, int(words.sum())
+
+
+def palette_pack(attrs, first, palettes, counts, dst, pool, stream=None):
+    """src/device/palette.zig pack into the device u32 pool at the word offsets dst."""
+    stream = _current_stream() if stream is None else stream
+    first = np.ascontiguousarray(first, dtype=np.uint32)
+    counts = np.ascontiguousarray(counts, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    native.check(native.lib().pyrb_palette_pack(ctypes.byref(_exec(stream)), _addr(attrs), first.ctypes.data,
+                                                len(first) - 1, _addr(palettes), counts.ctypes.data, dst.ctypes.data,
+                                                _addr(pool)))
+
+
 @dataclass
 class HostBuilt:
     log2_size: int

@@ -100,6 +100,8 @@ SIGNATURES = {
     "pyrb_pyrd_save": (ctypes.c_int32, [ctypes.POINTER(Exec), ctypes.POINTER(BuiltC), _p,
                                         ctypes.POINTER(ctypes.c_uint64)]),
     "pyrb_pyrd_load": (ctypes.c_int32, [ctypes.POINTER(Exec), _p, _u64, ctypes.POINTER(BuiltC)]),
+    "pyrb_palette_scan": (ctypes.c_int32, [ctypes.POINTER(Exec), _u64, _p, _u32, _u64, _p]),
+    "pyrb_palette_pack": (ctypes.c_int32, [ctypes.POINTER(Exec), _u64, _p, _u32, _u64, _p, _p, _u64]),
     "pyrb_build_noalloc": (ctypes.c_int32, [_p, _u32, _u32, _u64, _u32, _u64, _u32, _u64, _u32, _u64, _u64, _u32,
                                             _u64, _u64, _u32, ctypes.POINTER(BuiltC)]),
 }
