@@ -469,6 +469,38 @@ def run_batched(args, emit=True):
     n_u = o.voxel_count
     t_batched = min(times)
 
+    # chunk install: attribute palettes over the batch (scan + pack), device time
+    bd = batch_desc(K)
+    out = native.BuiltC()
+    native.check(L.pyrb_build_batch(ctypes.byref(ex), ctypes.byref(bd), 5, roots.data_ptr(), first.data_ptr(),
+                                    fprim.data_ptr(), ctypes.byref(out)))
+    rts, fv = roots.numpy().view(np.uint32), first.numpy().view(np.uint32)
+    nz = np.nonzero(rts != 0xFFFFFFFF)[0]
+    pfirst = np.concatenate([fv[nz], [out.voxel_count]]).astype(np.uint32)
+    pal_t, pack_t = [], []
+    for _ in range(3):
+        a, b2, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        pal, pcnt = gpu_build.palette_scan(out.attrs, pfirst, stream=sptr)
+        b2.record(stream)
+        dst, words = gpu_build.palette_layout(pfirst, pcnt)
+        pool = torch.empty(max(words, 1), dtype=torch.int32, device="cuda")
+        b3 = torch.cuda.Event(enable_timing=True)
+        b3.record(stream)
+        gpu_build.palette_pack(out.attrs, pfirst, pal, pcnt, dst, pool, stream=sptr)
+        c2.record(stream)
+        torch.cuda.synchronize()
+        pal_t.append(a.elapsed_time(b2))
+        pack_t.append(b3.elapsed_time(c2))
+        del pool
+    L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(out))
+    n_attr = int(pfirst[-1])
+    palette = {"chunks": int(len(nz)), "palette_chunks": int((pcnt != 0xFFFFFFFF).sum()),
+               "scan_ms": min(pal_t), "pack_ms": min(pack_t), "pool_words": int(words),
+               "attr_words": n_attr, "pool_fraction": words / max(n_attr, 1),
+               "scan_gbs": 4 * n_attr / (min(pal_t) / 1e3) / 1e9,
+               "pack_gbs": (4 * n_attr + 4 * words) / (min(pack_t) / 1e3) / 1e9}
+
     # per-chunk loop of plain builds (asynchronous, one stream)
     def loop_once():
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -493,7 +525,7 @@ def run_batched(args, emit=True):
     res = {"chunks": int(comb["chunks"]), "entries": total, "unique_voxels": n_u, "batched_ms": t_batched,
            "batched_voxels_per_s": n_u / (t_batched / 1e3), "per_chunk_loop_ms": t_loop,
            "per_chunk_loop_voxels_per_s": n_u / (t_loop / 1e3), "speedup_vs_per_chunk_loop": t_loop / t_batched,
-           "n_gpus": world, "scaling": "weak", "chunks_per_gpu": K,
+           "n_gpus": world, "scaling": "weak", "chunks_per_gpu": K, "palette": palette,
            "tuning": {k: best[k] for k in ("radix_bits", "tile_keys", "load_factor_pct")},
            "edges": {str(1 << l): int((log2s == l).sum()) for l in (5, 6, 7, 8)}}
     if dist:
