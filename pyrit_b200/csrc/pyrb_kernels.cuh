@@ -271,8 +271,17 @@ constexpr size_t sort_smem_bytes() {
     constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
     constexpr int KW = int(sizeof(KeyT) / 4);  // words per key
     constexpr int U = (kWarps * RADIX > (KW + 1) * TILE) ? kWarps * RADIX : (KW + 1) * TILE;
-    return size_t(U + 3 * RADIX + 2 * kWarps + 8) * 4;
+    return size_t(U + 3 * RADIX + 2 * kWarps + 8 + TILE) * 4;
 }
+
+// Asynchronous 4-byte global -> shared copies (cp.async): no register holds the value
+// while it is in flight.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // One LSD pass of the onesweep radix sort over a tile of kBlock * IT entries:
 //  1. keys are loaded warp-striped (a warp owns 32 * IT consecutive entries) and
@@ -285,6 +294,10 @@ constexpr size_t sort_smem_bytes() {
 //     tiles per SM) and their loads overlap the look-back of this tile's digits;
 //  4. each digit's run is written contiguously from shared memory at the segment's
 //     digit base (k_digit_base) + the look-back prefix.
+#ifndef PYRB_SORT_WINDOW
+#define PYRB_SORT_WINDOW 4
+#endif
+constexpr int kSortWindow = PYRB_SORT_WINDOW;  // predecessors per look-back round
 constexpr int kMatchMaxGroups = 16;  // distinct digits per warp above which ballots are cheaper
 
 // 4 resident tiles per SM: caps the pass at 64 registers (the 16-key tiles spill a
@@ -305,6 +318,7 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
     uint32_t* gofs = texcl + RADIX;       // global write offset per digit
     uint32_t* scratch = gofs + RADIX;     // 2*kWarps + 1 words
     uint32_t* s_tile = scratch + 2 * kWarps + 4;
+    uint32_t* vland = s_tile + 4;         // [TILE] values in tile order, copied asynchronously
 
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = dyn_tile(d.counters, pass, s_tile);
@@ -325,6 +339,14 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
         keys[j] = idx < sp.count ? kin[sp.start + idx] : KeyT(0);
     }
+    // the values travel to shared memory while the keys are ranked (each thread copies
+    // and later reads the same entries, so its own wait suffices)
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        uint32_t idx = warp * 32 * IT + j * 32 + lane;
+        if (idx < sp.count) cp_async4(vland + idx, vin + sp.start + idx);
+    }
+    cp_async_commit();
     __syncthreads();
     const unsigned lt = lanemask_lt();
     uint32_t* wh = whist + warp * RADIX;
@@ -394,27 +416,21 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
     __syncthreads();
     KeyT* sk = reinterpret_cast<KeyT*>(whist);
     uint32_t* sv = whist + KW * TILE;
+    cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < IT; ++j) {
         uint32_t idx = warp * 32 * IT + j * 32 + lane;
-        if (idx < sp.count) sk[rank[j]] = keys[j];
+        if (idx < sp.count) {
+            sk[rank[j]] = keys[j];
+            sv[rank[j]] = vland[idx];
+        }
     }
-    uint32_t vals[IT];
-#pragma unroll
-    for (int j = 0; j < IT; ++j) {
-        uint32_t idx = warp * 32 * IT + j * 32 + lane;
-        vals[j] = idx < sp.count ? vin[sp.start + idx] : 0u;
-    }
-    // look-back per digit
+    // look-back per digit (the tile's entries are staged: few live registers)
     const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
     for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
-        uint64_t excl = lookback_serial(status + dg, RADIX, tile, sp.first_tile, tcnt[dg], d.counters + kCtrError);
+        uint64_t excl = lookback_window<kSortWindow>(status + dg, RADIX, tile, sp.first_tile, tcnt[dg],
+                                                     d.counters + kCtrError);
         gofs[dg] = seg_begin + __ldg(gbase + dg) + uint32_t(excl) - texcl[dg];
-    }
-#pragma unroll
-    for (int j = 0; j < IT; ++j) {
-        uint32_t idx = warp * 32 * IT + j * 32 + lane;
-        if (idx < sp.count) sv[rank[j]] = vals[j];
     }
     __syncthreads();
     const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
