@@ -443,6 +443,60 @@ def run_ours(args):
     return 0
 
 
+def path_edit_bench(out, roots, first_voxel, first_prim, log2s, nz, per_chunk=32, reps=3):
+    """Path edits over a built batch: `per_chunk` random set/remove edits in every non-empty
+    chunk (one job each), through pyrb_path_edit on pools with an arena above the batch.
+    Times the call (edit ordering on the host, upload, the three kernels, read-back)."""
+    import torch
+    from pyrit_b200 import _cudart, gpu_build, native
+    rng = np.random.default_rng(5)
+    nz = list(nz)
+    counts = np.diff(np.concatenate([first_voxel[nz], [out.voxel_count]]).astype(np.int64))
+    nxt = np.concatenate([first_prim[nz][1:], [out.prim_count]]).astype(np.int64)
+    pcount = nxt - first_prim[nz].astype(np.int64)
+    caps = [per_chunk * ((int(log2s[c]) - 2) * 10 + 4) + 8 for c in nz]
+    nodes = torch.empty(out.node_words + sum(caps), dtype=torch.int32, device="cuda")
+    leaves = torch.empty(out.leaf_count + per_chunk * len(nz), dtype=torch.int64, device="cuda")
+    attrs = torch.empty(out.voxel_count + int(counts.sum()) + per_chunk * len(nz), dtype=torch.int32, device="cuda")
+    _cudart.dtod(nodes.data_ptr(), out.nodes, 4 * out.node_words)
+    _cudart.dtod(leaves.data_ptr(), out.leaves, 8 * out.leaf_count)
+    _cudart.dtod(attrs.data_ptr(), out.attrs, 4 * out.voxel_count)
+    edits = []
+    jobs0 = []
+    npos, lpos, apos = out.node_words, out.leaf_count, out.voxel_count
+    for k, c in enumerate(nz):
+        edge = 1 << int(log2s[c])
+        e = np.empty((per_chunk, 4), np.uint32)
+        e[:, :3] = rng.integers(0, edge, (per_chunk, 3))
+        e[:, 3] = np.where(rng.random(per_chunk) < 0.5, 0, rng.integers(1, 9, per_chunk))
+        j = native.PathEditJob(root=int(roots[c]), log2_size=int(log2s[c]), attr_src=int(first_voxel[c]),
+                               attr_count=int(counts[k]), attr_a=apos, attr_cap=int(counts[k]) + per_chunk,
+                               node_arena=npos, node_cap=caps[k], leaf_arena=lpos, leaf_cap=per_chunk,
+                               edit_first=len(edits), edit_count=per_chunk, rt_log2=5,
+                               prims=out.prims + 16 * int(first_prim[c]) if pcount[k] else 0,
+                               prim_count=int(pcount[k]),
+                               aabbs=out.aabbs + 24 * int(first_prim[c]) if pcount[k] else 0, aabbs_keep=1)
+        jobs0.append(j)
+        edits.extend(e.tolist())
+        npos += caps[k]
+        lpos += per_chunk
+        apos += int(counts[k]) + per_chunk
+    edits = np.array(edits, np.uint32)
+    times, flags = [], None
+    for _ in range(reps):
+        jobs = [native.PathEditJob.from_buffer_copy(j) for j in jobs0]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gpu_build.path_edit(nodes, leaves, attrs, jobs, edits)
+        times.append(time.perf_counter() - t0)
+        flags = np.array([j.out_flags for j in jobs], np.uint32)
+    t = min(times)
+    return {"jobs": len(nz), "edits": int(len(edits)), "attributes_rewritten": int(counts.sum()),
+            "ms": 1e3 * t, "edits_per_s": len(edits) / t,
+            "jobs_rebuild_needed": int(((flags & 0x7) != 0).sum()),
+            "how": "pyrb_path_edit over every chunk of the batch, %d random set/remove edits each" % per_chunk}
+
+
 def run_batched(args, emit=True):
     """1024 chunks of the mix (edges 32/64/128/256 with p .4/.3/.2/.1, heightfield tiled per
     chunk and scaled to the edge, 0..20 spherical caves), generated on the device: one
@@ -538,6 +592,7 @@ def run_batched(args, emit=True):
         pal_t.append(a.elapsed_time(b2))
         pack_t.append(b3.elapsed_time(c2))
         del pool
+    path_edit = path_edit_bench(out, rts, fv, fprim.numpy().view(np.uint32), log2s, nz)
     L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(out))
     n_attr = int(pfirst[-1])
     palette = {"chunks": int(len(nz)), "palette_chunks": int((pcnt != 0xFFFFFFFF).sum()),
@@ -570,7 +625,7 @@ def run_batched(args, emit=True):
     res = {"chunks": int(comb["chunks"]), "entries": total, "unique_voxels": n_u, "batched_ms": t_batched,
            "batched_voxels_per_s": n_u / (t_batched / 1e3), "per_chunk_loop_ms": t_loop,
            "per_chunk_loop_voxels_per_s": n_u / (t_loop / 1e3), "speedup_vs_per_chunk_loop": t_loop / t_batched,
-           "n_gpus": world, "scaling": "weak", "chunks_per_gpu": K, "palette": palette,
+           "n_gpus": world, "scaling": "weak", "chunks_per_gpu": K, "palette": palette, "path_edit": path_edit,
            "tuning": {k: best[k] for k in ("radix_bits", "tile_keys", "load_factor_pct")},
            "edges": {str(1 << l): int((log2s == l).sum()) for l in (5, 6, 7, 8)}}
     if dist:

@@ -283,6 +283,44 @@ PYRB_API pyrb_result pyrb_palette_scan(const pyrb_exec* e, uint64_t attrs, const
 PYRB_API pyrb_result pyrb_palette_pack(const pyrb_exec* e, uint64_t attrs, const uint32_t* first, uint32_t count,
                                        uint64_t palettes, const uint32_t* counts, const uint32_t* dst, uint64_t pool);
 
+/* Path edits (src/device/pathedit.zig; the kernel part of Context.pathEdit,
+ * src/context.zig:1093-1290): set, change or remove voxels of a finished geometry
+ * without rebuilding it. The brick of a change and the nodes above it are written as
+ * copies into an arena above the geometry (everything else stays shared); the
+ * attributes (depth-first order, 32-bit or the palette format) are rewritten from
+ * attr_src into attr_a; RT prims get their new subtree node and attribute rank in
+ * place, and their boxes are recomputed (with aabbs_keep they only grow, to the whole
+ * cell). `nodes`, `leaves`, `attributes` are the device pools (u32, u64, u32) the
+ * job offsets refer to; `edits` is a host array of n_edits {x, y, z, attribute}
+ * (chunk coordinates; attribute 0 removes), job j owning [edit_first, +edit_count),
+ * at most 4096 per job. Each job's edits are applied in order after a stable sort by
+ * brick, as the reference's host does. The caller lays out the arenas and attribute
+ * targets (node_cap >= edits * (levels * 10 + 4) + 8, leaf_cap >= edits, attr target
+ * of attr_count + edits values) and keeps them from overlapping between jobs. The
+ * out_* fields are written back into `jobs`: out_root, out_count (voxels after the
+ * edits) and out_flags (PYRB_PATH_EDIT_*; REBUILD, EMPTY and OVERFLOW mean the job
+ * must be rebuilt instead). Synchronises the exec's stream. */
+#define PYRB_PATH_EDIT_REBUILD  0x1u
+#define PYRB_PATH_EDIT_EMPTY    0x2u
+#define PYRB_PATH_EDIT_OVERFLOW 0x4u
+#define PYRB_PATH_EDIT_GREW     0x8u
+typedef struct pyrb_path_edit_job {  /* the reference's PathEditJob, field for field */
+    uint32_t node_offset, leaf_offset, root, log2_size;
+    uint32_t attr_src, attr_count, attr_a, attr_b, attr_cap;
+    uint32_t palette, pal_src, pal_dst;
+    uint32_t node_arena, node_cap, leaf_arena, leaf_cap;
+    uint32_t edit_first, edit_count, rt_log2, reserved0;
+    uint64_t prims;                 /* device RtPrim[prim_count] (16 B: node, attr_base, cell) or 0 */
+    uint32_t prim_count, reserved1;
+    uint64_t aabbs;                 /* device float[prim_count][6] or 0 */
+    uint32_t aabbs_keep;
+    uint32_t out_root, out_count, out_attr_b, out_flags;
+    uint32_t op, op_rank, op_attr;
+} pyrb_path_edit_job;
+PYRB_API pyrb_result pyrb_path_edit(const pyrb_exec* e, uint64_t nodes, uint64_t leaves, uint64_t attributes,
+                                    pyrb_path_edit_job* jobs, uint32_t count, const uint32_t* edits,
+                                    uint32_t n_edits);
+
 /* Library version (major << 16 | minor). */
 PYRB_API uint32_t pyrb_version(void);
 

@@ -126,6 +126,26 @@ uint64_t orc_palette_words(const uint32_t* first, uint32_t count, const uint32_t
 void orc_palette_pack(const uint32_t* attrs, const uint32_t* first, uint32_t count, const uint32_t* palettes,
                       const uint32_t* counts, const uint32_t* dst, uint32_t* pool);
 
+/* Path edits (src/device/pathedit.zig), restated in pathedit_ref.cpp. The job is
+ * the reference's PathEditJob (src/device/types.zig:613-658) field for field. */
+typedef struct orc_rt_prim { uint32_t node, attr_base; uint64_t cell; } orc_rt_prim;
+typedef struct orc_path_edit_job {
+    uint32_t node_offset, leaf_offset, root, log2_size;
+    uint32_t attr_src, attr_count, attr_a, attr_b, attr_cap;
+    uint32_t palette, pal_src, pal_dst;
+    uint32_t node_arena, node_cap, leaf_arena, leaf_cap;
+    uint32_t edit_first, edit_count, rt_log2, reserved0;
+    uint64_t prims;
+    uint32_t prim_count, reserved1;
+    uint64_t aabbs;
+    uint32_t aabbs_keep;
+    uint32_t out_root, out_count, out_attr_b, out_flags;
+    uint32_t op, op_rank, op_attr;
+} orc_path_edit_job;
+void orc_path_edit_order(const orc_path_edit_job* jobs, uint32_t count, uint32_t (*edits)[4]);
+void orc_path_edit(uint32_t* nodes, uint64_t* leaves, uint32_t* attrs, orc_path_edit_job* jobs, uint32_t count,
+                   uint32_t (*edits)[4]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,8 @@ def lib():
         L.orc_pyrd_save.restype = u64
         L.orc_free.argtypes = [p]
         L.orc_palette_scan.argtypes = [p, p, u32, p, p]
+        L.orc_path_edit_order.argtypes = [p, u32, p]
+        L.orc_path_edit.argtypes = [p, p, p, p, u32, p]
         L.orc_palette_words.argtypes = [p, u32, p, p]
         L.orc_palette_words.restype = u64
         L.orc_palette_pack.argtypes = [p, p, u32, p, p, p, p]
@@ -349,3 +351,41 @@ def palette_pack(attrs, first, palettes, counts, dst, total_words):
                            np.ascontiguousarray(counts, dtype=np.uint32).ctypes.data,
                            np.ascontiguousarray(dst, dtype=np.uint32).ctypes.data, pool.ctypes.data)
     return pool[:total_words]
+
+
+class OrcPathEditJob(ctypes.Structure):
+    """orc_path_edit_job (the reference's PathEditJob, src/device/types.zig:613-658)."""
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "node_offset", "leaf_offset", "root", "log2_size", "attr_src", "attr_count", "attr_a", "attr_b", "attr_cap",
+        "palette", "pal_src", "pal_dst", "node_arena", "node_cap", "leaf_arena", "leaf_cap", "edit_first",
+        "edit_count", "rt_log2", "reserved0")] + [
+        ("prims", ctypes.c_uint64), ("prim_count", ctypes.c_uint32), ("reserved1", ctypes.c_uint32),
+        ("aabbs", ctypes.c_uint64)] + [(n, ctypes.c_uint32) for n in (
+            "aabbs_keep", "out_root", "out_count", "out_attr_b", "out_flags", "op", "op_rank", "op_attr")]
+
+
+def path_edit(nodes, leaves, attrs, jobs, edits, prims=None, aabbs=None):
+    """pathedit.zig restated: edits each job in place on host copies of the pools.
+    jobs: list of dicts of job fields (prims/aabbs are taken as the given host arrays,
+    shared by all jobs with prim offsets in 'prim_first'). Returns (nodes, leaves, attrs,
+    prims, aabbs, jobs as dicts with the out_* fields)."""
+    nodes = np.array(nodes, dtype=np.uint32)
+    leaves = np.array(leaves, dtype=np.uint64)
+    attrs = np.array(attrs, dtype=np.uint32)
+    prims = None if prims is None else np.array(prims, dtype=np.uint8).reshape(-1, 16)
+    aabbs = None if aabbs is None else np.array(aabbs, dtype=np.float32).reshape(-1, 6)
+    e = np.array(edits, dtype=np.uint32).reshape(-1, 4)
+    arr = (OrcPathEditJob * max(len(jobs), 1))()
+    for i, jd in enumerate(jobs):
+        for k, v in jd.items():
+            if k in ("prim_first",):
+                continue
+            setattr(arr[i], k, v)
+        pf = jd.get("prim_first", 0)
+        arr[i].prims = 0 if prims is None or jd.get("prim_count", 0) == 0 else prims.ctypes.data + 16 * pf
+        arr[i].aabbs = 0 if aabbs is None or jd.get("prim_count", 0) == 0 else aabbs.ctypes.data + 24 * pf
+    L = lib()
+    L.orc_path_edit_order(arr, len(jobs), e.ctypes.data)
+    L.orc_path_edit(nodes.ctypes.data, leaves.ctypes.data, attrs.ctypes.data, arr, len(jobs), e.ctypes.data)
+    out = [{f: getattr(arr[i], f) for f, _ in OrcPathEditJob._fields_} for i in range(len(jobs))]
+    return nodes, leaves, attrs, prims, aabbs, out

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 
 CUDA_SOURCES = ["pyrb_build.cu"]
-CUDA_HEADERS = ["pyrb_device.cuh", "pyrb_internal.h", "pyrb_kernels.cuh"]
+CUDA_HEADERS = ["pyrb_device.cuh", "pyrb_internal.h", "pyrb_kernels.cuh", "pyrb_pathedit.cuh"]
 WORKLOAD_SOURCES = ["workloads.cpp", "workloads_gpu.cu"]
 
 NVCC_FLAGS = [

@@ -45,3 +45,10 @@ def htod(dst_addr: int, src_ptr: int, nbytes: int) -> None:
         rc = rt().cudaMemcpy(ctypes.c_void_p(dst_addr), ctypes.c_void_p(src_ptr), nbytes, 1)
         if rc != 0:
             raise RuntimeError(f"cudaMemcpy HtoD failed ({rc})")
+
+
+def dtod(dst_addr: int, src_addr: int, nbytes: int) -> None:
+    if nbytes:
+        rc = rt().cudaMemcpy(ctypes.c_void_p(dst_addr), ctypes.c_void_p(src_addr), nbytes, 3)
+        if rc != 0:
+            raise RuntimeError(f"cudaMemcpy DtoD failed ({rc})")

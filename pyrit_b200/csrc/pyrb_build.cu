@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -17,6 +18,7 @@
 #include "pyrit_b200.h"
 #include "pyrb_internal.h"
 #include "pyrb_kernels.cuh"
+#include "pyrb_pathedit.cuh"
 
 using namespace pyrb;
 
@@ -1128,6 +1130,98 @@ PYRB_API pyrb_result pyrb_palette_pack(const pyrb_exec* e, uint64_t attrs, const
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(st));
     return PYRB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Path edits (src/device/pathedit.zig; host side of Context.pathEdit,
+// src/context.zig:1093-1290, without its pool bookkeeping)
+// ---------------------------------------------------------------------------
+static_assert(sizeof(pyrb_path_edit_job) == sizeof(PathEditJob), "pyrb_path_edit_job layout");
+
+PYRB_API pyrb_result pyrb_path_edit(const pyrb_exec* e, uint64_t nodes, uint64_t leaves, uint64_t attributes,
+                                    pyrb_path_edit_job* jobs, uint32_t count, const uint32_t* edits,
+                                    uint32_t n_edits) {
+    if (count == 0) return PYRB_OK;
+    if (!jobs || !nodes || !leaves || !attributes || (n_edits && !edits))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL pointer");
+    uint32_t max_edits = 1;
+    std::vector<uint32_t> attr_tile(count + 1), prim_tile(count + 1);
+    uint64_t at = 0, pt = 0;
+    for (uint32_t j = 0; j < count; ++j) {
+        const pyrb_path_edit_job& jb = jobs[j];
+        if (jb.edit_count > kPeMaxEdits)
+            return fail(PYRB_ERROR_INVALID_ARGUMENT, "job %u: %u edits (at most %u per job)", j, jb.edit_count,
+                        kPeMaxEdits);
+        if (uint64_t(jb.edit_first) + jb.edit_count > n_edits)
+            return fail(PYRB_ERROR_INVALID_ARGUMENT, "job %u: edits beyond the %u given", j, n_edits);
+        if (jb.log2_size < 3 || jb.log2_size > 20 || jb.rt_log2 < 3 || jb.rt_log2 > jb.log2_size)
+            return fail(PYRB_ERROR_INVALID_ARGUMENT, "job %u: log2_size %u / rt_log2 %u", j, jb.log2_size, jb.rt_log2);
+        if (jb.node_arena < jb.node_offset || jb.leaf_arena < jb.leaf_offset)
+            return fail(PYRB_ERROR_INVALID_ARGUMENT, "job %u: arena below the geometry", j);
+        max_edits = std::max(max_edits, jb.edit_count);
+        attr_tile[j] = uint32_t(at);
+        prim_tile[j] = uint32_t(pt);
+        // attribute slots of the job's target (32-bit values, or 8 indices per word)
+        at += (uint64_t(jb.attr_count) + jb.edit_count + kPeTile - 1) / kPeTile;
+        pt += (uint64_t(jb.prim_count) + kBlock - 1) / kBlock;
+    }
+    attr_tile[count] = uint32_t(at);
+    prim_tile[count] = uint32_t(pt);
+    if (at >= (uint64_t(1) << 31) || pt >= (uint64_t(1) << 31)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many attributes");
+    // Context.pathEdit: each job's edits stably ordered by brick, so that a brick is
+    // one run (one new path per brick rather than per voxel)
+    std::vector<uint32_t> sorted(uint64_t(std::max(n_edits, 1u)) * 4, 0);
+    if (n_edits) std::memcpy(sorted.data(), edits, uint64_t(n_edits) * 16);
+    for (uint32_t j = 0; j < count; ++j) {
+        std::vector<std::array<uint32_t, 4>> v(jobs[j].edit_count);
+        for (uint32_t k = 0; k < jobs[j].edit_count; ++k)
+            std::memcpy(v[k].data(), edits + uint64_t(jobs[j].edit_first + k) * 4, 16);
+        auto key = [](const std::array<uint32_t, 4>& a) {
+            return (uint64_t(a[2] >> 2) << 42) | (uint64_t(a[1] >> 2) << 21) | uint64_t(a[0] >> 2);
+        };
+        std::stable_sort(v.begin(), v.end(), [&](const std::array<uint32_t, 4>& a, const std::array<uint32_t, 4>& b) {
+            return key(a) < key(b);
+        });
+        for (uint32_t k = 0; k < jobs[j].edit_count; ++k)
+            std::memcpy(sorted.data() + uint64_t(jobs[j].edit_first + k) * 4, v[k].data(), 16);
+    }
+    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+    Mem mem{e, st};
+    const uint64_t jobs_bytes = uint64_t(count) * sizeof(PathEditJob);
+    const uint64_t edit_bytes = uint64_t(std::max(n_edits, 1u)) * 16;
+    const uint64_t plan_bytes = uint64_t(count + 1) * 8;
+    const uint64_t block = mem.get(align_up(jobs_bytes, 256) + align_up(edit_bytes, 256) + plan_bytes);
+    if (!block) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the path edits");
+    PathEditDesc p;
+    p.nodes = reinterpret_cast<uint32_t*>(nodes);
+    p.leaves = reinterpret_cast<uint64_t*>(leaves);
+    p.attrs = reinterpret_cast<uint32_t*>(attributes);
+    p.jobs = reinterpret_cast<PathEditJob*>(block);
+    p.edits = reinterpret_cast<uint4*>(block + align_up(jobs_bytes, 256));
+    uint32_t* plan = reinterpret_cast<uint32_t*>(block + align_up(jobs_bytes, 256) + align_up(edit_bytes, 256));
+    p.attr_tile = plan;
+    p.prim_tile = plan + count + 1;
+    p.count = count;
+    auto done = [&](pyrb_result r) {
+        mem.put(block);
+        return r;
+    };
+    cudaError_t err = cudaMemcpyAsync(p.jobs, jobs, jobs_bytes, cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(p.edits, sorted.data(), edit_bytes, cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(plan, attr_tile.data(), uint64_t(count + 1) * 4, cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(plan + count + 1, prim_tile.data(), uint64_t(count + 1) * 4, cudaMemcpyHostToDevice, st);
+    if (err != cudaSuccess) return done(fail(PYRB_ERROR_CUDA, "path edit upload: %s", cudaGetErrorString(err)));
+    const size_t ops_smem = size_t(max_edits) * 16;
+    cudaFuncSetAttribute(k_path_attrs, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPeMaxEdits * 16));
+    launch(k_path_walk, (count + 3) / 4, 128, 0, st, p);
+    if (at) launch(k_path_attrs, uint32_t(at), kBlock, ops_smem, st, p);
+    if (pt) launch(k_path_boxes, uint32_t(pt), kBlock, 0, st, p);
+    err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaMemcpyAsync(jobs, p.jobs, jobs_bytes, cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess) return done(fail(PYRB_ERROR_CUDA, "path edit: %s", cudaGetErrorString(err)));
+    return done(PYRB_OK);
 }
 
 PYRB_API uint32_t pyrb_version(void) { return (0u << 16) | 1u; }

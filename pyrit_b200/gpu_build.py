@@ -148,6 +148,21 @@ def palette_pack(attrs, first, palettes, counts, dst, pool, stream=None):
                                                 _addr(pool)))
 
 
+def path_edit(nodes, leaves, attributes, jobs, edits, stream=None):
+    """Path edits (src/device/pathedit.zig): nodes/leaves/attributes are the device pools
+    (tensors or addresses), jobs a sequence of native.PathEditJob (their out_* fields are
+    filled in), edits a uint32[n, 4] host array {x, y, z, attribute} (attribute 0 removes)."""
+    stream = _current_stream() if stream is None else stream
+    arr = (native.PathEditJob * max(len(jobs), 1))(*jobs)
+    e = np.ascontiguousarray(edits, dtype=np.uint32).reshape(-1, 4)
+    native.check(native.lib().pyrb_path_edit(ctypes.byref(_exec(stream)), _addr(nodes), _addr(leaves),
+                                             _addr(attributes), arr, len(jobs), e.ctypes.data if len(e) else None,
+                                             len(e)))
+    for i in range(len(jobs)):
+        jobs[i] = arr[i]
+    return jobs
+
+
 @dataclass
 class HostBuilt:
     log2_size: int

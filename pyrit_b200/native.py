@@ -67,6 +67,19 @@ class Tuning(ctypes.Structure):
                 ("load_factor_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
+class PathEditJob(ctypes.Structure):
+    """pyrb_path_edit_job (the reference's PathEditJob, src/device/types.zig:613-658)."""
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "node_offset", "leaf_offset", "root", "log2_size", "attr_src", "attr_count", "attr_a", "attr_b", "attr_cap",
+        "palette", "pal_src", "pal_dst", "node_arena", "node_cap", "leaf_arena", "leaf_cap", "edit_first",
+        "edit_count", "rt_log2", "reserved0")] + [
+        ("prims", ctypes.c_uint64), ("prim_count", ctypes.c_uint32), ("reserved1", ctypes.c_uint32),
+        ("aabbs", ctypes.c_uint64)] + [(n, ctypes.c_uint32) for n in (
+            "aabbs_keep", "out_root", "out_count", "out_attr_b", "out_flags", "op", "op_rank", "op_attr")]
+
+
+PATH_EDIT_REBUILD, PATH_EDIT_EMPTY, PATH_EDIT_OVERFLOW, PATH_EDIT_GREW = 0x1, 0x2, 0x4, 0x8
+
 # name -> (restype, argtypes); every symbol declared in include/pyrit_b200.h
 _u32, _u64, _p = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
 _pu32 = ctypes.POINTER(ctypes.c_uint32)
@@ -101,6 +114,8 @@ SIGNATURES = {
                                         ctypes.POINTER(ctypes.c_uint64)]),
     "pyrb_pyrd_load": (ctypes.c_int32, [ctypes.POINTER(Exec), _p, _u64, ctypes.POINTER(BuiltC)]),
     "pyrb_palette_scan": (ctypes.c_int32, [ctypes.POINTER(Exec), _u64, _p, _u32, _u64, _p]),
+    "pyrb_path_edit": (ctypes.c_int32, [ctypes.POINTER(Exec), _u64, _u64, _u64, ctypes.POINTER(PathEditJob), _u32,
+                                        _p, _u32]),
     "pyrb_palette_pack": (ctypes.c_int32, [ctypes.POINTER(Exec), _u64, _p, _u32, _u64, _p, _p, _u64]),
     "pyrb_build_noalloc": (ctypes.c_int32, [_p, _u32, _u32, _u64, _u32, _u64, _u32, _u64, _u32, _u64, _u64, _u32,
                                             _u64, _u64, _u32, ctypes.POINTER(BuiltC)]),
