@@ -444,7 +444,9 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
 // number above bit lb, like packChunks.
 // ---------------------------------------------------------------------------
 template <int IT, typename KeyT>
-__global__ void __launch_bounds__(kBlock) k_unique(BuildDesc d, uint32_t fin) {
+// 5 tiles per SM (48 registers): the tile mostly waits for its predecessors' counts,
+// so more tiles in flight per SM measured 17 % faster than 4 at 64 registers
+__global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin) {
     grid_dep_wait();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
