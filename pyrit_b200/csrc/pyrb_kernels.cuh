@@ -594,12 +594,13 @@ constexpr int kBrickTile = kBlock * kBrickIT;
 // tile-local indices, so the look-back for the tile's global brick offset (by warp
 // 0, first) overlaps the mask assembly of the other warps, and the records leave
 // with coalesced stores.
-__global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
+// 6 tiles per SM (40 registers, 24 KB of staging: brick keys are re-read from the
+// unique keys at write-out): the tile mostly waits for its predecessors' counts
+__global__ void __launch_bounds__(kBlock, 6) k_brick(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
-    __shared__ uint64_t s_bkey[kBrickTile];
     __shared__ uint64_t s_bmask[kBrickTile];
     __shared__ uint32_t s_bfirst[kBrickTile];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -690,7 +691,6 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
         hcount += __popc(hbj);
         if (emit) {
             if (idx < uint32_t(kBrickTile)) {
-                s_bkey[idx] = bk;
                 s_bmask[idx] = v;
                 s_bfirst[idx] = first;
             } else {
@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(kBlock) k_brick(BuildDesc d) {
     for (uint32_t i = threadIdx.x; i < total; i += kBlock) {
         const uint64_t g = base + i;
         if (g < d.brick_bound) {
-            d.bkey[g] = s_bkey[i];
+            d.bkey[g] = __ldg(ukey + s_bfirst[i]) >> 6;
             d.bmask[g] = s_bmask[i];
             d.bfirst[g] = s_bfirst[i];
         } else {
