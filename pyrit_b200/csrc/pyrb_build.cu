@@ -235,7 +235,7 @@ uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels,
     uint32_t launches = 0;
     for (const LevelDesc& L : levels) {
         if (L.lv >= lv0) break;
-        launch(k_node_build, L.build_tiles, kBlock, node_build_smem_bytes(), st, d, L);
+        launch(k_node_build, L.build_tiles, kBlock, node_build_smem_bytes(L.lv == 2), st, d, L);
         prof.mark("node_build", L.lv);
         launch(k_node_own, L.own_tiles, kBlock, 0, st, d, L);
         prof.mark("node_own", L.lv);

@@ -867,17 +867,20 @@ constexpr int kNodeTile = kBlock * kNodeIT;     // tile of the node-owner kernel
 constexpr int kNBIT = 4;
 constexpr int kNodeBuildTile = kBlock * kNBIT;  // children per node-build tile
 constexpr int kNodeHalo = 8;
-constexpr size_t node_build_smem_bytes() {
-    return size_t(kNodeBuildTile + kNodeHalo) * (8 + 8 + 8 + 4 + 4 + 4) + size_t(kNodeBuildTile) * 4 + 64;
+// Level 2 stages the children's brick masks (its parents' boxes come from them) rather
+// than their boxes: 28 instead of 36 bytes per child, 6 tiles per SM instead of 5.
+constexpr size_t node_build_smem_bytes(bool bricks) {
+    return size_t(kNodeBuildTile + kNodeHalo) * (bricks ? 8 + 8 + 4 + 4 + 4 : 8 + 8 + 8 + 4 + 4 + 4) +
+           size_t(kNodeBuildTile) * 4 + 64;
 }
 
-__global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L) {
+__global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc L) {
     grid_dep_wait();
     extern __shared__ uint64_t smem64[];
     constexpr int N = kNodeBuildTile + kNodeHalo;
     uint64_t* skey = smem64;
-    uint64_t* slo = skey + N;
-    uint64_t* shi = slo + N;
+    uint64_t* slo = skey + N;                        // level 2: the brick masks
+    uint64_t* shi = L.lv == 2 ? slo : slo + N;
     uint32_t* sref = reinterpret_cast<uint32_t*>(shi + N);
     uint32_t* scnt = sref + N;
     uint32_t* sfirst = scnt + N;
@@ -921,7 +924,7 @@ __global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L)
         if (L.lv == 2) {
             const uint64_t m = L.cmask[c];
             scnt[i] = __popcll(m);
-            if (L.need_box) brick_box(m, slo[i], shi[i]);
+            if (L.need_box) slo[i] = m;
         } else {
             scnt[i] = L.ccnt[c];
             if (L.need_box) { slo[i] = L.clo[c]; shi[i] = L.chi[c]; }
@@ -977,7 +980,8 @@ __global__ void __launch_bounds__(kBlock) k_node_build(BuildDesc d, LevelDesc L)
             if (L.need_box) {
                 const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
                                oz = (idx >> 2) * child_size;
-                const uint64_t clo = slo[j], chi = shi[j];
+                uint64_t clo = slo[j], chi = shi[j];
+                if (L.lv == 2) brick_box(slo[j], clo, chi);
                 lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
                 lo[1] = min(lo[1], cell_y(clo) + oy); hi[1] = max(hi[1], cell_y(chi) + oy);
                 lo[2] = min(lo[2], cell_z(clo) + oz); hi[2] = max(hi[2], cell_z(chi) + oz);
