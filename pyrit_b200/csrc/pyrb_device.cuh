@@ -112,8 +112,8 @@ __device__ __forceinline__ uint32_t cas_acq_rel32(uint32_t* p, uint32_t cmp, uin
 // predecessors per round: the W status loads are independent and in flight
 // together. With hundreds of tiles in flight the nearest inclusive prefix is
 // typically ~16 tiles back (measured at 1024^3), so a serial walk costs ~16 load
-// latencies; wide windows cost status traffic (W x 8 B per digit per round), and
-// W = 4 measured best. Tiles [first, tile) precede `tile`; status[first - 1]
+// latencies; wide windows cost status traffic (W x 8 B per digit per round) and
+// registers: W = 2 measured best (1, 2, 3, 4, 8 and 16 tried). Tiles [first, tile) precede `tile`; status[first - 1]
 // is never read. Returns the exclusive prefix and publishes the inclusive one; a
 // predecessor that never publishes is waited for at most kSpinLimit polls, then
 // err bit 0 is set.

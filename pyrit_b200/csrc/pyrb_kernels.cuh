@@ -284,7 +284,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //  4. each digit's run is written contiguously from shared memory at the segment's
 //     digit base (k_digit_base) + the look-back prefix.
 #ifndef PYRB_SORT_WINDOW
-#define PYRB_SORT_WINDOW 4
+#define PYRB_SORT_WINDOW 2
 #endif
 constexpr int kSortWindow = PYRB_SORT_WINDOW;  // predecessors per look-back round
 constexpr int kMatchMaxGroups = 16;  // distinct digits per warp above which ballots are cheaper
