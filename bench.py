@@ -641,6 +641,41 @@ def run_batched(args, emit=True):
     return res
 
 
+def serve_autotune(vox, offs, log2s, budget_s, chunks=64):
+    """The autotuner on a served-size batch (the first `chunks` chunks of the pool): the
+    setting it finds stays applied for the serving that follows."""
+    import torch
+    from pyrit_b200 import autotune, native
+    L = native.lib()
+    stream = torch.cuda.current_stream()
+    ex = native.Exec()
+    ex.stream = ctypes.c_void_p(stream.cuda_stream)
+    k = min(chunks, len(log2s))
+    lg = np.ascontiguousarray(log2s[:k], dtype=np.uint32)
+    d_lg = torch.from_numpy(lg.view(np.int32)).cuda()
+    o32 = np.ascontiguousarray(offs[:k + 1], dtype=np.uint32)
+    d_off = torch.from_numpy(o32.view(np.int32)).cuda()
+    counts = torch.zeros(native.COUNTS_WORDS, dtype=torch.int32).pin_memory()
+    res = torch.zeros(k, dtype=torch.int32).pin_memory()
+
+    def once():
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        bd = native.Batch(count=k, log2_host=lg.ctypes.data, log2=d_lg.data_ptr(), voxels=vox.data_ptr(),
+                          voxel_offsets=d_off.data_ptr(), edits=0, edit_offsets=0, voxel_total=int(o32[-1]),
+                          edit_total=0)
+        out = native.BuiltC()
+        a.record(stream)
+        native.check(L.pyrb_build_batch_async(ctypes.byref(ex), ctypes.byref(bd), 5, res.data_ptr(), res.data_ptr(),
+                                              res.data_ptr(), counts.data_ptr(), ctypes.byref(out)))
+        b.record(stream)
+        L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(out))
+        return a, b
+
+    best, _ = autotune.sweep(once, reps=2, budget_s=budget_s)
+    autotune.apply(best)
+    return {x: best[x] for x in ("radix_bits", "tile_keys", "load_factor_pct")}
+
+
 def run_served(args, emit=True):
     """Poisson arrivals of chunk-build requests (a chunk of the 1024-chunk mix plus 0..64
     random edits) at --rate per second for --duration seconds, served by continuous
@@ -655,6 +690,7 @@ def run_served(args, emit=True):
     log2s = wl.chunk_mix(K, 0)
     vox, offs = wl.mix_chunks_device(log2s, 0, 0)
     pool = ChunkPool(vox, offs, log2s)
+    tuning = serve_autotune(vox, offs, log2s, args.tune_budget)
     out = {}
     for rate in args.rates:
         n = int(rate * args.duration)
@@ -682,7 +718,7 @@ def run_served(args, emit=True):
                           "config": {"workload": "Poisson chunk requests from the 1024-chunk mix + 0..64 edits",
                                      "duration_s": args.duration, "budget_gb": 40,
                                      "max_batch_voxels": args.max_batch_voxels},
-                          "served": out}), flush=True)
+                          "tuning": tuning, "served": out}), flush=True)
     del vox
     torch.cuda.empty_cache()
     return out
