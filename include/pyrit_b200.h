@@ -204,7 +204,9 @@ PYRB_API const char* pyrb_error_message(void);
 PYRB_API const char* pyrb_result_string(pyrb_result r);
 
 /* Tuning of the sort and the dedup tables (digit width 4, 8, 9, 10 or 11 bits; keys per
- * sort tile 1024, 2048 or 4096; hash load factor in percent, 25..90). Applies to
+ * sort tile 1024, 2048 or 4096, or 8192 with 8- or 9-bit digits; both 0, the default:
+ * chosen per build, 9 bits on 8192 entries where that takes one radix pass less than
+ * 8 bits, else 8 bits on 4096; hash load factor in percent, 25..90). Applies to
  * builds started afterwards on any thread. Returns PYRB_ERROR_INVALID_ARGUMENT for
  * unsupported values. */
 typedef struct pyrb_tuning {

@@ -1,7 +1,8 @@
 """Autotuner of the build's sort and dedup parameters.
 
 Sweeps the radix digit width (4, 8, 9, 10, 11 bits), the keys per sort tile (1024,
-2048, 4096) and the dedup hash-table load factor (50 %, 70 %) on a caller-supplied
+2048, 4096; 8192 with 8- or 9-bit digits) and the dedup hash-table load factor (50 %,
+70 %) on a caller-supplied
 workload, times every setting with CUDA events, applies the fastest through
 pyrb_set_tuning and can persist it as JSON. None of the parameters changes the
 output (the build is bit-exact for all of them); they only change speed and memory.
@@ -16,8 +17,13 @@ import time
 from . import gpu_build
 
 RADIX_BITS = (4, 8, 9, 10, 11)
-TILE_KEYS = (1024, 2048, 4096)
+TILE_KEYS = (1024, 2048, 4096, 8192)
 LOAD_FACTORS = (50, 70)
+
+
+def supported(radix_bits: int, tile_keys: int) -> bool:
+    """8192-entry sort tiles exist for 8- and 9-bit digits only."""
+    return tile_keys != 8192 or radix_bits in (8, 9)
 
 
 def default_path() -> str:
@@ -38,6 +44,8 @@ def sweep(run_once, reps: int = 3, radix_bits=RADIX_BITS, tile_keys=TILE_KEYS, l
     t_start = time.time()
     try:
         for rb, tk, lf in itertools.product(radix_bits, tile_keys, load_factors):
+            if not supported(rb, tk):
+                continue
             if time.time() - t_start > budget_s:
                 break
             gpu_build.set_tuning(rb, tk, lf)

@@ -195,9 +195,11 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t* status, uint32_t til
     return excl;
 }
 
-// Exclusive block scan of one u32 per thread (kBlock threads). Returns the
-// exclusive prefix; *total receives the block sum. Uses 2*kWarps words of smem.
+// Exclusive block scan of one u32 per thread (NW warps, kBlock threads by default).
+// Returns the exclusive prefix; *total receives the block sum. Uses 2*NW+1 words of smem.
+template <int NW = kWarps>
 __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* smem, uint32_t* total) {
+    static_assert(NW <= 32, "one warp scans the warp sums");
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t x = v;
 #pragma unroll
@@ -208,19 +210,19 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* smem, 
     if (lane == 31) smem[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < unsigned(kWarps) ? smem[lane] : 0;
+        uint32_t w = lane < unsigned(NW) ? smem[lane] : 0;
         uint32_t s = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(kFull, s, o);
             if (lane >= unsigned(o)) s += y;
         }
-        if (lane < unsigned(kWarps)) smem[kWarps + lane] = s - w;
-        if (lane == kWarps - 1) smem[2 * kWarps] = s;
+        if (lane < unsigned(NW)) smem[NW + lane] = s - w;
+        if (lane == NW - 1) smem[2 * NW] = s;
     }
     __syncthreads();
-    uint32_t r = smem[kWarps + warp] + x - v;
-    *total = smem[2 * kWarps];
+    uint32_t r = smem[NW + warp] + x - v;
+    *total = smem[2 * NW];
     __syncthreads();
     return r;
 }

@@ -214,10 +214,11 @@ __global__ void __launch_bounds__(kBlock) k_encode_hist(BuildDesc d) {
     }
 }
 
-// Exclusive scan of RADIX digit counts in smem (in -> out), DPT consecutive digits per thread.
-template <int RADIX>
+// Exclusive scan of RADIX digit counts in smem (in -> out) by NT threads, DPT
+// consecutive digits per thread.
+template <int RADIX, int NT = kBlock>
 __device__ __forceinline__ void scan_digits(const uint32_t* in, uint32_t* out, uint32_t* scratch) {
-    constexpr int DPT = (RADIX + kBlock - 1) / kBlock;
+    constexpr int DPT = (RADIX + NT - 1) / NT;
     uint32_t local[DPT];
     uint32_t sum = 0;
 #pragma unroll
@@ -227,7 +228,7 @@ __device__ __forceinline__ void scan_digits(const uint32_t* in, uint32_t* out, u
         sum += local[k];
     }
     uint32_t total;
-    uint32_t run = block_excl_scan(sum, scratch, &total);
+    uint32_t run = block_excl_scan<NT / 32>(sum, scratch, &total);
 #pragma unroll
     for (int k = 0; k < DPT; ++k) {
         uint32_t dg = threadIdx.x * DPT + k;
@@ -255,12 +256,12 @@ __global__ void __launch_bounds__(kBlock) k_digit_base(BuildDesc d) {
     for (uint32_t i = threadIdx.x; i < uint32_t(RADIX); i += kBlock) h[i] = s_out[i];
 }
 
-template <int RB, int IT, typename KeyT>
+template <int RB, int IT, typename KeyT, int NT = kBlock>
 constexpr size_t sort_smem_bytes() {
-    constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
+    constexpr int RADIX = 1 << RB, TILE = NT * IT, NW = NT / 32;
     constexpr int KW = int(sizeof(KeyT) / 4);  // words per key
-    constexpr int U = (kWarps * RADIX > (KW + 1) * TILE) ? kWarps * RADIX : (KW + 1) * TILE;
-    return size_t(U + 3 * RADIX + 2 * kWarps + 8 + TILE) * 4;
+    constexpr int U = (NW * RADIX > (KW + 1) * TILE) ? NW * RADIX : (KW + 1) * TILE;
+    return size_t(U + 3 * RADIX + 2 * NW + 8 + TILE) * 4;
 }
 
 // Asynchronous 4-byte global -> shared copies (cp.async): no register holds the value
@@ -272,7 +273,7 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// One LSD pass of the onesweep radix sort over a tile of kBlock * IT entries:
+// One LSD pass of the onesweep radix sort over a tile of NT * IT entries (NT threads):
 //  1. keys are loaded warp-striped (a warp owns 32 * IT consecutive entries) and
 //     ranked in input order with match_any against per-warp digit counters;
 //  2. the tile's digit counts are published at once as aggregates for the
@@ -289,24 +290,24 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 constexpr int kSortWindow = PYRB_SORT_WINDOW;  // predecessors per look-back round
 constexpr int kMatchMaxGroups = 16;  // distinct digits per warp above which ballots are cheaper
 
-// 4 resident tiles per SM: caps the pass at 64 registers (the 16-key tiles spill a
-// few words, cheaper than the lost occupancy)
+// 4 resident 256-thread tiles (or 2 of 512 threads) per SM: caps the pass at 64
+// registers (the 16-key tiles spill a few words, cheaper than the lost occupancy)
 #ifndef PYRB_SORT_MIN_BLOCKS
 #define PYRB_SORT_MIN_BLOCKS 4
 #endif
-template <int RB, int IT, typename KeyT>
-__global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(BuildDesc d, uint32_t pass, uint32_t src) {
+template <int RB, int IT, typename KeyT, int NT = kBlock>
+__global__ void __launch_bounds__(NT, PYRB_SORT_MIN_BLOCKS * kBlock / NT) k_sort_pass(BuildDesc d, uint32_t pass, uint32_t src) {
     grid_dep_wait();
-    constexpr int RADIX = 1 << RB, TILE = kBlock * IT;
+    constexpr int RADIX = 1 << RB, TILE = NT * IT, NW = NT / 32;
     constexpr int KW = int(sizeof(KeyT) / 4);
-    constexpr int U = (kWarps * RADIX > (KW + 1) * TILE) ? kWarps * RADIX : (KW + 1) * TILE;
+    constexpr int U = (NW * RADIX > (KW + 1) * TILE) ? NW * RADIX : (KW + 1) * TILE;
     extern __shared__ uint32_t smem[];
-    uint32_t* whist = smem;               // [kWarps][RADIX], later staging keys|vals
+    uint32_t* whist = smem;               // [NW][RADIX], later staging keys|vals
     uint32_t* tcnt = smem + U;            // tile count per digit
     uint32_t* texcl = tcnt + RADIX;       // tile-exclusive digit offsets
     uint32_t* gofs = texcl + RADIX;       // global write offset per digit
-    uint32_t* scratch = gofs + RADIX;     // 2*kWarps + 1 words
-    uint32_t* s_tile = scratch + 2 * kWarps + 4;
+    uint32_t* scratch = gofs + RADIX;     // 2*NW + 1 words
+    uint32_t* s_tile = scratch + 2 * NW + 4;
     uint32_t* vland = s_tile + 4;         // [TILE] values in tile order, copied asynchronously
 
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -320,7 +321,7 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
     uint32_t* vout = d.vbuf[src ^ 1];
     const uint32_t* gbase = d.hist + (uint64_t(sp.seg) * d.passes + pass) * RADIX;
 
-    for (uint32_t i = threadIdx.x; i < uint32_t(kWarps * RADIX); i += kBlock) whist[i] = 0;
+    for (uint32_t i = threadIdx.x; i < uint32_t(NW * RADIX); i += NT) whist[i] = 0;
     KeyT keys[IT];
     uint32_t rank[IT];
 #pragma unroll
@@ -379,10 +380,10 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
     __syncthreads();
     // cross-warp exclusive offsets per digit, tile totals, published at once
     uint64_t* status = d.sort_status + uint64_t(pass) * d.sort_tiles * RADIX;
-    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
+    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += NT) {
         uint32_t run = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
+        for (int w = 0; w < NW; ++w) {
             uint32_t c = whist[w * RADIX + dg];
             whist[w * RADIX + dg] = run;
             run += c;
@@ -391,7 +392,7 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
         if (tile != sp.first_tile) st_relaxed(status + uint64_t(tile) * RADIX + dg, kFlagAgg | run);
     }
     __syncthreads();
-    scan_digits<RADIX>(tcnt, texcl, scratch);
+    scan_digits<RADIX, NT>(tcnt, texcl, scratch);
     __syncthreads();
     // tile-local ranks; then keys to shared memory in digit order
 #pragma unroll
@@ -416,7 +417,7 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
     }
     // look-back per digit (the tile's entries are staged: few live registers)
     const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
-    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += kBlock) {
+    for (uint32_t dg = threadIdx.x; dg < uint32_t(RADIX); dg += NT) {
         uint64_t excl = lookback_window<kSortWindow>(status + dg, RADIX, tile, sp.first_tile, tcnt[dg],
                                                      d.counters + kCtrError);
         gofs[dg] = seg_begin + __ldg(gbase + dg) + uint32_t(excl) - texcl[dg];
@@ -424,7 +425,7 @@ __global__ void __launch_bounds__(kBlock, PYRB_SORT_MIN_BLOCKS) k_sort_pass(Buil
     __syncthreads();
     const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
     bool oob = false;
-    for (uint32_t i = threadIdx.x; i < sp.count; i += kBlock) {
+    for (uint32_t i = threadIdx.x; i < sp.count; i += NT) {
         KeyT k = sk[i];
         uint32_t pos = gofs[uint32_t(k >> shift) & dmask] + i;
         if (pos >= seg_begin && pos < seg_end) {
@@ -452,10 +453,17 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // a sort tile larger than kBlock * IT entries is taken in parts, each a unique tile
+    const uint32_t parts = d.tile_keys / (kBlock * IT);
     const uint32_t tile = dyn_tile(d.counters, 8, &s_tile);
-    const uint32_t ntiles = d.seg_tile[d.seg_count];
+    const uint32_t ntiles = d.seg_tile[d.seg_count] * parts;
     if (tile >= ntiles) return;
-    const TileSpan sp = tile_span(d, tile);
+    TileSpan sp = tile_span(d, tile / parts);
+    {
+        const uint32_t skip = (tile % parts) * (kBlock * IT);
+        sp.start += skip;
+        sp.count = sp.count > skip ? min(sp.count - skip, uint32_t(kBlock * IT)) : 0u;
+    }
     const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
     const KeyT* keys = static_cast<const KeyT*>(d.kbuf[fin]);
     const uint32_t* vals = d.vbuf[fin];

@@ -308,7 +308,9 @@ def last_stats() -> native.Stats:
     return s
 
 
-def set_tuning(radix_bits: int = 8, tile_keys: int = 4096, load_factor_pct: int = 50) -> None:
+def set_tuning(radix_bits: int = 0, tile_keys: int = 0, load_factor_pct: int = 50) -> None:
+    """Digit width and keys per sort tile (0 and 0: chosen per build, the default) and
+    the dedup table load factor, for builds started afterwards."""
     t = native.Tuning(radix_bits=radix_bits, tile_keys=tile_keys, load_factor_pct=load_factor_pct)
     native.check(native.lib().pyrb_set_tuning(ctypes.byref(t)))
 

@@ -43,6 +43,16 @@ def test_host_only_calls():
     t = native.Tuning(radix_bits=5, tile_keys=4096, load_factor_pct=50)  # 5 is not a supported width
     assert L.pyrb_set_tuning(ctypes.byref(t)) == -1
     assert b"radix_bits" in L.pyrb_error_message()
+    t = native.Tuning(radix_bits=10, tile_keys=8192, load_factor_pct=50)  # 8192-entry tiles take 8 or 9 bits
+    assert L.pyrb_set_tuning(ctypes.byref(t)) == -1
+    assert b"8192" in L.pyrb_error_message()
+    t = native.Tuning(radix_bits=0, tile_keys=4096, load_factor_pct=50)  # automatic is both or neither
+    assert L.pyrb_set_tuning(ctypes.byref(t)) == -1
+    t = native.Tuning(radix_bits=0, tile_keys=0, load_factor_pct=50)
+    assert L.pyrb_set_tuning(ctypes.byref(t)) == 0
+    g = native.Tuning()
+    L.pyrb_get_tuning(ctypes.byref(g))
+    assert (g.radix_bits, g.tile_keys, g.load_factor_pct) == (0, 0, 50)
 
 
 def test_struct_layouts():

@@ -87,3 +87,20 @@ def test_uniform_batch_equals_chunks_api():
     log2s = [4] * 12
     chunks = [_chunk(rng, 4, "rand") for _ in log2s]
     _check(log2s, chunks, None, rt=3)
+
+
+@pytest.mark.parametrize("radix_bits", [8, 9])
+def test_mixed_batch_with_large_sort_tiles(radix_bits):
+    """8192-entry sort tiles over segments of many sizes: full 32^3 chunks span four
+    tiles, small chunks share none, empty ones take none."""
+    from pyrit_b200 import gpu_build
+    rng = np.random.default_rng(11)
+    log2s = [5, 3, 5, 4, 5, 3]
+    kinds = ["full", "rand", "rand", "empty", "full", "rand"]
+    chunks = [_chunk(rng, l, k) for l, k in zip(log2s, kinds)]
+    old = gpu_build.get_tuning()
+    try:
+        gpu_build.set_tuning(radix_bits, 8192, 50)
+        _check(log2s, chunks, None, rt=3)
+    finally:
+        gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)

@@ -150,7 +150,8 @@ def test_noise256_with_edits_matches_oracle(gb):
 
 
 @pytest.mark.parametrize("radix_bits,tile_keys,lf", [(4, 1024, 50), (8, 2048, 70), (11, 4096, 50), (11, 1024, 90),
-                                                     (8, 4096, 25), (9, 4096, 50), (10, 2048, 70), (9, 1024, 50)])
+                                                     (8, 4096, 25), (9, 4096, 50), (10, 2048, 70), (9, 1024, 50),
+                                                     (8, 8192, 50), (9, 8192, 70)])
 def test_tuning_variants_are_bit_exact(gb, radix_bits, tile_keys, lf):
     """The autotuner's knobs (digit width, tile, load factor) never change the output."""
     _, pts = _scene_points(6)
@@ -162,6 +163,22 @@ def test_tuning_variants_are_bit_exact(gb, radix_bits, tile_keys, lf):
     finally:
         gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
     assert_same_build(g, o, label=f"tuning {radix_bits}/{tile_keys}/{lf}")
+
+
+@pytest.mark.parametrize("radix_bits", [8, 9])
+def test_large_sort_tiles_match_oracle(gb, radix_bits):
+    """8192-entry sort tiles (512-thread sort blocks, unique in two parts) over many
+    tiles, ragged last tile included."""
+    pts = np.concatenate([wl.noise_grid(7, 1), wl.noise_edits(7, 1)])
+    o = orc.gb_build(7, 5, pts)
+    old = gb.get_tuning()
+    try:
+        gb.set_tuning(radix_bits, 8192, 50)
+        g = gb.build(7, 5, dev(pts)).download()
+    finally:
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+    assert len(pts) % 8192 != 0
+    assert_same_build(g, o, label=f"tiles 8192, {radix_bits} bits")
 
 
 def test_invalid_arguments(gb):
