@@ -317,6 +317,7 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
         cudaFuncSetAttribute(k_encode_hist<RB, IT, KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
         cudaFuncSetAttribute(k_sort_pass<RB, SIT, KeyT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
         cudaFuncSetAttribute(k_sort_pass<RB, SIT, KeyT, NT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_unique<SIT, KeyT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     });
     launch(k_encode_hist<RB, IT, KeyT>, d.sort_tiles, kBlock, hist_smem, st, d);
     prof.mark("encode_hist");
@@ -326,8 +327,8 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
         launch(k_sort_pass<RB, SIT, KeyT, NT>, d.sort_tiles, NT, sort_smem, st, d, p, p & 1);
         prof.mark("sort_pass", p);
     }
-    launch(k_unique<SIT, KeyT>, d.sort_tiles * parts, kBlock, 0, st, d, d.passes & 1);
-    prof.mark("unique");
+    launch(k_unique<SIT, KeyT>, d.sort_tiles * parts, kBlock, unique_smem_bytes<SIT, KeyT>(), st, d, d.passes & 1);
+    prof.mark("unique_brick");
     return cudaGetLastError();
 }
 
@@ -483,7 +484,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     }
     if (words >= (uint64_t(1) << 32)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "node buffer bound exceeds 2^32 words");
     d.brick_bound = B;
-    d.brick_tiles = std::max((nmax + kBrickTile - 1) / kBrickTile, 1u);
+    d.brick_tiles = d.sort_tiles * std::max(1u, tile_keys / 4096u);  // the unique tiles
     d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
     d.leaf_cap = next_pow2((uint64_t(B) * 100 + lf - 1) / lf, 1024);
     d.node_bound = uint32_t(words);
@@ -494,7 +495,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     const uint64_t o_counters = zl.take(kCtrCount * 4);
     const uint64_t o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
     const uint64_t o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
-    const uint64_t o_uniq_status = zl.take(uint64_t(d.sort_tiles) * std::max(1u, tile_keys / 4096u) * 8);
+    const uint64_t o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
     const uint64_t o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
     const uint64_t o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
     const uint64_t o_leaf_table = zl.take(uint64_t(d.leaf_cap) * 16);
@@ -654,13 +655,11 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     CUL(cudaGetLastError());
     CUL(launch_sort_any(rb, it, d, st, prof));
     launches += 3 + passes;
-    launch(k_brick, d.brick_tiles, kBlock, 0, st, d);
-    prof.mark("brick");
     launch(k_leaf_insert, leaf_insert_grid(d), kBlock, 0, st, d);
     prof.mark("leaf_insert");
     launch(k_leaf_own, d.leafown_tiles, kBlock, 0, st, d);
     prof.mark("leaf_own");
-    launches += 3;
+    launches += 2;
     const uint32_t lv0 = tail_level(log2, B, P);
     launches += launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
     if (job.mode == kModeBatch && min_log2 < log2) {
@@ -1349,7 +1348,7 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
         words += uint64_t(P[lv]) * kNodeStride;
     }
     d.brick_bound = B;
-    d.brick_tiles = std::max((nmax + kBrickTile - 1) / kBrickTile, 1u);
+    d.brick_tiles = d.sort_tiles * std::max(1u, tile_keys / 4096u);  // the unique tiles
     d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
     d.leaf_cap = next_pow2((uint64_t(B) * 100 + lf - 1) / lf, 1024);
     d.node_bound = uint32_t(words);
@@ -1364,7 +1363,7 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     const uint64_t o_counters = zl.take(kCtrCount * 4);
     const uint64_t o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
     const uint64_t o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
-    const uint64_t o_uniq_status = zl.take(uint64_t(d.sort_tiles) * std::max(1u, tile_keys / 4096u) * 8);
+    const uint64_t o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
     const uint64_t o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
     const uint64_t o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
     const uint64_t o_leaf_table = zl.take(uint64_t(d.leaf_cap) * 16);
@@ -1493,7 +1492,6 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     launch(k_plan, 1, 1024, 0, st, d);
     CU(cudaGetLastError());
     CU((launch_sort<8, 16>(d, st, prof)));
-    launch(k_brick, d.brick_tiles, kBlock, 0, st, d);
     launch(k_leaf_insert, leaf_insert_grid(d), kBlock, 0, st, d);
     launch(k_leaf_own, d.leafown_tiles, kBlock, 0, st, d);
     const uint32_t lv0 = tail_level(log2, B, P);

@@ -91,7 +91,7 @@ struct BuildDesc {
     // bricks + leaves
     uint32_t brick_bound;
     uint32_t brick_tiles;
-    uint64_t* brick_status;  // [brick_tiles]
+    uint64_t* brick_status;  // [brick_tiles]: the unique tiles count bricks too
     uint64_t* bkey;
     uint64_t* bmask;
     uint32_t* bfirst;

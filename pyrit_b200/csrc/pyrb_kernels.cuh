@@ -439,19 +439,41 @@ __global__ void __launch_bounds__(NT, PYRB_SORT_MIN_BLOCKS * kBlock / NT) k_sort
 }
 
 // ---------------------------------------------------------------------------
-// Unique voxels: the last entry of a run of equal keys decides; it is kept if it
-// is valid and its attribute is non-zero (gbuild.zig:366-388). Positions by a
-// look-back scan in global (segment-major) order; keys get the segment (chunk)
-// number above bit lb, like packChunks.
+// Unique voxels and bricks, one pass over the sorted entries.
+// Unique: the last entry of a run of equal keys decides; it is kept if it is valid
+// and its attribute is non-zero (gbuild.zig:366-388). Positions by a look-back over
+// the tiles in global (segment-major) order; keys get the segment (chunk) number
+// above bit lb, like packChunks; chunkFirst (:237-242).
+// Bricks (brickHeads/brickBuild, :394-428): runs of the kept keys with equal
+// key >> 6 -> (brick key, 64-bit mask, first voxel). A brick belongs to the tile
+// holding the first ENTRY (kept or not) of its run of equal key >> 6, a test on the
+// tile's own entries and the one before it; that tile reads ahead past its end while
+// the run goes on (a brick has at most 64 distinct keys). The tile's kept entries,
+// and those read ahead, are compacted in shared memory, its bricks counted there and
+// published for a second look-back, and each brick assembled by one thread.
 // ---------------------------------------------------------------------------
+constexpr int kUniqAhead = 64;  // kept keys read ahead: the distinct keys of one brick
+
+template <int IT, typename KeyT>
+constexpr size_t unique_smem_bytes() {
+    constexpr size_t CAP = size_t(kBlock) * IT + kUniqAhead;
+    return CAP * (sizeof(KeyT) + 4 + 2);  // keys, values, brick heads
+}
+
 template <int IT, typename KeyT>
 // 5 tiles per SM (48 registers): the tile mostly waits for its predecessors' counts,
 // so more tiles in flight per SM measured 17 % faster than 4 at 64 registers
 __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin) {
     grid_dep_wait();
-    __shared__ uint32_t s_tile;
+    constexpr int TILE = kBlock * IT, CAP = TILE + kUniqAhead;
+    extern __shared__ __align__(16) unsigned char usmem[];
+    KeyT* s_key = reinterpret_cast<KeyT*>(usmem);                 // [CAP] kept keys, tile order
+    uint32_t* s_val = reinterpret_cast<uint32_t*>(s_key + CAP);   // [CAP] their attributes
+    uint16_t* s_head = reinterpret_cast<uint16_t*>(s_val + CAP);  // [CAP] compacted index of each brick head
+    __shared__ uint32_t s_tile, s_extra;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
-    __shared__ uint64_t s_base;
+    __shared__ uint64_t s_ubase, s_bbase;
+    __shared__ KeyT s_lead;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // a sort tile larger than kBlock * IT entries is taken in parts, each a unique tile
     const uint32_t parts = d.tile_keys / (kBlock * IT);
@@ -464,68 +486,171 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
         sp.start += skip;
         sp.count = sp.count > skip ? min(sp.count - skip, uint32_t(kBlock * IT)) : 0u;
     }
-    const uint32_t seg_end = __ldg(d.seg_entry + sp.seg + 1);
+    const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg), seg_end = __ldg(d.seg_entry + sp.seg + 1);
     const KeyT* keys = static_cast<const KeyT*>(d.kbuf[fin]);
     const uint32_t* vals = d.vbuf[fin];
     const KeyT inv = KeyT(1) << d.lb;
+    const KeyT NONE = ~KeyT(0);  // never the brick of a key: key >> 6 has its top 6 bits clear
     const uint32_t wbase = warp * 32 * IT;
 
-    KeyT k[IT];
-    uint32_t v[IT];
-    unsigned keepb[IT];
-    uint32_t wcount = 0;
-    // all loads first (no shuffle between them), then the run-end tests
-#pragma unroll
-    for (int j = 0; j < IT; ++j) {
-        uint32_t idx = wbase + j * 32 + lane;
-        bool in = idx < sp.count;
-        uint32_t e = sp.start + idx;
-        k[j] = in ? keys[e] : inv;
-        v[j] = in ? vals[e] : 0;
-    }
-#pragma unroll
-    for (int j = 0; j < IT; ++j) {
-        uint32_t idx = wbase + j * 32 + lane;
-        bool in = idx < sp.count;
-        uint32_t e = sp.start + idx;
-        // successor key: lane + 1 of this row, lane 0 of the next row (every lane shuffles)
-        const KeyT down = __shfl_down_sync(kFull, k[j], 1);
-        const KeyT row_next = __shfl_sync(kFull, k[j + 1 < IT ? j + 1 : j], 0);
-        KeyT nk = lane < 31 ? down : row_next;
-        if ((lane == 31 && j + 1 == IT) || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~KeyT(0);
-        bool last = !in ? false : (e + 1 == seg_end || nk != k[j]);
-        bool keep = in && last && !(k[j] & inv) && v[j] != 0;
-        keepb[j] = __ballot_sync(kFull, keep);
-        wcount += __popc(keepb[j]);
-    }
     uint32_t total;
-    uint32_t wexcl = block_excl_scan(lane == 0 ? wcount : 0, s_scan, &total);
-    wexcl = __shfl_sync(kFull, wexcl, 0);
-    if (warp == 0) {
-        if (lane == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | total);
-        // positions are global over all segments: look back to tile 0
-        uint64_t ex = lookback_warp(d.uniq_status, tile, 0, total, d.counters + kCtrError);
-        if (lane == 0) s_base = ex;
-    }
-    __syncthreads();
-    const uint64_t base = s_base + wexcl;
-    uint32_t run = 0;
-    const uint64_t segbits = uint64_t(sp.seg) << d.lb;
+    {
+        KeyT k[IT];
+        uint32_t v[IT];
+        unsigned keepb[IT];
+        uint32_t wcount = 0;
+        // all loads first (no shuffle between them), then the run-end tests
 #pragma unroll
-    for (int j = 0; j < IT; ++j) {
-        if ((keepb[j] >> lane) & 1) {
-            uint64_t pos = base + run + __popc(keepb[j] & lanemask_lt());
-            if (pos < d.n_total) {
-                d.ukey[pos] = segbits | uint64_t(k[j]);
-                d.uval[pos] = v[j];
-            } else {
-                atomicOr(d.counters + kCtrError, kErrBound);
+        for (int j = 0; j < IT; ++j) {
+            uint32_t idx = wbase + j * 32 + lane;
+            bool in = idx < sp.count;
+            uint32_t e = sp.start + idx;
+            k[j] = in ? keys[e] : inv;
+            v[j] = in ? vals[e] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            uint32_t idx = wbase + j * 32 + lane;
+            bool in = idx < sp.count;
+            uint32_t e = sp.start + idx;
+            // successor key: lane + 1 of this row, lane 0 of the next row (every lane shuffles)
+            const KeyT down = __shfl_down_sync(kFull, k[j], 1);
+            const KeyT row_next = __shfl_sync(kFull, k[j + 1 < IT ? j + 1 : j], 0);
+            KeyT nk = lane < 31 ? down : row_next;
+            if ((lane == 31 && j + 1 == IT) || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~KeyT(0);
+            bool last = !in ? false : (e + 1 == seg_end || nk != k[j]);
+            bool keep = in && last && !(k[j] & inv) && v[j] != 0;
+            keepb[j] = __ballot_sync(kFull, keep);
+            wcount += __popc(keepb[j]);
+        }
+        uint32_t wexcl = block_excl_scan(lane == 0 ? wcount : 0, s_scan, &total);
+        wexcl = __shfl_sync(kFull, wexcl, 0);
+        // kept entries compacted in tile order
+        uint32_t run = 0;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            if ((keepb[j] >> lane) & 1) {
+                const uint32_t p = wexcl + run + __popc(keepb[j] & lanemask_lt());
+                s_key[p] = k[j];
+                s_val[p] = v[j];
+            }
+            run += __popc(keepb[j]);
+        }
+    }
+    if (threadIdx.x == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | total);
+    if (warp == kWarps - 1) {
+        // the brick run of the entry before the tile (bricks of that run belong to an
+        // earlier tile); the tile's last run, if it started here, read on past the end
+        const KeyT lead = (sp.count > 0 && sp.start > seg_begin) ? KeyT(keys[sp.start - 1] >> 6) : NONE;
+        uint32_t extra = 0;
+        if (sp.count > 0) {
+            const uint32_t e_last = sp.start + sp.count - 1;
+            const KeyT klast = keys[e_last];
+            const KeyT rb = klast >> 6;
+            if (!(klast & inv) && rb != lead && e_last + 1 < seg_end) {
+                bool more = true;
+                for (uint32_t base = e_last + 1; more && base < seg_end; base += 32) {
+                    const uint32_t e = base + lane;
+                    const KeyT ke = e < seg_end ? keys[e] : NONE;
+                    const bool in_run = e < seg_end && KeyT(ke >> 6) == rb;
+                    bool keep = false;
+                    uint32_t ve = 0;
+                    if (in_run) {
+                        const KeyT kn = e + 1 < seg_end ? keys[e + 1] : NONE;
+                        ve = vals[e];
+                        keep = (e + 1 == seg_end || kn != ke) && ve != 0;
+                    }
+                    const unsigned kb = __ballot_sync(kFull, keep);
+                    if (keep) {
+                        const uint32_t p = extra + __popc(kb & lanemask_lt());
+                        if (p < uint32_t(kUniqAhead)) {
+                            s_key[total + p] = ke;
+                            s_val[total + p] = ve;
+                        } else {
+                            atomicOr(d.counters + kCtrError, kErrBound);
+                        }
+                    }
+                    extra = min(extra + __popc(kb), uint32_t(kUniqAhead));
+                    more = __all_sync(kFull, in_run);
+                }
             }
         }
-        run += __popc(keepb[j]);
+        if (lane == 0) { s_extra = extra; s_lead = lead; }
     }
-    if (d.chunked && threadIdx.x == 0 && total > 0) atomicMin(d.chunk_first + sp.seg, uint32_t(s_base));
-    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrUnique] = uint32_t(s_base + total);
+    __syncthreads();
+    // brick heads over the compacted entries: a key whose brick differs from the
+    // previous kept key's (the first one: from the brick of the entry before the tile)
+    const uint32_t M = total + s_extra;
+    const KeyT lead = s_lead;
+    const uint32_t ch = ((M + kWarps - 1) / kWarps + 31) & ~31u;  // entries per warp, whole rows
+    const uint32_t w_lo = min(warp * ch, M), w_hi = min(w_lo + ch, M);
+    uint32_t wheads = 0;
+    for (uint32_t i0 = w_lo; i0 < w_hi; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool head = i < w_hi && KeyT(s_key[i] >> 6) != (i == 0 ? lead : KeyT(s_key[i - 1] >> 6));
+        wheads += __popc(__ballot_sync(kFull, head));
+    }
+    uint32_t btotal;
+    uint32_t hexcl = block_excl_scan(lane == 0 ? wheads : 0, s_scan, &btotal);
+    hexcl = __shfl_sync(kFull, hexcl, 0);
+    if (threadIdx.x == 0 && tile != 0) st_relaxed(d.brick_status + tile, kFlagAgg | btotal);
+    for (uint32_t i0 = w_lo; i0 < w_hi; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool head = i < w_hi && KeyT(s_key[i] >> 6) != (i == 0 ? lead : KeyT(s_key[i - 1] >> 6));
+        const unsigned hb = __ballot_sync(kFull, head);
+        if (head) s_head[hexcl + __popc(hb & lanemask_lt())] = uint16_t(i);
+        hexcl += __popc(hb);
+    }
+    __syncthreads();
+    // positions are global over all segments: warps 0 and 1 look back to tile 0 for
+    // the voxel and the brick offsets while the others assemble the first two rounds
+    // of brick masks
+    auto brick_mask = [&](uint32_t b, uint32_t& lo) -> uint64_t {
+        lo = s_head[b];
+        const uint32_t hi = b + 1 < btotal ? s_head[b + 1] : M;
+        uint64_t mask = 0;
+        for (uint32_t i = lo; i < hi; ++i) mask |= 1ull << (uint32_t(s_key[i]) & 63);
+        return mask;
+    };
+    if (warp == 0) {
+        uint64_t ex = lookback_warp(d.uniq_status, tile, 0, total, d.counters + kCtrError);
+        if (lane == 0) s_ubase = ex;
+    } else if (warp == 1) {
+        uint64_t ex = lookback_warp(d.brick_status, tile, 0, btotal, d.counters + kCtrError);
+        if (lane == 0) s_bbase = ex;
+    }
+    uint32_t lo0 = 0, lo1 = 0;
+    const uint32_t b0 = threadIdx.x, b1 = threadIdx.x + kBlock;
+    const uint64_t m0 = b0 < btotal ? brick_mask(b0, lo0) : 0, m1 = b1 < btotal ? brick_mask(b1, lo1) : 0;
+    __syncthreads();
+    const uint64_t ubase = s_ubase, bbase = s_bbase;
+    const uint64_t segbits = uint64_t(sp.seg) << d.lb;
+    for (uint32_t i = threadIdx.x; i < total; i += kBlock) {
+        const uint64_t pos = ubase + i;
+        if (pos < d.n_total) {
+            d.ukey[pos] = segbits | uint64_t(s_key[i]);
+            d.uval[pos] = s_val[i];
+        } else {
+            atomicOr(d.counters + kCtrError, kErrBound);
+        }
+    }
+    for (uint32_t b = threadIdx.x; b < btotal; b += kBlock) {
+        uint32_t lo;
+        const uint64_t mask = b == b0 ? (lo = lo0, m0) : b == b1 ? (lo = lo1, m1) : brick_mask(b, lo);
+        const uint64_t g = bbase + b;
+        if (g < d.brick_bound) {
+            d.bkey[g] = (segbits | uint64_t(s_key[lo])) >> 6;
+            d.bmask[g] = mask;
+            d.bfirst[g] = uint32_t(ubase + lo);
+        } else {
+            atomicOr(d.counters + kCtrError, kErrBound);
+        }
+    }
+    if (d.chunked && threadIdx.x == 0 && total > 0) atomicMin(d.chunk_first + sp.seg, uint32_t(ubase));
+    if (tile == ntiles - 1 && threadIdx.x == 0) {
+        d.counters[kCtrUnique] = uint32_t(ubase + total);
+        d.counters[kCtrBricks] = uint32_t(bbase + btotal);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -590,136 +715,9 @@ __device__ __forceinline__ void leaf_insert2(uint4* table, uint32_t cap, bool w0
     }
 }
 
-// ---------------------------------------------------------------------------
-// Bricks: 4^3 runs of the sorted unique keys -> (brick key, mask, first voxel).
-// A warp owns 32*8 consecutive keys; a run is emitted by the warp that holds its
-// first key (reading at most 63 keys past its chunk).
-// ---------------------------------------------------------------------------
+// Brick-indexed kernels (leaf owners) take tiles of kBrickTile bricks.
 constexpr int kBrickIT = 8;
 constexpr int kBrickTile = kBlock * kBrickIT;
-
-// Records of the bricks whose heads lie in a tile are staged in shared memory at
-// tile-local indices, so the look-back for the tile's global brick offset (by warp
-// 0, first) overlaps the mask assembly of the other warps, and the records leave
-// with coalesced stores.
-// 6 tiles per SM (40 registers, 24 KB of staging: brick keys are re-read from the
-// unique keys at write-out): the tile mostly waits for its predecessors' counts
-__global__ void __launch_bounds__(kBlock, 6) k_brick(BuildDesc d) {
-    grid_dep_wait();
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_scan[2 * kWarps + 2];
-    __shared__ uint64_t s_base;
-    __shared__ uint64_t s_bmask[kBrickTile];
-    __shared__ uint32_t s_bfirst[kBrickTile];
-    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = dyn_tile(d.counters, 9, &s_tile);
-    const uint32_t U = min(d.counters[kCtrUnique], d.n_total);
-    const uint32_t ntiles = (U + kBrickTile - 1) / kBrickTile;
-    if (tile >= ntiles) return;
-    const uint32_t wstart = tile * kBrickTile + warp * 32 * kBrickIT;
-    const uint64_t* ukey = d.ukey;
-    const uint64_t NONE = ~0ull;
-
-    uint64_t key[kBrickIT];
-    unsigned hb[kBrickIT];
-    uint32_t wheads = 0;
-    uint64_t prev_last = (wstart > 0 && wstart - 1 < U) ? ukey[wstart - 1] : NONE;
-#pragma unroll
-    for (int j = 0; j < kBrickIT; ++j) {  // all loads first
-        uint32_t e = wstart + j * 32 + lane;
-        key[j] = e < U ? ukey[e] : NONE;
-    }
-#pragma unroll
-    for (int j = 0; j < kBrickIT; ++j) {
-        uint32_t e = wstart + j * 32 + lane;
-        uint64_t pk = __shfl_up_sync(kFull, key[j], 1);
-        if (lane == 0) pk = prev_last;
-        prev_last = __shfl_sync(kFull, key[j], 31);
-        bool head = e < U && (e == 0 || (key[j] >> 6) != (pk >> 6));
-        hb[j] = __ballot_sync(kFull, head);
-        wheads += __popc(hb[j]);
-    }
-    uint32_t total;
-    uint32_t wexcl = block_excl_scan(lane == 0 ? wheads : 0, s_scan, &total);
-    wexcl = __shfl_sync(kFull, wexcl, 0);
-    if (warp == 0) {
-        if (lane == 0 && tile != 0) st_relaxed(d.brick_status + tile, kFlagAgg | total);
-        uint64_t ex = lookback_warp(d.brick_status, tile, 0, total, d.counters + kCtrError);
-        if (lane == 0) s_base = ex;
-    }
-
-    bool c_on = false, c_own = false;
-    uint64_t c_brick = 0, c_mask = 0;
-    uint32_t c_idx = 0, c_first = 0, hcount = 0;
-#pragma unroll
-    for (int j = 0; j < kBrickIT + 2; ++j) {
-        if (j >= kBrickIT && !(c_on && c_own)) break;
-        uint32_t e = wstart + j * 32 + lane;
-        uint64_t kj;
-        unsigned hbj;
-        if (j < kBrickIT) { kj = key[j]; hbj = hb[j]; }
-        else { kj = e < U ? ukey[e] : NONE; hbj = 0; }
-        bool valid = e < U;
-        uint64_t bk = valid ? (kj >> 6) : NONE;
-        // brick of the entry after lane 31
-        uint32_t en = wstart + (j + 1) * 32;
-        uint64_t nextk;
-        if (j + 1 < kBrickIT) nextk = __shfl_sync(kFull, key[j + 1 < kBrickIT ? j + 1 : 0], 0);
-        else nextk = en < U ? ukey[en] : NONE;
-        uint64_t nb = nextk == NONE ? NONE : (nextk >> 6);
-        unsigned peers = __match_any_sync(kFull, bk);
-        unsigned gstart = __ffs(peers) - 1, glast = 31 - __clz(peers);
-        uint64_t v = valid ? (1ull << (kj & 63)) : 0;
-        bool cont = (gstart == 0) && c_on && bk == c_brick && !((hbj >> 0) & 1);
-        if (lane == 0 && cont) v |= c_mask;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint64_t y = __shfl_up_sync(kFull, v, o);
-            if (lane >= gstart + o) v |= y;
-        }
-        bool ghead = (hbj >> gstart) & 1;
-        // tile-local brick index
-        uint32_t idx = ghead ? wexcl + hcount + __popc(hbj & ((2u << gstart) - 1)) - 1 : c_idx;
-        bool own = ghead ? (j < kBrickIT) : (cont && c_own);
-        uint32_t first = ghead ? wstart + j * 32 + gstart : c_first;
-        const uint64_t next_in_warp = __shfl_down_sync(kFull, bk, 1);  // every lane takes part
-        uint64_t after = (lane == 31) ? nb : next_in_warp;
-        bool ends = valid && lane == glast && after != bk;
-        bool emit = ends && own && (ghead || cont);
-        // carry of the group holding lane 31
-        bool l31_valid = __shfl_sync(kFull, valid ? 1 : 0, 31);
-        bool l31_ends = __shfl_sync(kFull, ends ? 1 : 0, 31);
-        const bool l31_seg = __shfl_sync(kFull, (ghead || cont) ? 1 : 0, 31) != 0;
-        c_on = l31_valid && !l31_ends && l31_seg;
-        c_brick = __shfl_sync(kFull, bk, 31);
-        c_mask = __shfl_sync(kFull, v, 31);
-        c_idx = __shfl_sync(kFull, idx, 31);
-        c_own = __shfl_sync(kFull, own ? 1 : 0, 31) != 0;
-        c_first = __shfl_sync(kFull, first, 31);
-        hcount += __popc(hbj);
-        if (emit) {
-            if (idx < uint32_t(kBrickTile)) {
-                s_bmask[idx] = v;
-                s_bfirst[idx] = first;
-            } else {
-                atomicOr(d.counters + kCtrError, kErrBound);
-            }
-        }
-    }
-    __syncthreads();
-    const uint64_t base = s_base;
-    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrBricks] = uint32_t(base + total);
-    for (uint32_t i = threadIdx.x; i < total; i += kBlock) {
-        const uint64_t g = base + i;
-        if (g < d.brick_bound) {
-            d.bkey[g] = __ldg(ukey + s_bfirst[i]) >> 6;
-            d.bmask[g] = s_bmask[i];
-            d.bfirst[g] = s_bfirst[i];
-        } else {
-            atomicOr(d.counters + kCtrError, kErrBound);
-        }
-    }
-}
 
 // Leaf dedup insert, two bricks per thread per round. Equal masks of a warp row are
 // collapsed with match_any first: only the lowest brick of each group touches the table.

@@ -181,6 +181,44 @@ def test_large_sort_tiles_match_oracle(gb, radix_bits):
     assert_same_build(g, o, label=f"tiles 8192, {radix_bits} bits")
 
 
+def _dup_runs(last_attr, seed=5):
+    """Bricks whose run of equal key >> 6 crosses sort tiles: 9000 copies of voxel
+    (0,0,0) (the last copy decides: attr `last_attr`, 0 deletes), then its brick
+    neighbours and other bricks, so that the brick's first kept voxel lies two tiles
+    after the tile where its run begins; and a second brick of 10000 entries."""
+    rng = np.random.default_rng(seed)
+    a = np.zeros((9000, 4), np.uint32)
+    a[:, 3] = rng.integers(1, 200, 9000)
+    a[-1, 3] = last_attr
+    nb = np.array([[1, 0, 0, 3], [0, 1, 0, 0], [3, 3, 3, 7]], np.uint32)   # (0,1,0) is deleted
+    other = np.concatenate([rng.integers(4, 32, (3000, 3)), rng.integers(0, 6, (3000, 1))], 1).astype(np.uint32)
+    dups = np.repeat(np.array([[9, 9, 9, 4], [9, 9, 10, 0]], np.uint32), 5000, axis=0)
+    return np.concatenate([a, other, nb, dups])
+
+
+@pytest.mark.parametrize("last_attr", [5, 0])
+@pytest.mark.parametrize("tuning", [(8, 4096), (9, 8192), (8, 1024)])
+def test_brick_runs_across_tiles(gb, last_attr, tuning):
+    pts = _dup_runs(last_attr)
+    o = orc.gb_build(5, 3, pts)
+    old = gb.get_tuning()
+    try:
+        gb.set_tuning(tuning[0], tuning[1], 50)
+        g = gb.build(5, 3, dev(pts)).download()
+    finally:
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+    assert_same_build(g, o, label=f"duplicate runs, last attr {last_attr}, tuning {tuning}")
+
+
+def test_brick_runs_all_deleted(gb):
+    """A run of one brick's entries over several tiles with nothing kept: no brick."""
+    a = np.zeros((10000, 4), np.uint32)
+    a[:, 0] = np.arange(10000) % 4
+    a[:, 3] = 0
+    pts = np.concatenate([a, np.array([[8, 8, 8, 2], [31, 31, 31, 1]], np.uint32)])
+    assert_same_build(gb.build(5, 3, dev(pts)).download(), orc.gb_build(5, 3, pts), label="all deleted")
+
+
 def test_invalid_arguments(gb):
     from pyrit_b200.native import PyrbError
     pts = dev(np.array([[1, 1, 1, 1]], np.uint32))
