@@ -487,6 +487,10 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.brick_tiles = d.sort_tiles * std::max(1u, tile_keys / 4096u);  // the unique tiles
     d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
     d.leaf_cap = next_pow2((uint64_t(B) * 100 + lf - 1) / lf, 1024);
+    d.leaf_regions = 1;
+    while (d.leaf_regions < kMaxLeafRegions && d.leaf_cap / d.leaf_regions > kLeafRegionSlots) d.leaf_regions <<= 1;
+    d.leaf_region_shift = 0;
+    while ((d.leaf_cap >> d.leaf_region_shift) > d.leaf_regions) ++d.leaf_region_shift;
     d.node_bound = uint32_t(words);
     d.prim_bound = P[rt - 1];
 
@@ -498,7 +502,9 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     const uint64_t o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
     const uint64_t o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
     const uint64_t o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
-    const uint64_t o_leaf_table = zl.take(uint64_t(d.leaf_cap) * 16);
+    // a table filled region by region is cleared by its insert kernel, not by the memset
+    uint64_t o_leaf_table = d.leaf_regions > 1 ? 0 : zl.take(uint64_t(d.leaf_cap) * 16);
+    const uint64_t o_regions = zl.take(3 * kMaxLeafRegions * 4);
     uint64_t o_table[kMaxLevels + 2], o_bstat[kMaxLevels + 2], o_ostat[kMaxLevels + 2];
     uint32_t cap[kMaxLevels + 2], btiles[kMaxLevels + 2], otiles[kMaxLevels + 2];
     for (uint32_t lv = 2; lv < log2; ++lv) {
@@ -519,6 +525,7 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     const uint64_t ff_bytes = align_up(fl.size, 256) - zero_bytes;
     Layout ol = fl;
     ol.size = zero_bytes + ff_bytes;
+    if (d.leaf_regions > 1) o_leaf_table = ol.take(uint64_t(d.leaf_cap) * 16);
     const uint64_t o_seg_entry = ol.take(uint64_t(K + 1) * 4);
     const uint64_t o_seg_tile = ol.take(uint64_t(K + 1) * 4);
     const uint64_t kbytes = key64 ? 8 : 4;
@@ -567,6 +574,13 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.brick_status = static_cast<uint64_t*>(at(o_brick_status));
     d.leafown_status = static_cast<uint64_t*>(at(o_leafown_status));
     d.leaf_table = static_cast<uint4*>(at(o_leaf_table));
+    d.region_count = static_cast<uint32_t*>(at(o_regions));
+    d.region_cursor = d.region_count + kMaxLeafRegions;
+    d.region_zeroed = d.region_count + 2 * kMaxLeafRegions;
+    // the sort buffers are dead once the unique voxels are out: N x (kb + 4) bytes from
+    // k0 hold the B region-grouped masks, k1 their brick indices
+    d.pmask = static_cast<uint64_t*>(at(o_k0));
+    d.pidx = static_cast<uint32_t*>(at(o_k1));
     d.chunk_first = static_cast<uint32_t*>(at(o_chunk_first));
     d.roots = static_cast<uint32_t*>(at(o_roots));
     d.prim_start = static_cast<uint32_t*>(at(o_prim_start));
@@ -655,7 +669,15 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     CUL(cudaGetLastError());
     CUL(launch_sort_any(rb, it, d, st, prof));
     launches += 3 + passes;
-    launch(k_leaf_insert, leaf_insert_grid(d), kBlock, 0, st, d);
+    if (d.leaf_regions > 1) {
+        launch(k_leaf_part, std::max(std::min((B + kBrickTile - 1) / kBrickTile, 148u * 8u), 1u), kBlock, 0, st, d);
+        prof.mark("leaf_part");
+        ++launches;
+        const uint32_t S = d.leaf_cap / d.leaf_regions, nz = (S + kZeroSlots - 1) / kZeroSlots;
+        launch(k_leaf_insert_regions, d.leaf_regions * (nz + 1) + (B + kInsTile - 1) / kInsTile, kBlock, 0, st, d);
+    } else {
+        launch(k_leaf_insert, leaf_insert_grid(d), kBlock, 0, st, d);
+    }
     prof.mark("leaf_insert");
     launch(k_leaf_own, d.leafown_tiles, kBlock, 0, st, d);
     prof.mark("leaf_own");

@@ -23,6 +23,11 @@ constexpr int kCtrParents = 36;    // + lv: P_lv
 constexpr int kCtrUniqueLv = 64;   // + lv: U_lv
 constexpr int kCtrTiles = 96;      // dynamic tile counters, one per launch
 constexpr int kCtrCount = 160;
+constexpr uint32_t kMaxLeafRegions = 64;
+#ifndef PYRB_LEAF_REGION_LOG
+#define PYRB_LEAF_REGION_LOG 21
+#endif
+constexpr uint32_t kLeafRegionSlots = 1u << PYRB_LEAF_REGION_LOG;  // 2^21: 32 MB of 16-byte slots, a quarter of L2
 
 constexpr int kMaxLevels = 24;
 constexpr int kMaxPasses = 8;
@@ -99,6 +104,16 @@ struct BuildDesc {
     uint32_t* bref;          // [B] leaf index of an owner brick, kNoRef for the others
     uint4* leaf_table;       // {mask lo, mask hi, ~owner, leaf index}
     uint32_t leaf_cap;
+    // Tables larger than L2 are filled region by region: leaf_regions > 1 groups the
+    // bricks by the table region (leaf_cap / leaf_regions slots) of their mask's home
+    // slot first, so the inserts in flight at any time touch a slice that stays in L2.
+    uint32_t leaf_regions;
+    uint32_t leaf_region_shift;  // log2(leaf_cap / leaf_regions)
+    uint32_t* region_count;      // [leaf_regions] bricks per region (zero-initialised)
+    uint32_t* region_cursor;     // [leaf_regions] (zero-initialised)
+    uint32_t* region_zeroed;     // [leaf_regions] clearing tiles finished (zero-initialised)
+    uint64_t* pmask;             // [B] masks grouped by region (in the dead sort buffers)
+    uint32_t* pidx;              // [B] their brick indices
     uint32_t leafown_tiles;
     uint64_t* leafown_status;
     uint64_t* leaves;        // output

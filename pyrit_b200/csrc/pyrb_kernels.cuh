@@ -454,6 +454,11 @@ __global__ void __launch_bounds__(NT, PYRB_SORT_MIN_BLOCKS * kBlock / NT) k_sort
 // ---------------------------------------------------------------------------
 constexpr int kUniqAhead = 64;  // kept keys read ahead: the distinct keys of one brick
 
+// Table region of a mask's home slot (see BuildDesc::leaf_regions).
+__device__ __forceinline__ uint32_t leaf_region(const BuildDesc& d, uint64_t mask) {
+    return (uint32_t(mix64(mask)) & (d.leaf_cap - 1)) >> d.leaf_region_shift;
+}
+
 template <int IT, typename KeyT>
 constexpr size_t unique_smem_bytes() {
     constexpr size_t CAP = size_t(kBlock) * IT + kUniqAhead;
@@ -474,6 +479,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_ubase, s_bbase;
     __shared__ KeyT s_lead;
+    __shared__ uint32_t s_rcount[kMaxLeafRegions];  // the tile's bricks per leaf-table region
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // a sort tile larger than kBlock * IT entries is taken in parts, each a unique tile
     const uint32_t parts = d.tile_keys / (kBlock * IT);
@@ -492,6 +498,8 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     const KeyT inv = KeyT(1) << d.lb;
     const KeyT NONE = ~KeyT(0);  // never the brick of a key: key >> 6 has its top 6 bits clear
     const uint32_t wbase = warp * 32 * IT;
+    const bool regions = d.leaf_regions > 1;
+    if (threadIdx.x < kMaxLeafRegions) s_rcount[threadIdx.x] = 0;
 
     uint32_t total;
     {
@@ -642,9 +650,15 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
             d.bkey[g] = (segbits | uint64_t(s_key[lo])) >> 6;
             d.bmask[g] = mask;
             d.bfirst[g] = uint32_t(ubase + lo);
+            if (regions) atomicAdd(&s_rcount[leaf_region(d, mask)], 1u);
         } else {
             atomicOr(d.counters + kCtrError, kErrBound);
         }
+    }
+    if (regions) {
+        __syncthreads();
+        if (threadIdx.x < d.leaf_regions && s_rcount[threadIdx.x])
+            atomicAdd(d.region_count + threadIdx.x, s_rcount[threadIdx.x]);
     }
     if (d.chunked && threadIdx.x == 0 && total > 0) atomicMin(d.chunk_first + sp.seg, uint32_t(ubase));
     if (tile == ntiles - 1 && threadIdx.x == 0) {
@@ -664,9 +678,13 @@ __device__ __forceinline__ void claim_owner(uint4* slot, uint32_t idx) {
     if (ld_relaxed32(op) < inv) atomicMax(op, inv);
 }
 
-__device__ __forceinline__ uint32_t leaf_insert_at(uint4* table, uint32_t cap, uint64_t mask, uint32_t idx, uint32_t* err,
+// Linear probing wraps inside the slot's region of smask + 1 slots (the whole table
+// unless the table is filled region by region).
+__device__ __forceinline__ uint32_t probe_next(uint32_t h, uint32_t smask) { return (h & ~smask) | ((h + 1) & smask); }
+
+__device__ __forceinline__ uint32_t leaf_insert_at(uint4* table, uint32_t smask, uint64_t mask, uint32_t idx, uint32_t* err,
                                                    uint32_t h, uint32_t probe0) {
-    for (uint32_t probe = probe0; probe < cap; ++probe) {
+    for (uint32_t probe = probe0; probe <= smask; ++probe) {
         unsigned long long* kp = reinterpret_cast<unsigned long long*>(table + h);
         unsigned long long cur = ld_relaxed(reinterpret_cast<const uint64_t*>(kp));
         if (cur == 0) {
@@ -681,21 +699,21 @@ __device__ __forceinline__ uint32_t leaf_insert_at(uint4* table, uint32_t cap, u
             claim_owner(table + h, idx);
             return h;
         }
-        h = (h + 1) & (cap - 1);
+        h = probe_next(h, smask);
     }
     atomicOr(err, kErrTable);
     return 0;
 }
 
 __device__ __forceinline__ uint32_t leaf_insert(uint4* table, uint32_t cap, uint64_t mask, uint32_t idx, uint32_t* err) {
-    return leaf_insert_at(table, cap, mask, idx, err, uint32_t(mix64(mask)) & (cap - 1), 0);
+    return leaf_insert_at(table, cap - 1, mask, idx, err, uint32_t(mix64(mask)) & (cap - 1), 0);
 }
 
 // The first probe of two inserts, their loads and compare-and-swaps in flight together
 // (each thread takes two bricks per round: the inserts are latency-bound on random
 // table slots; measured 11 % faster than one at a time).
-__device__ __forceinline__ void leaf_insert2(uint4* table, uint32_t cap, bool w0, uint64_t m0, uint32_t i0, bool w1,
-                                             uint64_t m1, uint32_t i1, uint32_t* s0, uint32_t* s1, uint32_t* err) {
+__device__ __forceinline__ void leaf_insert2(uint4* table, uint32_t cap, uint32_t smask, bool w0, uint64_t m0, uint32_t i0,
+                                             bool w1, uint64_t m1, uint32_t i1, uint32_t* s0, uint32_t* s1, uint32_t* err) {
     const uint32_t h0 = uint32_t(mix64(m0)) & (cap - 1), h1 = uint32_t(mix64(m1)) & (cap - 1);
     unsigned long long* p0 = reinterpret_cast<unsigned long long*>(table + h0);
     unsigned long long* p1 = reinterpret_cast<unsigned long long*>(table + h1);
@@ -706,12 +724,12 @@ __device__ __forceinline__ void leaf_insert2(uint4* table, uint32_t cap, bool w0
     if (w0) {
         if (r0 == 0) { atomicMax(&table[h0].z, ~i0); *s0 = h0; }
         else if (r0 == m0) { claim_owner(table + h0, i0); *s0 = h0; }
-        else *s0 = leaf_insert_at(table, cap, m0, i0, err, (h0 + 1) & (cap - 1), 1);
+        else *s0 = leaf_insert_at(table, smask, m0, i0, err, probe_next(h0, smask), 1);
     }
     if (w1) {
         if (r1 == 0) { atomicMax(&table[h1].z, ~i1); *s1 = h1; }
         else if (r1 == m1) { claim_owner(table + h1, i1); *s1 = h1; }
-        else *s1 = leaf_insert_at(table, cap, m1, i1, err, (h1 + 1) & (cap - 1), 1);
+        else *s1 = leaf_insert_at(table, smask, m1, i1, err, probe_next(h1, smask), 1);
     }
 }
 
@@ -719,8 +737,58 @@ __device__ __forceinline__ void leaf_insert2(uint4* table, uint32_t cap, bool w0
 constexpr int kBrickIT = 8;
 constexpr int kBrickTile = kBlock * kBrickIT;
 
-// Leaf dedup insert, two bricks per thread per round. Equal masks of a warp row are
-// collapsed with match_any first: only the lowest brick of each group touches the table.
+// Bricks grouped by the leaf-table region of their mask (BuildDesc::leaf_regions):
+// per tile, ranks within each region by shared-memory counters, one global cursor
+// reservation per region; the order inside a region does not matter (the owner is
+// the minimum brick index whatever the insert order).
+__global__ void __launch_bounds__(kBlock) k_leaf_part(BuildDesc d) {
+    grid_dep_wait();
+    __shared__ uint32_t s_base[kMaxLeafRegions], s_cnt[kMaxLeafRegions], s_res[kMaxLeafRegions];
+    const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
+    const uint32_t R = d.leaf_regions;
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t r = 0; r < R; ++r) { s_base[r] = run; run += d.region_count[r]; }
+    }
+    for (uint32_t t0 = blockIdx.x * kBrickTile; t0 < B; t0 += gridDim.x * kBrickTile) {
+        if (threadIdx.x < R) s_cnt[threadIdx.x] = 0;
+        __syncthreads();
+        uint64_t m[kBrickIT];
+        uint32_t reg[kBrickIT], rk[kBrickIT];
+#pragma unroll
+        for (int j = 0; j < kBrickIT; ++j) {
+            const uint32_t b = t0 + j * kBlock + threadIdx.x;
+            m[j] = b < B ? d.bmask[b] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < kBrickIT; ++j) {
+            const uint32_t b = t0 + j * kBlock + threadIdx.x;
+            reg[j] = leaf_region(d, m[j]);
+            rk[j] = b < B ? atomicAdd(&s_cnt[reg[j]], 1u) : 0u;
+        }
+        __syncthreads();
+        if (threadIdx.x < R && s_cnt[threadIdx.x]) s_res[threadIdx.x] = atomicAdd(d.region_cursor + threadIdx.x, s_cnt[threadIdx.x]);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kBrickIT; ++j) {
+            const uint32_t b = t0 + j * kBlock + threadIdx.x;
+            if (b < B) {
+                const uint32_t p = s_base[reg[j]] + s_res[reg[j]] + rk[j];
+                if (p < B) {
+                    d.pmask[p] = m[j];
+                    d.pidx[p] = b;
+                } else {
+                    atomicOr(d.counters + kCtrError, kErrBound);
+                }
+            }
+        }
+        __syncthreads();  // s_cnt and s_res are reused by the next tile
+    }
+}
+
+// Leaf dedup insert in brick order, two bricks per thread per round. Equal masks of a
+// warp row are collapsed with match_any first: only the lowest brick of each group
+// touches the table.
 __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
     grid_dep_wait();
     const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
@@ -733,13 +801,85 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
         const unsigned g0 = __match_any_sync(kFull, m0), g1 = __match_any_sync(kFull, m1);
         const unsigned l0 = __ffs(g0) - 1, l1 = __ffs(g1) - 1;
         uint32_t s0 = 0, s1 = 0;
-        leaf_insert2(d.leaf_table, d.leaf_cap, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1, &s0, &s1,
-                     d.counters + kCtrError);
+        leaf_insert2(d.leaf_table, d.leaf_cap, d.leaf_cap - 1, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1,
+                     &s0, &s1, d.counters + kCtrError);
         s0 = __shfl_sync(kFull, s0, l0);
         s1 = __shfl_sync(kFull, s1, l1);
         if (v0) d.bslot[b0] = s0;
         if (v1) d.bslot[b1] = s1;
     }
+}
+
+// Leaf dedup insert region by region (BuildDesc::leaf_regions > 1), over the bricks
+// grouped by region (k_leaf_part). The tiles of a region, taken in order, first clear
+// the region's slots (the table is not cleared before the build), then insert its
+// bricks once every clearing tile of the region has finished: the region's slots are
+// written while they sit in L2 and the inserts find them there. Probing wraps inside
+// the region. A tile waits only for tiles with smaller numbers, which are running or
+// done; the wait is bounded.
+constexpr uint32_t kZeroSlots = 2048;        // slots a clearing tile clears (32 KB)
+constexpr uint32_t kInsTile = 2 * kBlock;    // bricks an insert tile takes
+__global__ void __launch_bounds__(kBlock) k_leaf_insert_regions(BuildDesc d) {
+    grid_dep_wait();
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_tbase[kMaxLeafRegions + 1], s_ibase[kMaxLeafRegions + 1];
+    const uint32_t R = d.leaf_regions, S = d.leaf_cap / R, smask = S - 1;
+    const uint32_t nz = (S + kZeroSlots - 1) / kZeroSlots;
+    if (threadIdx.x == 0) {
+        uint32_t t = 0, b = 0;
+        for (uint32_t r = 0; r < R; ++r) {
+            s_tbase[r] = t;
+            s_ibase[r] = b;
+            const uint32_t c = d.region_count[r];
+            t += nz + (c + kInsTile - 1) / kInsTile;
+            b += c;
+        }
+        s_tbase[R] = t;
+        s_ibase[R] = b;
+    }
+    const uint32_t tile = dyn_tile(d.counters, 11, &s_tile);  // its barrier publishes s_tbase
+    if (tile >= s_tbase[R]) return;
+    uint32_t r = 0;
+    while (s_tbase[r + 1] <= tile) ++r;
+    const uint32_t k = tile - s_tbase[r];
+    uint4* region = d.leaf_table + size_t(r) * S;
+    if (k < nz) {
+        const uint32_t end = min(S, (k + 1) * kZeroSlots);
+        for (uint32_t i = k * kZeroSlots + threadIdx.x; i < end; i += kBlock) region[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(d.region_zeroed + r, 1u);
+        }
+        return;
+    }
+    if (threadIdx.x == 0) {
+        uint32_t spins = 0;
+        while (ld_acquire32(d.region_zeroed + r) < nz) {
+            if (++spins > kSpinLimit) { atomicOr(d.counters + kCtrError, kErrSpin); break; }
+            if (spins > 8) __nanosleep(128);
+        }
+    }
+    __syncthreads();
+    const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t i0 = s_ibase[r] + (k - nz) * kInsTile + threadIdx.x, i1 = i0 + kBlock, iend = s_ibase[r + 1];
+    const uint32_t b0 = i0 < iend ? d.pidx[i0] : 0u, b1 = i1 < iend ? d.pidx[i1] : 0u;
+    const bool v0 = i0 < iend && b0 < B, v1 = i1 < iend && b1 < B;  // b >= B: never, unless counts disagree
+    if ((i0 < iend && !v0) || (i1 < iend && !v1)) atomicOr(d.counters + kCtrError, kErrBound);
+    const uint64_t m0 = v0 ? d.pmask[i0] : 0, m1 = v1 ? d.pmask[i1] : 0;  // masks are never 0
+    const unsigned g0 = __match_any_sync(kFull, m0), g1 = __match_any_sync(kFull, m1);
+    const unsigned l0 = __ffs(g0) - 1, l1 = __ffs(g1) - 1;
+    uint32_t s0 = 0, s1 = 0;
+    leaf_insert2(d.leaf_table, d.leaf_cap, smask, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1, &s0, &s1,
+                 d.counters + kCtrError);
+    s0 = __shfl_sync(kFull, s0, l0);
+    s1 = __shfl_sync(kFull, s1, l1);
+    // the lowest lane of a group need not hold its lowest brick: the others claim too
+    if (v0 && lane != l0) claim_owner(d.leaf_table + s0, b0);
+    if (v1 && lane != l1) claim_owner(d.leaf_table + s1, b1);
+    if (v0) d.bslot[b0] = s0;
+    if (v1) d.bslot[b1] = s1;
 }
 
 // ---------------------------------------------------------------------------

@@ -219,6 +219,28 @@ def test_brick_runs_all_deleted(gb):
     assert_same_build(gb.build(5, 3, dev(pts)).download(), orc.gb_build(5, 3, pts), label="all deleted")
 
 
+@pytest.mark.parametrize("lf", [50, 25])
+def test_leaf_table_regions_with_repeated_masks(gb, lf):
+    """A leaf table larger than 32 MB is filled region by region (bricks grouped by the
+    region of their mask's home slot): 1.5 M bricks of one voxel each at one of four
+    places, so four masks repeat ~375 k times each across regions and warps."""
+    rng = np.random.default_rng(17)
+    cells = rng.choice(128 ** 3, 1_500_000, replace=False)
+    bx, by, bz = cells % 128, (cells // 128) % 128, cells // (128 * 128)
+    corner = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [3, 3, 3]])[rng.integers(0, 4, len(cells))]
+    pts = np.stack([bx * 4 + corner[:, 0], by * 4 + corner[:, 1], bz * 4 + corner[:, 2],
+                    rng.integers(1, 6, len(cells))], 1).astype(np.uint32)
+    o = orc.gb_build(9, 5, pts)
+    old = gb.get_tuning()
+    try:
+        gb.set_tuning(8, 4096, lf)
+        g = gb.build(9, 5, dev(pts)).download()
+    finally:
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+    assert len(o.leaves) == 4
+    assert_same_build(g, o, label=f"leaf regions, load factor {lf}")
+
+
 def test_invalid_arguments(gb):
     from pyrit_b200.native import PyrbError
     pts = dev(np.array([[1, 1, 1, 1]], np.uint32))
