@@ -221,9 +221,10 @@ def test_brick_runs_all_deleted(gb):
 
 @pytest.mark.parametrize("lf", [50, 25])
 def test_leaf_table_regions_with_repeated_masks(gb, lf):
-    """A leaf table larger than 32 MB is filled region by region (bricks grouped by the
-    region of their mask's home slot): 1.5 M bricks of one voxel each at one of four
-    places, so four masks repeat ~375 k times each across regions and warps."""
+    """A leaf table larger than one region (64 MB; here at load factor 25 %) is filled
+    region by region (bricks grouped by the region of their mask's home slot, each
+    region cleared right before its inserts): 1.5 M bricks of one voxel each at one of
+    four places, so four masks repeat ~375 k times each across regions and warps."""
     rng = np.random.default_rng(17)
     cells = rng.choice(128 ** 3, 1_500_000, replace=False)
     bx, by, bz = cells % 128, (cells // 128) % 128, cells // (128 * 128)
