@@ -705,10 +705,6 @@ __device__ __forceinline__ uint32_t leaf_insert_at(uint4* table, uint32_t smask,
     return 0;
 }
 
-__device__ __forceinline__ uint32_t leaf_insert(uint4* table, uint32_t cap, uint64_t mask, uint32_t idx, uint32_t* err) {
-    return leaf_insert_at(table, cap - 1, mask, idx, err, uint32_t(mix64(mask)) & (cap - 1), 0);
-}
-
 // The first probe of two inserts, their loads and compare-and-swaps in flight together
 // (each thread takes two bricks per round: the inserts are latency-bound on random
 // table slots; measured 11 % faster than one at a time).
