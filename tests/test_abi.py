@@ -60,3 +60,18 @@ def test_struct_layouts():
     assert ctypes.sizeof(native.BuiltC) == 88
     assert ctypes.sizeof(native.ChunkBatch) == 32
     assert ctypes.sizeof(native.Exec) == 32
+
+
+def test_autotune_offers_only_supported_settings():
+    """8192-entry tiles exist for 8- and 9-bit digits only; the sweep skips the rest."""
+    from pyrit_b200 import autotune
+    assert 8192 in autotune.TILE_KEYS
+    offered = [(rb, tk) for rb in autotune.RADIX_BITS for tk in autotune.TILE_KEYS if autotune.supported(rb, tk)]
+    assert (9, 8192) in offered and (8, 8192) in offered
+    assert all(tk != 8192 or rb in (8, 9) for rb, tk in offered)
+    L = native.lib()
+    for rb, tk in offered:  # every offered setting is accepted by the library
+        t = native.Tuning(radix_bits=rb, tile_keys=tk, load_factor_pct=50)
+        assert L.pyrb_set_tuning(ctypes.byref(t)) == 0
+    t = native.Tuning(radix_bits=0, tile_keys=0, load_factor_pct=50)
+    assert L.pyrb_set_tuning(ctypes.byref(t)) == 0
