@@ -288,7 +288,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 #define PYRB_SORT_WINDOW 2
 #endif
 constexpr int kSortWindow = PYRB_SORT_WINDOW;  // predecessors per look-back round
-constexpr int kMatchMaxGroups = 16;  // distinct digits per warp above which ballots are cheaper
+#ifndef PYRB_MATCH_MAX_GROUPS
+#define PYRB_MATCH_MAX_GROUPS 16
+#endif
+constexpr int kMatchMaxGroups = PYRB_MATCH_MAX_GROUPS;  // distinct digits per warp above which ballots are cheaper
 
 // 4 resident 256-thread tiles (or 2 of 512 threads) per SM: caps the pass at 64
 // registers (the 16-key tiles spill a few words, cheaper than the lost occupancy)
