@@ -172,6 +172,66 @@ def cpu_builder_time(vox, ed, reps=1, log2=8):
     return best, n
 
 
+def stage_profile(log2, rt, dpts, sptr, flush, steps):
+    """Mean duration (ms) of every stage of a build: CUDA events after every launch
+    (pyrb_profile_enable), over `steps` builds with L2 flushed before each."""
+    from pyrit_b200 import gpu_build, native
+    L = native.lib()
+    L.pyrb_profile_enable(1)
+    stage = {}
+    try:
+        for s in range(steps):
+            flush.fill_(s & 0xFF)
+            b = gpu_build.build(log2, rt, dpts, stream=sptr)
+            ms = (ctypes.c_float * 256)()
+            names = ctypes.create_string_buffer(256 * 32)
+            k = L.pyrb_profile_read(ms, names, 32, 256)
+            for i in range(min(k, 256)):
+                nm = names.raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode()
+                stage.setdefault(nm, []).append(ms[i])
+            b.free()
+    finally:
+        L.pyrb_profile_enable(0)
+    return {k: statistics.mean(v) for k, v in stage.items()}
+
+
+def kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak):
+    """Algorithmic bytes / CUDA-event time of the build's HBM kernels against `peak`
+    (GB/s). Bytes per launch (the roofline basis of the design notes):
+      encode_hist   n_in (16 + kb + 4)           read PyrVoxels, write key + value
+      sort_pass     n_in 2 (kb + 4)              read and write key + value
+      unique_brick  n_in (kb + 4) + 12 n_u + 20 B
+      leaf_part     20 B; leaf_insert 28 B; leaf_own 16 B + 8 L
+      node level l  20 C + 28 P + 4 W            children C, parents P, words W written
+    with B bricks, L leaves, W = 2 U + C U / P for U unique parents."""
+    B = int(st.brick_count)
+    out = {}
+
+    def add(name, ms, nbytes):
+        if ms and ms > 0:
+            gbs = nbytes / (ms / 1e3) / 1e9
+            out[name] = {"ms": round(ms, 4), "alg_bytes": int(nbytes), "gbs": round(gbs, 1),
+                         "frac": round(gbs / peak, 4)}
+
+    add("encode_hist", stage_ms.get("encode_hist"), n_in * (16 + key_bytes + 4))
+    sort_keys = [k for k in stage_ms if k.startswith("sort_pass")]
+    if sort_keys:
+        add("sort_pass", statistics.mean(stage_ms[k] for k in sort_keys), n_in * 2 * (key_bytes + 4))
+    add("unique_brick", stage_ms.get("unique_brick"), n_in * (key_bytes + 4) + 12 * n_u + 20 * B)
+    add("leaf_part", stage_ms.get("leaf_part"), 20 * B)
+    add("leaf_insert", stage_ms.get("leaf_insert"), 28 * B)
+    add("leaf_own", stage_ms.get("leaf_own"), 16 * B + 8 * leaves)
+    for lv in range(2, 24):
+        nb, no = stage_ms.get("node_build:%d" % lv), stage_ms.get("node_own:%d" % lv)
+        if nb is None or no is None:
+            continue
+        C = B if lv == 2 else int(st.level_parents[lv - 1])
+        P, U = int(st.level_parents[lv]), int(st.level_unique[lv])
+        W = 2 * U + (C * U // P if P else 0)
+        add("node_dedup:%d" % lv, nb + no, 20 * C + 28 * P + 4 * W)
+    return out
+
+
 def sub_volume(pts, log2):
     """Entries of the workload inside the octant [0, 2^log2)^3 (a bounded CPU sample)."""
     m = (pts[:, 0] < (1 << log2)) & (pts[:, 1] < (1 << log2)) & (pts[:, 2] < (1 << log2))
@@ -299,6 +359,7 @@ def run_ours(args):
     o = native.BuiltC()
     native.check(L.pyrb_build_finish(ctypes.c_void_p(counts_ptr), ctypes.byref(o)))
     assert o.voxel_count == n_u, "result changed between runs"
+    sizes = {"leaves": o.leaf_count, "node_words": o.node_words, "prims": o.prim_count}
     step_ms = [a.elapsed_time(b) for a, b in evs]
     t_ms = sum(step_ms)
     t_max = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
@@ -308,21 +369,7 @@ def run_ours(args):
     value = world * n_u * args.steps / (t_ms / 1e3)
 
     # per-stage profile (CUDA events after every launch of the build)
-    L.pyrb_profile_enable(1)
-    stage = {}
-    prof_steps = min(args.steps, 20)
-    for s in range(prof_steps):
-        flush.fill_(s & 0xFF)
-        b = gpu_build.build(LOG2, RT, dpts, stream=sptr)
-        ms = (ctypes.c_float * 256)()
-        names = ctypes.create_string_buffer(256 * 32)
-        k = L.pyrb_profile_read(ms, names, 32, 256)
-        for i in range(min(k, 256)):
-            nm = names.raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode()
-            stage.setdefault(nm, []).append(ms[i])
-        b.free()
-    L.pyrb_profile_enable(0)
-    stage_ms = {k: statistics.mean(v) for k, v in stage.items()}
+    stage_ms = stage_profile(LOG2, RT, dpts, sptr, flush, min(args.steps, 20))
     sort_keys = [k for k in stage_ms if k.startswith("sort_pass")]
     sort_ms = statistics.mean(stage_ms[k] for k in sort_keys)
     key_bytes = 4 if 3 * LOG2 + 1 <= 32 else 8
@@ -332,7 +379,7 @@ def run_ours(args):
     traffic = committed_traffic("k_sort_pass", args.workload)
 
     # whole-build algorithmic bytes (read input once; write keys+attrs, leaves, nodes, prims)
-    alg_bytes = 16 * n_in + 12 * n_u + 8 * o.leaf_count + 4 * o.node_words + 40 * o.prim_count
+    alg_bytes = 16 * n_in + 12 * n_u + 8 * sizes["leaves"] + 4 * sizes["node_words"] + 40 * sizes["prims"]
     hbm_gbs = alg_bytes * args.steps / (t_ms / 1e3) / 1e9 / world
 
     # e2e through the public C ABI with host input
@@ -407,14 +454,29 @@ def run_ours(args):
                        "ratio": (st.level_parents[lv] / st.level_unique[lv]) if st.level_unique[lv] else None}
              for lv in range(2, LOG2)}
 
+    # the other configurations of the metric, on one GPU: the batched build of 1024
+    # mixed chunks against the per-chunk loop, served requests at 20k/s, and the
+    # worst-case 1024^3 build with its per-kernel roofline
+    extras = {}
+    if world == 1 and not args.no_extras:
+        for name, fn in (("batched", lambda: run_batched(args, emit=False)),
+                         ("served", lambda: run_served(args, emit=False)),
+                         ("worst_case", lambda: run_worst_case(args))):
+            try:
+                extras[name] = fn()
+            except Exception as exc:  # reported in the line, the headline stands
+                extras[name] = {"error": "%s: %s" % (type(exc).__name__, exc)}
+            gpu_build.set_tuning(0, 0, 50)  # the autotuned setting of one form does not leak into the next
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded value noise + edit overlay)",
             "config": {"workload": desc, "log2_size": LOG2, "rt_log2": RT, "entries": n_in, "unique_voxels": n_u,
-                       "bricks": st.brick_count, "leaves": o.leaf_count, "node_words": o.node_words,
-                       "prims": o.prim_count, "sort_passes": st.sort_passes, "radix_bits": st.radix_bits,
+                       "bricks": st.brick_count, "leaves": sizes["leaves"], "node_words": sizes["node_words"],
+                       "prims": sizes["prims"], "sort_passes": st.sort_passes, "radix_bits": st.radix_bits,
                        "l2": "flushed between steps (512 MiB write outside the timed events)",
                        "key_bits": 8 * key_bytes, "dedup_per_level": dedup,
                        "scratch_bytes": int(st.scratch_bytes), "output_bytes_bound": int(st.output_bytes),
@@ -436,11 +498,75 @@ def run_ours(args):
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_worst_case(args, reps=3):
+    """Worst-case dedup build at full size: 1024^3 i.i.d. Bernoulli(0.15) occupancy,
+    materials 1..255, +10^6 uniform set/remove edits (162 M entries, 2.6 GB of input in
+    HBM). Device time per build (CUDA events, L2 flushed between builds), the
+    algorithmic-bytes roofline of every HBM kernel from per-stage events, and the
+    dedup ratio (parents formed / unique nodes kept) per level."""
+    import torch
+    from pyrit_b200 import gpu_build, native
+    L = native.lib()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    LOG2, RT, desc, _ = SPECS["bernoulli1024"]
+    vox, ed, pts = make_input("bernoulli1024")
+    n_in = len(pts)
+    dpts = torch.from_numpy(pts.view(np.int32)).cuda()
+    del vox, ed, pts
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    counts = torch.zeros(native.COUNTS_WORDS, dtype=torch.int32).pin_memory()
+    ex = native.Exec()
+    ex.stream = ctypes.c_void_p(sptr)
+
+    def build_async():
+        out = native.BuiltC()
+        native.check(L.pyrb_build_async(ctypes.byref(ex), LOG2, RT, 0, 0, 0, dpts.data_ptr(), n_in,
+                                        ctypes.c_void_p(counts.data_ptr()), ctypes.byref(out)))
+        return out
+
+    for _ in range(2):
+        L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(build_async()))
+    torch.cuda.synchronize()
+    times = []
+    for s in range(reps):
+        flush.fill_(s & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        o = build_async()
+        b.record(stream)
+        L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(o))
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    o = native.BuiltC()
+    native.check(L.pyrb_build_finish(ctypes.c_void_p(counts.data_ptr()), ctypes.byref(o)))
+    n_u, leaves = o.voxel_count, o.leaf_count
+    st = gpu_build.last_stats()
+    stage_ms = stage_profile(LOG2, RT, dpts, sptr, flush, reps)
+    peak, peak_kind = load_peaks()
+    key_bytes = 4 if 3 * LOG2 + 1 <= 32 else 8
+    kernels = kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak)
+    dedup = {str(lv): {"parents": int(st.level_parents[lv]), "unique": int(st.level_unique[lv]),
+                       "ratio": (st.level_parents[lv] / st.level_unique[lv]) if st.level_unique[lv] else None}
+             for lv in range(2, LOG2)}
+    t = statistics.median(times)
+    del dpts, flush
+    torch.cuda.empty_cache()
+    return {"workload": desc, "entries": n_in, "unique_voxels": n_u, "bricks": int(st.brick_count),
+            "leaves": leaves, "ms_per_build": t, "voxels_per_s": n_u / (t / 1e3),
+            "sort_passes": int(st.sort_passes), "radix_bits": int(st.radix_bits),
+            "peak_gbs": peak, "peak_kind": peak_kind, "kernels": kernels, "dedup_per_level": dedup,
+            "scratch_plus_output_bytes_per_entry": (st.scratch_bytes + st.output_bytes) / n_in,
+            "how": "pyrb_build_async on the resident input, CUDA events around each build (median of %d), "
+                   "per-stage events from pyrb_profile_enable" % reps}
 
 
 def path_edit_bench(out, roots, first_voxel, first_prim, log2s, nz, per_chunk=32, reps=3):
@@ -575,6 +701,13 @@ def run_batched(args, emit=True):
                                     fprim.data_ptr(), ctypes.byref(out)))
     rts, fv = roots.numpy().view(np.uint32), first.numpy().view(np.uint32)
     nz = np.nonzero(rts != 0xFFFFFFFF)[0]
+    # every chunk's voxel count as the batch stores it: the root's count word
+    from pyrit_b200 import _cudart
+    batch_voxels = np.zeros(K, np.uint32)
+    one = np.zeros(1, np.uint32)
+    for c in nz:
+        _cudart.dtoh(one.ctypes.data, out.nodes + 4 * (int(rts[c]) + 1), 4)
+        batch_voxels[c] = one[0]
     pfirst = np.concatenate([fv[nz], [out.voxel_count]]).astype(np.uint32)
     pal_t, pack_t = [], []
     for _ in range(3):
@@ -601,7 +734,10 @@ def run_batched(args, emit=True):
                "scan_gbs": 4 * n_attr / (min(pal_t) / 1e3) / 1e9,
                "pack_gbs": (4 * n_attr + 4 * words) / (min(pack_t) / 1e3) / 1e9}
 
-    # per-chunk loop of plain builds (asynchronous, one stream)
+    # per-chunk loop of plain builds (asynchronous, one stream; each chunk's counts land
+    # in its own pinned slot)
+    loop_counts = torch.zeros((K, native.COUNTS_WORDS), dtype=torch.int32).pin_memory()
+
     def loop_once():
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -609,7 +745,7 @@ def run_batched(args, emit=True):
             out = native.BuiltC()
             n = int(offs[c + 1] - offs[c])
             native.check(L.pyrb_build_async(ctypes.byref(ex), int(log2s[c]), 5, 0, 0, 0,
-                                            vox.data_ptr() + 16 * int(offs[c]), n, counts.data_ptr(),
+                                            vox.data_ptr() + 16 * int(offs[c]), n, loop_counts[c].data_ptr(),
                                             ctypes.byref(out)))
             L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(out))
         b.record(stream)
@@ -620,12 +756,22 @@ def run_batched(args, emit=True):
     a, b = loop_once()
     torch.cuda.synchronize()
     t_loop = a.elapsed_time(b)
+    # the batch builds what the loop builds: each chunk's voxel count, empty chunks included
+    loop_voxels = np.zeros(K, np.uint32)
+    for c in range(K):
+        f = native.BuiltC()
+        native.check(L.pyrb_build_finish(ctypes.c_void_p(loop_counts[c].data_ptr()), ctypes.byref(f)))
+        loop_voxels[c] = f.voxel_count
+    mismatch = np.nonzero(loop_voxels != batch_voxels)[0]
+    assert len(mismatch) == 0, "batched and per-chunk voxel counts differ at chunks %s" % mismatch[:8].tolist()
     comb = shard.combine({"voxels": n_u, "entries": total, "chunks": K, "batched_ms": t_batched, "loop_ms": t_loop})
     n_u, total, t_batched, t_loop = int(comb["voxels"]), int(comb["entries"]), comb["batched_ms"], comb["loop_ms"]
     res = {"chunks": int(comb["chunks"]), "entries": total, "unique_voxels": n_u, "batched_ms": t_batched,
            "batched_voxels_per_s": n_u / (t_batched / 1e3), "per_chunk_loop_ms": t_loop,
            "per_chunk_loop_voxels_per_s": n_u / (t_loop / 1e3), "speedup_vs_per_chunk_loop": t_loop / t_batched,
            "n_gpus": world, "scaling": "weak", "chunks_per_gpu": K, "palette": palette, "path_edit": path_edit,
+           "per_chunk_voxels_checked": "nodes[root + 1] of every chunk of the batch equals the voxel count of its "
+                                       "plain build in the loop (%d chunks, %d empty)" % (K, K - len(nz)),
            "tuning": {k: best[k] for k in ("radix_bits", "tile_keys", "load_factor_pct")},
            "edges": {str(1 << l): int((log2s == l).sum()) for l in (5, 6, 7, 8)}}
     if dist:
@@ -737,7 +883,9 @@ def main():
     ap.add_argument("--max-batch-voxels", type=int, default=64 << 20)
     ap.add_argument("--chunks", type=int, default=1024)
     ap.add_argument("--batched-reps", type=int, default=3)
-    ap.add_argument("--tune-budget", type=float, default=30.0)
+    ap.add_argument("--tune-budget", type=float, default=15.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default run: skip the batched, served and worst-case objects")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -41,6 +41,7 @@ typedef int32_t pyrb_result;
 #define PYRB_OK                      0
 #define PYRB_ERROR_INVALID_ARGUMENT -1
 #define PYRB_ERROR_OUT_OF_MEMORY    -3
+#define PYRB_ERROR_CAPACITY         -4  /* world path: a chunk's generator count exceeds the capacity */
 #define PYRB_ERROR_CUDA             -6
 
 /* Memory and stream of a build (replaces gpu_build.Exec, src/gpu_build.zig:14-23).
@@ -139,8 +140,11 @@ PYRB_API pyrb_result pyrb_build_chunks(const pyrb_exec* e, uint32_t log2_size, u
  * coordinates, chunk c at [edit_offsets[c], edit_offsets[c+1]) (device u32[count+1]);
  * edit_total = edit_offsets[count] (host copy, sizes the scratch).
  * Edits act as if applied after the generated voxels in list order: attribute 0
- * removes, anything else sets. Counts above capacity are clamped (the reference
- * grows the capacity and retries, src/world.zig:989-996). */
+ * removes, anything else sets. Nothing is ever cut off: when a generator count
+ * exceeds `capacity`, no result is kept and the call returns PYRB_ERROR_CAPACITY;
+ * pyrb_last_capacity_need() then gives the largest count, so the host can grow the
+ * capacity, generate again and retry, as the reference's world job does
+ * (src/world.zig:968-996, growCapacity :850-879). */
 PYRB_API pyrb_result pyrb_build_chunks_edits(const pyrb_exec* e, uint32_t log2_size, uint32_t rt_log2_req,
                                              uint32_t count, uint32_t capacity, uint64_t voxels, uint64_t counts,
                                              uint64_t edits, uint64_t edit_offsets, uint32_t edit_total,
@@ -226,20 +230,23 @@ PYRB_API void pyrb_profile_enable(int on);
 PYRB_API uint32_t pyrb_profile_read(float* ms, char* names, uint32_t name_len, uint32_t cap);
 
 /* A plain build that allocates no device memory (no counterpart in the reference).
- * For callers that cannot allocate while they build: a render or frame loop that must
- * not call cudaMalloc (it synchronises the whole device), code running while a stream
- * is captured into a CUDA graph (allocation calls are illegal there), or engines whose
- * device memory is fully budgeted up front. All scratch lives in a fixed 64 MiB
- * device array inside the library (held by every GPU that loads the library until the
- * process exits); the caller passes the input (device PyrVoxel[n_new]) and every
- * output buffer (device memory) with its capacity in elements. Limits: log2_size in
- * [3, 8], n_new <= 2^20; larger requests and too small outputs return
- * PYRB_ERROR_INVALID_ARGUMENT with the sizes needed. The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress), so make one call per device
- * before any stream capture. All calls share the one array: calls whose work
- * overlaps on the GPU (other streams, other threads) race and corrupt each other --
- * serialise them. Output layout and values are identical to pyrb_build with
- * n_old = 0. Synchronises `stream` once at the end to read the counts. */
+ * For callers that cannot allocate while they build: a render or frame loop must not
+ * call cudaMalloc, which synchronises the whole device and stalls the frame, and an
+ * engine whose device memory is budgeted up front has no allocator to hand over for
+ * scratch. All scratch lives in a fixed 64 MiB device array inside the library (held
+ * by every GPU that loads the library until the process exits); the caller passes the
+ * input (device PyrVoxel[n_new]) and every output buffer (device memory) with its
+ * capacity in elements. Limits: log2_size in [3, 8], n_new <= 2^20; larger requests
+ * and too small outputs return PYRB_ERROR_INVALID_ARGUMENT with the sizes needed.
+ * The first call on a device (with that device current) looks up the array's device
+ * address with cudaGetSymbolAddress; make that first call before any stream capture.
+ * The address is kept for the process (after cudaDeviceReset, load the library
+ * again). All calls share the one array, which keeps the last call's contents (each
+ * call clears what must start at zero): calls whose work overlaps on the GPU (other
+ * streams, other threads) race and corrupt each other -- serialise them. The buffers
+ * in `out` stay the caller's: never pass this pyrb_built to pyrb_built_free. Output
+ * layout and values are identical to pyrb_build with n_old = 0; pyrb_last_stats
+ * reports the call. Synchronises `stream` once at the end to read the counts. */
 PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32_t rt_log2_req, uint64_t edits,
                                         uint32_t n_new, uint64_t nodes, uint32_t node_capacity, uint64_t leaves,
                                         uint32_t leaf_capacity, uint64_t keys, uint64_t attrs,
@@ -322,6 +329,29 @@ typedef struct pyrb_path_edit_job {  /* the reference's PathEditJob, field for f
 PYRB_API pyrb_result pyrb_path_edit(const pyrb_exec* e, uint64_t nodes, uint64_t leaves, uint64_t attributes,
                                     pyrb_path_edit_job* jobs, uint32_t count, const uint32_t* edits,
                                     uint32_t n_edits);
+
+/* Device memory a build would take, computed on the host without building (the upper
+ * bounds the build allocates from): `entries` raw input entries (n_old + n_new for
+ * pyrb_build; total for pyrb_build_chunks; count * capacity + edit_total for
+ * pyrb_build_chunks_edits; voxel_total + edit_total for a batch) in `count` chunks of
+ * edge 2^log2_size, or, when chunk_log2 (host u32[count]) is given, of edges
+ * 2^chunk_log2[c] (a pyrb_build_batch; log2_size is ignored). Uses the current tuning.
+ * scratch_bytes: freed when the build returns; output_bytes: the six output buffers.
+ * The reference bounds its build scratch with a counting Exec (tests/cpu_test.zig:1559-1629). */
+PYRB_API pyrb_result pyrb_build_memory(uint32_t log2_size, uint32_t count, const uint32_t* chunk_log2,
+                                       uint64_t entries, uint64_t* scratch_bytes, uint64_t* output_bytes);
+
+/* Largest generator count of the calling thread's last PYRB_ERROR_CAPACITY result
+ * (the capacity to grow to; src/world.zig:968-996), 0 if there was none. */
+PYRB_API uint32_t pyrb_last_capacity_need(void);
+
+/* Diagnostic of the device-side error path: runs one bounded wait that nothing ends
+ * (which 0: the per-digit look-back of the sort passes; 1: the warp look-back of the
+ * compaction kernels) on the exec's stream. The wait gives up after its poll limit
+ * (about a second), sets the error word and returns, so the context stays usable; the
+ * call returns what a build returns then: PYRB_ERROR_CUDA with the message "device-side
+ * build error ... look-back wait limit". Synchronises the exec's stream. */
+PYRB_API pyrb_result pyrb_selftest_wait_limit(const pyrb_exec* e, uint32_t which);
 
 /* Library version (major << 16 | minor). */
 PYRB_API uint32_t pyrb_version(void);

@@ -274,10 +274,24 @@ TailDesc make_tail(uint32_t lv0, const uint32_t* P, const std::vector<LevelDesc>
     return T;
 }
 
-pyrb_result device_error(uint32_t bits) {
-    return fail(PYRB_ERROR_CUDA, "device-side build error 0x%x (%s%s%s)", bits,
+thread_local uint32_t g_capacity_need = 0;
+
+// Result of a build whose counter block reports an error. A generator count above
+// the chunk capacity alone is PYRB_ERROR_CAPACITY with the capacity that would have
+// held every chunk (nothing is cut off: the build's outputs are discarded); any
+// other error bit is a device-side failure.
+pyrb_result device_error(const uint32_t* ctr) {
+    const uint32_t bits = ctr[kCtrError];
+    if (bits == kErrCapacity) {
+        g_capacity_need = ctr[kCtrNeed];
+        return fail(PYRB_ERROR_CAPACITY,
+                    "a chunk holds %u generated voxels, more than the capacity; grow the capacity to at least %u "
+                    "and generate again (nothing was cut off, no result was kept)",
+                    ctr[kCtrNeed], ctr[kCtrNeed]);
+    }
+    return fail(PYRB_ERROR_CUDA, "device-side build error 0x%x (%s%s%s%s)", bits,
                 (bits & kErrSpin) ? "look-back wait limit " : "", (bits & kErrTable) ? "dedup table full " : "",
-                (bits & kErrBound) ? "upper bound exceeded" : "");
+                (bits & kErrBound) ? "upper bound exceeded " : "", (bits & kErrCapacity) ? "chunk over capacity" : "");
 }
 
 void fill_counts(const uint32_t* ctr, pyrb_built* out) {
@@ -366,15 +380,45 @@ void auto_tuning(uint32_t sort_bits, uint32_t* rb, uint32_t* tile_keys) {
     *tile_keys = nine ? 8192u : 4096u;
 }
 
-pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint32_t* host_counts = nullptr) {
-    if (!out) return fail(PYRB_ERROR_INVALID_ARGUMENT, "out is NULL");
-    std::memset(out, 0, sizeof(*out));
+// Everything a build needs that the host can work out before any GPU work: the
+// digit plan, the upper bounds of every count, the scratch layout and the output
+// sizes. Used by the builds themselves, by the fixed-array build and by
+// pyrb_build_memory (how much device memory a build would take).
+struct Plan {
+    BuildDesc d;
+    uint32_t K = 1, rb = 8, it = 16, lf = 50, passes = 1, min_log2 = 3, rt = 3, n = 0, nmax = 1, B = 1;
+    bool chunked = false, key64 = false;
+    uint32_t P[kMaxLevels + 2] = {};
+    uint32_t cap[kMaxLevels + 2] = {}, btiles[kMaxLevels + 2] = {}, otiles[kMaxLevels + 2] = {};
+    uint64_t o_counters = 0, o_hist = 0, o_sort_status = 0, o_uniq_status = 0, o_brick_status = 0,
+             o_leafown_status = 0, o_leaf_table = 0, o_regions = 0;
+    uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
+    uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
+    uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bslot = 0, o_bref = 0;
+    uint64_t o_set[2][7] = {};
+    uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
+    // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
+    uint64_t out_size[6] = {};
+    uint64_t out_bytes() const {
+        uint64_t s = 0;
+        for (uint64_t v : out_size) s += v;
+        return s;
+    }
+};
+
+// Digit width, tile and load factor of a build: the fixed tuning given, else the
+// library's current tuning (64-bit keys: 8-bit digits on 2048-key tiles).
+struct Tune {
+    uint32_t rb, tile_keys, lf;
+};
+
+pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     const uint32_t log2 = job.log2;
     if (log2 < 3 || log2 > 20) return fail(PYRB_ERROR_INVALID_ARGUMENT, "log2_size must lie in [3, 20] (got %u)", log2);
     const uint32_t lb = 3 * log2;
-    const bool key64 = lb + 1 > 32;
-    const uint32_t K = job.K;
-    const bool chunked = job.mode == kModeChunks || job.mode == kModeChunksEdits || job.mode == kModeBatch;
+    p.key64 = lb + 1 > 32;
+    const uint32_t K = p.K = job.K;
+    p.chunked = job.mode == kModeChunks || job.mode == kModeChunksEdits || job.mode == kModeBatch;
     // chunks per edge (kModeBatch mixes edges; every other mode has K chunks of edge 2^log2)
     uint64_t per_log2[24] = {};
     uint32_t min_log2 = log2;
@@ -388,14 +432,13 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     } else {
         per_log2[log2] = K;
     }
-    if (chunked) {
+    p.min_log2 = min_log2;
+    if (p.chunked) {
         uint32_t bits = 0;
         while ((uint64_t(1) << bits) < K) ++bits;
         if (lb + bits + 1 > 64) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many chunks for this chunk size");
     }
-    const uint32_t rt = std::min(std::max(job.rt_req, 3u), min_log2);
-    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
-    Mem mem{e, st};
+    const uint32_t rt = p.rt = std::min(std::max(job.rt_req, 3u), min_log2);
 
     // raw entries (upper bound for the chunk modes)
     uint64_t n64 = 0;
@@ -407,17 +450,26 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
         default: n64 = job.n_new; break;
     }
     if (n64 >= (uint64_t(1) << 31)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many entries for one build (%llu)", (unsigned long long)n64);
-    const uint32_t n = uint32_t(n64);
-    const uint32_t nmax = std::max(n, 1u);
+    const uint32_t n = p.n = uint32_t(n64);
+    const uint32_t nmax = p.nmax = std::max(n, 1u);
 
     // tuning (64-bit keys use 8-bit digits and 2048-key tiles)
-    uint32_t rb = key64 ? 8u : g_radix_bits.load();
-    uint32_t tile_keys = key64 ? 2048u : g_tile_keys.load();
-    if (rb == 0) auto_tuning(lb + 1, &rb, &tile_keys);
-    const uint32_t it = tile_keys / kBlock;
-    const uint32_t lf = g_load_pct.load();
+    uint32_t rb, tile_keys, lf;
+    if (fixed) {
+        rb = fixed->rb;
+        tile_keys = fixed->tile_keys;
+        lf = fixed->lf;
+    } else {
+        rb = p.key64 ? 8u : g_radix_bits.load();
+        tile_keys = p.key64 ? 2048u : g_tile_keys.load();
+        if (rb == 0) auto_tuning(lb + 1, &rb, &tile_keys);
+        lf = g_load_pct.load();
+    }
+    p.rb = rb;
+    p.it = tile_keys / kBlock;
+    p.lf = lf;
 
-    BuildDesc d;
+    BuildDesc& d = p.d;
     std::memset(&d, 0, sizeof(d));
     d.mode = job.mode;
     d.log2 = log2;
@@ -430,32 +482,19 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     d.n_new = job.n_new;
     d.n_total = n;
     d.top = log2 - 1;
-    d.old_keys = reinterpret_cast<const uint64_t*>(job.old_keys);
-    d.old_vals = reinterpret_cast<const uint32_t*>(job.old_vals);
-    d.voxels = reinterpret_cast<const uint4*>(job.voxels);
-    d.offsets = reinterpret_cast<const uint32_t*>(job.offsets);
-    d.gen_counts = reinterpret_cast<const uint32_t*>(job.gen_counts);
-    d.edits = reinterpret_cast<const uint4*>(job.edits);
-    d.edit_offsets = reinterpret_cast<const uint32_t*>(job.edit_offsets);
-    d.src_keys = reinterpret_cast<const uint64_t*>(job.src_keys);
-    d.src_vals = reinterpret_cast<const uint32_t*>(job.src_vals);
-    d.chunk_log2 = reinterpret_cast<const uint32_t*>(job.chunk_log2);
-    d.voxel_offsets = reinterpret_cast<const uint32_t*>(job.voxel_offsets);
-    d.edit_offsets2 = reinterpret_cast<const uint32_t*>(job.edit_offsets2);
-    d.voxel_starts = reinterpret_cast<const uint64_t*>(job.voxel_starts);
-    d.chunked = chunked ? 1u : 0u;
+    d.chunked = p.chunked ? 1u : 0u;
 
     // digit plan over lb + 1 bits (the invalid bit on top)
     const uint32_t sort_bits = lb + 1;
-    const uint32_t passes = (sort_bits + rb - 1) / rb;
+    const uint32_t passes = p.passes = (sort_bits + rb - 1) / rb;
     d.passes = passes;
     d.radix = 1u << rb;
     {
         uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 0;
-        for (uint32_t p = 0; p < passes; ++p) {
-            uint32_t b = base + (p < extra ? 1 : 0);
-            d.pass_shift[p] = sh;
-            d.pass_bits[p] = b;
+        for (uint32_t q = 0; q < passes; ++q) {
+            uint32_t b = base + (q < extra ? 1 : 0);
+            d.pass_shift[q] = sh;
+            d.pass_bits[q] = b;
             sh += b;
         }
     }
@@ -474,8 +513,8 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
         }
         return total;
     };
-    const uint32_t B = uint32_t(std::max<uint64_t>(std::min<uint64_t>(nmax, cells(2)), 1));
-    uint32_t P[kMaxLevels + 2] = {};
+    const uint32_t B = p.B = uint32_t(std::max<uint64_t>(std::min<uint64_t>(nmax, cells(2)), 1));
+    uint32_t* P = p.P;
     uint64_t words = 2;
     for (uint32_t lv = 2; lv < log2; ++lv) {
         uint64_t prev = lv == 2 ? B : P[lv - 1];
@@ -501,136 +540,143 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
 
     // ---- scratch layout
     Layout zl;  // zero-initialised region
-    const uint64_t o_counters = zl.take(kCtrCount * 4);
-    const uint64_t o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
-    const uint64_t o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
-    const uint64_t o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
-    const uint64_t o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
-    const uint64_t o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
+    p.o_counters = zl.take(kCtrCount * 4);
+    p.o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
+    p.o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
+    p.o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
+    p.o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
+    p.o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
     // a table filled region by region is cleared by its insert kernel, not by the memset
-    uint64_t o_leaf_table = d.leaf_regions > 1 ? 0 : zl.take(uint64_t(d.leaf_cap) * 16);
-    const uint64_t o_regions = zl.take(3 * kMaxLeafRegions * 4);
-    uint64_t o_table[kMaxLevels + 2], o_bstat[kMaxLevels + 2], o_ostat[kMaxLevels + 2];
-    uint32_t cap[kMaxLevels + 2], btiles[kMaxLevels + 2], otiles[kMaxLevels + 2];
+    p.o_leaf_table = d.leaf_regions > 1 ? 0 : zl.take(uint64_t(d.leaf_cap) * 16);
+    p.o_regions = zl.take(3 * kMaxLeafRegions * 4);
     for (uint32_t lv = 2; lv < log2; ++lv) {
-        cap[lv] = next_pow2((uint64_t(P[lv]) * 100 + lf - 1) / lf, 1024);
+        p.cap[lv] = next_pow2((uint64_t(P[lv]) * 100 + lf - 1) / lf, 1024);
         uint32_t child = lv == 2 ? B : P[lv - 1];
-        btiles[lv] = std::max((child + kNodeBuildTile - 1) / kNodeBuildTile, 1u);
-        otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
-        o_table[lv] = zl.take(uint64_t(cap[lv]) * 16);
-        o_bstat[lv] = zl.take(uint64_t(btiles[lv]) * 8);
-        o_ostat[lv] = zl.take(uint64_t(otiles[lv]) * 8);
+        p.btiles[lv] = std::max((child + kNodeBuildTile - 1) / kNodeBuildTile, 1u);
+        p.otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
+        p.o_table[lv] = zl.take(uint64_t(p.cap[lv]) * 16);
+        p.o_bstat[lv] = zl.take(uint64_t(p.btiles[lv]) * 8);
+        p.o_ostat[lv] = zl.take(uint64_t(p.otiles[lv]) * 8);
     }
-    const uint64_t zero_bytes = align_up(zl.size, 256);
-    Layout fl = zl;  // 0xFF region follows
-    fl.size = zero_bytes;
-    const uint64_t o_chunk_first = fl.take(uint64_t(K) * 4);
-    const uint64_t o_roots = fl.take(uint64_t(K) * 4);
-    const uint64_t o_prim_start = fl.take(uint64_t(K) * 4);
-    const uint64_t ff_bytes = align_up(fl.size, 256) - zero_bytes;
-    Layout ol = fl;
-    ol.size = zero_bytes + ff_bytes;
-    if (d.leaf_regions > 1) o_leaf_table = ol.take(uint64_t(d.leaf_cap) * 16);
-    const uint64_t o_seg_entry = ol.take(uint64_t(K + 1) * 4);
-    const uint64_t o_seg_tile = ol.take(uint64_t(K + 1) * 4);
-    const uint64_t kbytes = key64 ? 8 : 4;
-    const uint64_t o_k0 = ol.take(uint64_t(nmax) * kbytes), o_v0 = ol.take(uint64_t(nmax) * 4);
-    const uint64_t o_k1 = ol.take(uint64_t(nmax) * kbytes), o_v1 = ol.take(uint64_t(nmax) * 4);
-    const uint64_t o_bkey = ol.take(uint64_t(B) * 8), o_bmask = ol.take(uint64_t(B) * 8);
-    const uint64_t o_bfirst = ol.take(uint64_t(B) * 4), o_bslot = ol.take(uint64_t(B) * 4);
-    const uint64_t o_bref = ol.take(uint64_t(B) * 4);
+    p.zero_bytes = align_up(zl.size, 256);
+    Layout fl;  // 0xFF region follows
+    fl.size = p.zero_bytes;
+    p.o_chunk_first = fl.take(uint64_t(K) * 4);
+    p.o_roots = fl.take(uint64_t(K) * 4);
+    p.o_prim_start = fl.take(uint64_t(K) * 4);
+    p.ff_bytes = align_up(fl.size, 256) - p.zero_bytes;
+    Layout ol;
+    ol.size = p.zero_bytes + p.ff_bytes;
+    if (d.leaf_regions > 1) p.o_leaf_table = ol.take(uint64_t(d.leaf_cap) * 16);
+    p.o_seg_entry = ol.take(uint64_t(K + 1) * 4);
+    p.o_seg_tile = ol.take(uint64_t(K + 1) * 4);
+    const uint64_t kbytes = p.key64 ? 8 : 4;
+    p.o_k0 = ol.take(uint64_t(nmax) * kbytes);
+    p.o_v0 = ol.take(uint64_t(nmax) * 4);
+    p.o_k1 = ol.take(uint64_t(nmax) * kbytes);
+    p.o_v1 = ol.take(uint64_t(nmax) * 4);
+    p.o_bkey = ol.take(uint64_t(B) * 8);
+    p.o_bmask = ol.take(uint64_t(B) * 8);
+    p.o_bfirst = ol.take(uint64_t(B) * 4);
+    p.o_bslot = ol.take(uint64_t(B) * 4);
+    p.o_bref = ol.take(uint64_t(B) * 4);
     // parent record sets: A for even offsets from level 2, B for odd
-    uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
-    uint64_t o_set[2][7];
+    const uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
     for (int s = 0; s < 2; ++s) {
-        uint64_t m = std::max(setn[s], 1u);
-        o_set[s][0] = ol.take(m * 8);                 // key
-        o_set[s][1] = ol.take(m * 4);                 // cnt
-        o_set[s][2] = ol.take(m * 4);                 // first
-        o_set[s][3] = ol.take(m * 4);                 // slot
-        o_set[s][4] = ol.take(m * 8);                 // lo
-        o_set[s][5] = ol.take(m * 8);                 // hi
-        o_set[s][6] = ol.take(m * kNodeStride * 4);   // words
+        const uint64_t m = std::max(setn[s], 1u);
+        p.o_set[s][0] = ol.take(m * 8);                 // key
+        p.o_set[s][1] = ol.take(m * 4);                 // cnt
+        p.o_set[s][2] = ol.take(m * 4);                 // first
+        p.o_set[s][3] = ol.take(m * 4);                 // slot
+        p.o_set[s][4] = ol.take(m * 8);                 // lo
+        p.o_set[s][5] = ol.take(m * 8);                 // hi
+        p.o_set[s][6] = ol.take(m * kNodeStride * 4);   // words
     }
-    const uint64_t scratch_bytes = align_up(ol.size, 256);
+    p.scratch_bytes = align_up(ol.size, 256);
+    const uint64_t prims = std::max(d.prim_bound, 1u);
+    const uint64_t outs[6] = {uint64_t(d.node_bound) * 4, uint64_t(B) * 8, uint64_t(nmax) * 8, uint64_t(nmax) * 4,
+                              prims * 16, prims * 24};
+    for (int i = 0; i < 6; ++i) p.out_size[i] = outs[i];
+    return PYRB_OK;
+}
 
-    // ---- allocations
-    uint64_t scratch = mem.get(scratch_bytes);
-    if (!scratch) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the build scratch (%llu bytes)", (unsigned long long)scratch_bytes);
-    uint64_t o_nodes = mem.get(uint64_t(d.node_bound) * 4);
-    uint64_t o_leaves = mem.get(uint64_t(B) * 8);
-    uint64_t o_ukey = mem.get(uint64_t(nmax) * 8);
-    uint64_t o_uval = mem.get(uint64_t(nmax) * 4);
-    uint64_t o_prims = mem.get(uint64_t(std::max(d.prim_bound, 1u)) * 16);
-    uint64_t o_aabbs = mem.get(uint64_t(std::max(d.prim_bound, 1u)) * 24);
-    auto release_outputs = [&] {
-        for (uint64_t p : {o_nodes, o_leaves, o_ukey, o_uval, o_prims, o_aabbs}) mem.put(p);
-    };
-    if (!o_nodes || !o_leaves || !o_ukey || !o_uval || !o_prims || !o_aabbs) {
-        release_outputs();
-        mem.put(scratch);
-        return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the build outputs");
-    }
+// Device pointers of a plan: scratch block at `scratch`, outputs given; fills the
+// level descriptors.
+void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job, std::vector<LevelDesc>& levels) {
+    BuildDesc& d = p.d;
     auto at = [&](uint64_t off) { return reinterpret_cast<void*>(scratch + off); };
-    d.counters = static_cast<uint32_t*>(at(o_counters));
-    d.hist = static_cast<uint32_t*>(at(o_hist));
-    d.sort_status = static_cast<uint64_t*>(at(o_sort_status));
-    d.uniq_status = static_cast<uint64_t*>(at(o_uniq_status));
-    d.brick_status = static_cast<uint64_t*>(at(o_brick_status));
-    d.leafown_status = static_cast<uint64_t*>(at(o_leafown_status));
-    d.leaf_table = static_cast<uint4*>(at(o_leaf_table));
-    d.region_count = static_cast<uint32_t*>(at(o_regions));
+    d.old_keys = reinterpret_cast<const uint64_t*>(job.old_keys);
+    d.old_vals = reinterpret_cast<const uint32_t*>(job.old_vals);
+    d.voxels = reinterpret_cast<const uint4*>(job.voxels);
+    d.offsets = reinterpret_cast<const uint32_t*>(job.offsets);
+    d.gen_counts = reinterpret_cast<const uint32_t*>(job.gen_counts);
+    d.edits = reinterpret_cast<const uint4*>(job.edits);
+    d.edit_offsets = reinterpret_cast<const uint32_t*>(job.edit_offsets);
+    d.src_keys = reinterpret_cast<const uint64_t*>(job.src_keys);
+    d.src_vals = reinterpret_cast<const uint32_t*>(job.src_vals);
+    d.chunk_log2 = reinterpret_cast<const uint32_t*>(job.chunk_log2);
+    d.voxel_offsets = reinterpret_cast<const uint32_t*>(job.voxel_offsets);
+    d.edit_offsets2 = reinterpret_cast<const uint32_t*>(job.edit_offsets2);
+    d.voxel_starts = reinterpret_cast<const uint64_t*>(job.voxel_starts);
+    d.counters = static_cast<uint32_t*>(at(p.o_counters));
+    d.hist = static_cast<uint32_t*>(at(p.o_hist));
+    d.sort_status = static_cast<uint64_t*>(at(p.o_sort_status));
+    d.uniq_status = static_cast<uint64_t*>(at(p.o_uniq_status));
+    d.brick_status = static_cast<uint64_t*>(at(p.o_brick_status));
+    d.leafown_status = static_cast<uint64_t*>(at(p.o_leafown_status));
+    d.leaf_table = static_cast<uint4*>(at(p.o_leaf_table));
+    d.region_count = static_cast<uint32_t*>(at(p.o_regions));
     d.region_cursor = d.region_count + kMaxLeafRegions;
     d.region_zeroed = d.region_count + 2 * kMaxLeafRegions;
     // the sort buffers are dead once the unique voxels are out: N x (kb + 4) bytes from
     // k0 hold the B region-grouped masks, k1 their brick indices
-    d.pmask = static_cast<uint64_t*>(at(o_k0));
-    d.pidx = static_cast<uint32_t*>(at(o_k1));
-    d.chunk_first = static_cast<uint32_t*>(at(o_chunk_first));
-    d.roots = static_cast<uint32_t*>(at(o_roots));
-    d.prim_start = static_cast<uint32_t*>(at(o_prim_start));
-    d.seg_entry = static_cast<uint32_t*>(at(o_seg_entry));
-    d.seg_tile = static_cast<uint32_t*>(at(o_seg_tile));
-    d.kbuf[0] = at(o_k0);
-    d.vbuf[0] = static_cast<uint32_t*>(at(o_v0));
-    d.kbuf[1] = at(o_k1);
-    d.vbuf[1] = static_cast<uint32_t*>(at(o_v1));
-    d.bkey = static_cast<uint64_t*>(at(o_bkey));
-    d.bmask = static_cast<uint64_t*>(at(o_bmask));
-    d.bfirst = static_cast<uint32_t*>(at(o_bfirst));
-    d.bslot = static_cast<uint32_t*>(at(o_bslot));
-    d.bref = static_cast<uint32_t*>(at(o_bref));
-    d.ukey = reinterpret_cast<uint64_t*>(o_ukey);
-    d.uval = reinterpret_cast<uint32_t*>(o_uval);
-    d.leaves = reinterpret_cast<uint64_t*>(o_leaves);
-    d.nodes = reinterpret_cast<uint32_t*>(o_nodes);
-    d.prims = reinterpret_cast<uint8_t*>(o_prims);
-    d.aabbs = reinterpret_cast<float*>(o_aabbs);
+    d.pmask = static_cast<uint64_t*>(at(p.o_k0));
+    d.pidx = static_cast<uint32_t*>(at(p.o_k1));
+    d.chunk_first = static_cast<uint32_t*>(at(p.o_chunk_first));
+    d.roots = static_cast<uint32_t*>(at(p.o_roots));
+    d.prim_start = static_cast<uint32_t*>(at(p.o_prim_start));
+    d.seg_entry = static_cast<uint32_t*>(at(p.o_seg_entry));
+    d.seg_tile = static_cast<uint32_t*>(at(p.o_seg_tile));
+    d.kbuf[0] = at(p.o_k0);
+    d.vbuf[0] = static_cast<uint32_t*>(at(p.o_v0));
+    d.kbuf[1] = at(p.o_k1);
+    d.vbuf[1] = static_cast<uint32_t*>(at(p.o_v1));
+    d.bkey = static_cast<uint64_t*>(at(p.o_bkey));
+    d.bmask = static_cast<uint64_t*>(at(p.o_bmask));
+    d.bfirst = static_cast<uint32_t*>(at(p.o_bfirst));
+    d.bslot = static_cast<uint32_t*>(at(p.o_bslot));
+    d.bref = static_cast<uint32_t*>(at(p.o_bref));
+    d.nodes = reinterpret_cast<uint32_t*>(outs[0]);
+    d.leaves = reinterpret_cast<uint64_t*>(outs[1]);
+    d.ukey = reinterpret_cast<uint64_t*>(outs[2]);
+    d.uval = reinterpret_cast<uint32_t*>(outs[3]);
+    d.prims = reinterpret_cast<uint8_t*>(outs[4]);
+    d.aabbs = reinterpret_cast<float*>(outs[5]);
 
-    std::vector<LevelDesc> levels;
-    for (uint32_t lv = 2; lv < log2; ++lv) {
+    levels.clear();
+    for (uint32_t lv = 2; lv < d.log2; ++lv) {
         LevelDesc L;
         std::memset(&L, 0, sizeof(L));
         L.lv = lv;
-        L.child_bound = lv == 2 ? B : P[lv - 1];
-        L.parent_bound = P[lv];
-        L.build_tiles = btiles[lv];
-        L.own_tiles = otiles[lv];
-        L.need_box = lv + 1 <= rt ? 1u : 0u;
-        L.pcap = cap[lv];
+        L.child_bound = lv == 2 ? p.B : p.P[lv - 1];
+        L.parent_bound = p.P[lv];
+        L.build_tiles = p.btiles[lv];
+        L.own_tiles = p.otiles[lv];
+        L.need_box = lv + 1 <= d.rt_log2 ? 1u : 0u;
+        L.pcap = p.cap[lv];
         L.tile_ctr_build = 12 + 2 * (lv - 2);
         L.tile_ctr_own = 13 + 2 * (lv - 2);
         const int ps = (lv - 2) & 1;
-        L.pkey = static_cast<uint64_t*>(at(o_set[ps][0]));
-        L.pcnt = static_cast<uint32_t*>(at(o_set[ps][1]));
-        L.pfirst = static_cast<uint32_t*>(at(o_set[ps][2]));
-        L.pslot = static_cast<uint32_t*>(at(o_set[ps][3]));
-        L.plo = static_cast<uint64_t*>(at(o_set[ps][4]));
-        L.phi = static_cast<uint64_t*>(at(o_set[ps][5]));
-        L.pwords = static_cast<uint32_t*>(at(o_set[ps][6]));
-        L.ptable = static_cast<uint4*>(at(o_table[lv]));
-        L.build_status = static_cast<uint64_t*>(at(o_bstat[lv]));
-        L.own_status = static_cast<uint64_t*>(at(o_ostat[lv]));
+        L.pkey = static_cast<uint64_t*>(at(p.o_set[ps][0]));
+        L.pcnt = static_cast<uint32_t*>(at(p.o_set[ps][1]));
+        L.pfirst = static_cast<uint32_t*>(at(p.o_set[ps][2]));
+        L.pslot = static_cast<uint32_t*>(at(p.o_set[ps][3]));
+        L.plo = static_cast<uint64_t*>(at(p.o_set[ps][4]));
+        L.phi = static_cast<uint64_t*>(at(p.o_set[ps][5]));
+        L.pwords = static_cast<uint32_t*>(at(p.o_set[ps][6]));
+        L.ptable = static_cast<uint4*>(at(p.o_table[lv]));
+        L.build_status = static_cast<uint64_t*>(at(p.o_bstat[lv]));
+        L.own_status = static_cast<uint64_t*>(at(p.o_ostat[lv]));
         if (lv == 2) {
             L.ckey = d.bkey;
             L.cmask = d.bmask;
@@ -649,31 +695,26 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
         }
         levels.push_back(L);
     }
+}
 
-    // ---- launches
-    auto cleanup = [&] {
-        release_outputs();
-        mem.put(scratch);
-    };
-#define CUL(call)                                                                                 \
-    do {                                                                                          \
-        cudaError_t err_ = (call);                                                                \
-        if (err_ != cudaSuccess) {                                                                \
-            cleanup();                                                                            \
-            return fail(PYRB_ERROR_CUDA, "%s: %s", #call, cudaGetErrorString(err_));              \
-        }                                                                                         \
-    } while (0)
+// The launches of a bound plan on `st` (the scratch is cleared here). Returns the
+// number of kernels launched, or 0 with the CUDA error in *err.
+uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaStream_t st, cudaError_t* err) {
+    const BuildDesc& d = p.d;
     Prof prof(st);
-    CUL(cudaMemsetAsync(at(0), 0, zero_bytes, st));
-    CUL(cudaMemsetAsync(at(zero_bytes), 0xFF, ff_bytes, st));
+    uint8_t* base = reinterpret_cast<uint8_t*>(d.counters) - p.o_counters;
+    *err = cudaMemsetAsync(base, 0, p.zero_bytes, st);
+    if (*err == cudaSuccess) *err = cudaMemsetAsync(base + p.zero_bytes, 0xFF, p.ff_bytes, st);
+    if (*err != cudaSuccess) return 0;
     prof.mark("memset");
     uint32_t launches = 0;
     launch(k_plan, 1, 1024, 0, st, d);
     ++launches;
     prof.mark("plan");
-    CUL(cudaGetLastError());
-    CUL(launch_sort_any(rb, it, d, st, prof));
-    launches += 3 + passes;
+    if ((*err = cudaGetLastError()) != cudaSuccess) return 0;
+    if ((*err = launch_sort_any(p.rb, p.it, d, st, prof)) != cudaSuccess) return 0;
+    launches += 3 + p.passes;
+    const uint32_t B = p.B;
     if (d.leaf_regions > 1) {
         launch(k_leaf_part, std::max(std::min((B + kBrickTile - 1) / kBrickTile, 148u * 8u), 1u), kBlock, 0, st, d);
         prof.mark("leaf_part");
@@ -687,44 +728,93 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
     launch(k_leaf_own, d.leafown_tiles, kBlock, 0, st, d);
     prof.mark("leaf_own");
     launches += 2;
-    const uint32_t lv0 = tail_level(log2, B, P);
-    launches += launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
-    if (job.mode == kModeBatch && min_log2 < log2) {
-        launch(k_batch_roots, std::max(std::min((K + 255) / 256, 1024u), 1u), 256, 0, st, d, log2);
+    const uint32_t lv0 = tail_level(d.log2, B, p.P);
+    launches += launch_levels(d, levels, lv0, make_tail(lv0, p.P, levels, d.leaf_table), st, prof);
+    if (d.mode == kModeBatch && p.min_log2 < d.log2) {
+        launch(k_batch_roots, std::max(std::min((p.K + 255) / 256, 1024u), 1u), 256, 0, st, d, d.log2);
         prof.mark("batch_roots");
         ++launches;
     }
-    CUL(cudaGetLastError());
+    if ((*err = cudaGetLastError()) != cudaSuccess) return 0;
+    return launches;
+}
 
-    const uint64_t out_bytes = uint64_t(d.node_bound) * 4 + uint64_t(B) * 8 + uint64_t(nmax) * 12 +
-                               uint64_t(std::max(d.prim_bound, 1u)) * 40;
+pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint32_t* host_counts = nullptr) {
+    if (!out) return fail(PYRB_ERROR_INVALID_ARGUMENT, "out is NULL");
+    std::memset(out, 0, sizeof(*out));
+    Plan p;
+    pyrb_result r = plan_build(job, nullptr, p);
+    if (r != PYRB_OK) return r;
+    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+    Mem mem{e, st};
+
+    // ---- allocations
+    uint64_t scratch = mem.get(p.scratch_bytes);
+    if (!scratch) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the build scratch (%llu bytes)", (unsigned long long)p.scratch_bytes);
+    uint64_t outs[6] = {};
+    bool ok = true;
+    for (int i = 0; i < 6; ++i) ok = (outs[i] = mem.get(p.out_size[i])) != 0 && ok;
+    auto release_outputs = [&] {
+        for (uint64_t q : outs) mem.put(q);
+    };
+    auto cleanup = [&] {
+        release_outputs();
+        mem.put(scratch);
+    };
+    if (!ok) {
+        cleanup();
+        return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the build outputs");
+    }
+    std::vector<LevelDesc> levels;
+    bind_plan(p, scratch, outs, job, levels);
+    const BuildDesc& d = p.d;
+    const uint32_t K = p.K;
+
+#define CUL(call)                                                                                 \
+    do {                                                                                          \
+        cudaError_t err_ = (call);                                                                \
+        if (err_ != cudaSuccess) {                                                                \
+            cleanup();                                                                            \
+            return fail(PYRB_ERROR_CUDA, "%s: %s", #call, cudaGetErrorString(err_));              \
+        }                                                                                         \
+    } while (0)
+    cudaError_t lerr = cudaSuccess;
+    const uint32_t launches = launch_plan(p, levels, st, &lerr);
+    CUL(lerr);
+
+    const uint64_t scratch_bytes = p.scratch_bytes, out_bytes = p.out_bytes();
+    auto fill_out = [&] {
+        out->log2_size = d.log2;
+        out->rt_log2 = d.rt_log2;
+        out->nodes = outs[0];
+        out->leaves = outs[1];
+        out->keys = outs[2];
+        out->attrs = outs[3];
+        out->prims = outs[4];
+        out->aabbs = outs[5];
+    };
+    auto fill_meta = [&](uint32_t* meta) {
+        meta[0] = d.log2; meta[1] = d.rt_log2; meta[2] = p.passes; meta[3] = p.rb; meta[4] = launches;
+        std::memcpy(meta + 5, &scratch_bytes, 8);
+        std::memcpy(meta + 7, &out_bytes, 8);
+    };
     // ---- asynchronous form: counts land in pinned host memory, no synchronisation
     if (host_counts) {
         CUL(cudaMemcpyAsync(host_counts, d.counters, kCtrCount * 4, cudaMemcpyDeviceToHost, st));
-        if (chunked) {
+        if (p.chunked) {
             if (job.roots) CUL(cudaMemcpyAsync(job.roots, d.roots, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
             if (job.first_voxel) CUL(cudaMemcpyAsync(job.first_voxel, d.chunk_first, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
             if (job.first_prim) CUL(cudaMemcpyAsync(job.first_prim, d.prim_start, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
         }
         mem.put(scratch);
-        uint32_t* meta = host_counts + kCtrCount;
-        meta[0] = log2; meta[1] = rt; meta[2] = passes; meta[3] = rb; meta[4] = launches;
-        std::memcpy(meta + 5, &scratch_bytes, 8);
-        std::memcpy(meta + 7, &out_bytes, 8);
-        out->log2_size = log2;
-        out->rt_log2 = rt;
-        out->nodes = o_nodes;
-        out->leaves = o_leaves;
-        out->keys = o_ukey;
-        out->attrs = o_uval;
-        out->prims = o_prims;
-        out->aabbs = o_aabbs;
+        fill_meta(host_counts + kCtrCount);
+        fill_out();
         return PYRB_OK;
     }
     // ---- read back
     uint32_t ctr[kCtrCount];
     CUL(cudaMemcpyAsync(ctr, d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
-    if (chunked) {
+    if (p.chunked) {
         if (job.roots) CUL(cudaMemcpyAsync(job.roots, d.roots, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
         if (job.first_voxel) CUL(cudaMemcpyAsync(job.first_voxel, d.chunk_first, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
         if (job.first_prim) CUL(cudaMemcpyAsync(job.first_prim, d.prim_start, uint64_t(K) * 4, cudaMemcpyDeviceToHost, st));
@@ -735,20 +825,12 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
 #undef CUL
     if (ctr[kCtrError]) {
         release_outputs();
-        return device_error(ctr[kCtrError]);
+        return device_error(ctr);
     }
-    out->log2_size = log2;
-    out->rt_log2 = rt;
-    out->nodes = o_nodes;
-    out->leaves = o_leaves;
-    out->keys = o_ukey;
-    out->attrs = o_uval;
-    out->prims = o_prims;
-    out->aabbs = o_aabbs;
+    fill_out();
     fill_counts(ctr, out);
-    uint32_t meta[16] = {log2, rt, passes, rb, launches};
-    std::memcpy(meta + 5, &scratch_bytes, 8);
-    std::memcpy(meta + 7, &out_bytes, 8);
+    uint32_t meta[16] = {};
+    fill_meta(meta);
     fill_stats(ctr, meta);
     return PYRB_OK;
 }
@@ -932,7 +1014,7 @@ PYRB_API pyrb_result pyrb_build_async(const pyrb_exec* e, uint32_t log2_size, ui
 
 PYRB_API pyrb_result pyrb_build_finish(const uint32_t* host_counts, pyrb_built* out) {
     if (!host_counts || !out) return fail(PYRB_ERROR_INVALID_ARGUMENT, "NULL argument");
-    if (host_counts[kCtrError]) return device_error(host_counts[kCtrError]);
+    if (host_counts[kCtrError]) return device_error(host_counts);
     fill_counts(host_counts, out);
     fill_stats(host_counts, host_counts + kCtrCount);
     return PYRB_OK;
@@ -968,6 +1050,7 @@ PYRB_API const char* pyrb_result_string(pyrb_result r) {
         case PYRB_OK: return "ok";
         case PYRB_ERROR_INVALID_ARGUMENT: return "invalid argument";
         case PYRB_ERROR_OUT_OF_MEMORY: return "out of memory";
+        case PYRB_ERROR_CAPACITY: return "capacity exceeded";
         case PYRB_ERROR_CUDA: return "CUDA error";
         default: return "unknown result";
     }
@@ -1272,19 +1355,73 @@ PYRB_API pyrb_result pyrb_path_edit(const pyrb_exec* e, uint64_t nodes, uint64_t
     return done(PYRB_OK);
 }
 
-PYRB_API uint32_t pyrb_version(void) { return (0u << 16) | 1u; }
+PYRB_API pyrb_result pyrb_build_memory(uint32_t log2_size, uint32_t count, const uint32_t* chunk_log2,
+                                       uint64_t entries, uint64_t* scratch_bytes, uint64_t* output_bytes) {
+    if (count == 0) return fail(PYRB_ERROR_INVALID_ARGUMENT, "count is 0");
+    if (entries >= (uint64_t(1) << 31))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many entries for one build (%llu)", (unsigned long long)entries);
+    Job j;
+    j.K = count;
+    if (chunk_log2) {
+        uint32_t lmax = 0;
+        for (uint32_t c = 0; c < count; ++c) lmax = std::max(lmax, chunk_log2[c]);
+        j.mode = kModeBatch;
+        j.log2 = lmax;
+        j.chunk_log2_host = chunk_log2;
+        j.voxel_total = uint32_t(entries);
+    } else if (count > 1) {
+        j.mode = kModeChunks;
+        j.log2 = log2_size;
+        j.total = uint32_t(entries);
+    } else {
+        j.mode = kModePlain;
+        j.log2 = log2_size;
+        j.n_new = uint32_t(entries);
+    }
+    Plan p;
+    pyrb_result r = plan_build(j, nullptr, p);
+    if (r != PYRB_OK) return r;
+    if (scratch_bytes) *scratch_bytes = p.scratch_bytes;
+    if (output_bytes) *output_bytes = p.out_bytes();
+    return PYRB_OK;
+}
+
+PYRB_API uint32_t pyrb_last_capacity_need(void) { return g_capacity_need; }
+
+PYRB_API pyrb_result pyrb_selftest_wait_limit(const pyrb_exec* e, uint32_t which) {
+    if (which > 1) return fail(PYRB_ERROR_INVALID_ARGUMENT, "which must be 0 or 1");
+    cudaStream_t st = e ? reinterpret_cast<cudaStream_t>(e->stream) : nullptr;
+    Mem mem{e, st};
+    const uint64_t block = mem.get(1024);
+    if (!block) return fail(PYRB_ERROR_OUT_OF_MEMORY, "device memory for the wait self-test");
+    uint64_t* status = reinterpret_cast<uint64_t*>(block);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(block + 64);
+    uint32_t ctr[kCtrCount] = {};
+    cudaError_t err = cudaMemsetAsync(reinterpret_cast<void*>(block), 0, 1024, st);
+    if (err == cudaSuccess) {
+        k_selftest_wait<<<1, 32, 0, st>>>(status, counters, which);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpyAsync(ctr, counters, sizeof(ctr), cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    mem.put(block);
+    if (err != cudaSuccess) return fail(PYRB_ERROR_CUDA, "wait self-test: %s", cudaGetErrorString(err));
+    return ctr[kCtrError] ? device_error(ctr) : PYRB_OK;
+}
+
+PYRB_API uint32_t pyrb_version(void) { return (0u << 16) | 2u; }
 
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
 // Build without any device allocation (pyrb_build_noalloc).
 //
-// Some callers cannot allocate device memory while they build: a frame loop that
-// must not call cudaMalloc (it synchronises the device), code that runs while a
-// stream is being captured into a CUDA graph (allocation calls are illegal there),
-// or hosts whose memory is fully budgeted up front. For them all scratch of the
-// build lives in this fixed, file-scope device array; the caller brings input and
-// output buffers. Every GPU that loads the library keeps the array until exit.
+// Some callers cannot allocate device memory while they build: a render or frame
+// loop must not call cudaMalloc (it synchronises the whole device and stalls the
+// frame), and an engine whose device memory is budgeted up front has no allocator
+// to offer for scratch. For them all scratch of the build lives in this fixed,
+// file-scope device array; the caller brings input and output buffers. Every GPU
+// that loads the library keeps the array until the process exits.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1297,8 +1434,11 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 std::mutex g_static_mu;
 void* g_static_addr[64] = {};
 
-// Device address of the array on the current device. The first call per device
-// resolves it with cudaGetSymbolAddress (the array's name is only a host stand-in).
+// Device address of the array on the current device. The name g_static_scratch is
+// only a host-side stand-in in host code; the first call per device (with that
+// device current) resolves the real address with cudaGetSymbolAddress, and later
+// calls reuse it. The address belongs to the device's primary context: after a
+// cudaDeviceReset the library must be loaded again.
 pyrb_result static_scratch(void** out) {
     int dev = 0;
     CU(cudaGetDevice(&dev));
@@ -1336,200 +1476,45 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     if (!nodes || !leaves || !keys || !attrs || !prims || !aabbs)
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "pyrb_build_noalloc: every output buffer is required");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const uint32_t log2 = log2_size, lb = 3 * log2, K = 1;
-    const uint32_t rt = std::min(std::max(rt_log2_req, 3u), log2);
-    const uint32_t n = n_new, nmax = std::max(n, 1u);
-    const uint32_t rb = 8, tile_keys = 4096, lf = 50;
-
-    BuildDesc d;
-    std::memset(&d, 0, sizeof(d));
-    d.mode = kModePlain;
-    d.log2 = log2;
-    d.rt_log2 = rt;
-    d.lb = lb;
-    d.seg_count = K;
-    d.n_new = n;
-    d.n_total = n;
-    d.top = log2 - 1;
-    d.voxels = reinterpret_cast<const uint4*>(edits);
-    const uint32_t sort_bits = lb + 1, passes = (sort_bits + rb - 1) / rb;
-    d.passes = passes;
-    d.radix = 1u << rb;
-    {
-        uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 0;
-        for (uint32_t p = 0; p < passes; ++p) {
-            d.pass_shift[p] = sh;
-            d.pass_bits[p] = base + (p < extra ? 1 : 0);
-            sh += d.pass_bits[p];
-        }
-    }
-    d.tile_keys = tile_keys;
-    d.sort_tiles = std::max((n + tile_keys - 1) / tile_keys, 1u);
-    auto cells = [&](uint32_t edge_log2) -> uint64_t { return uint64_t(1) << (3 * (log2 - edge_log2)); };
-    const uint32_t B = uint32_t(std::max<uint64_t>(std::min<uint64_t>(nmax, cells(2)), 1));
-    uint32_t P[kMaxLevels + 2] = {};
-    uint64_t words = 2;
-    for (uint32_t lv = 2; lv < log2; ++lv) {
-        uint64_t prev = lv == 2 ? B : P[lv - 1];
-        P[lv] = uint32_t(std::max<uint64_t>(std::min<uint64_t>(prev, cells(lv + 1)), 1));
-        words += uint64_t(P[lv]) * kNodeStride;
-    }
-    d.brick_bound = B;
-    d.brick_tiles = d.sort_tiles * std::max(1u, tile_keys / 4096u);  // the unique tiles
-    d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
-    d.leaf_cap = next_pow2((uint64_t(B) * 100 + lf - 1) / lf, 1024);
-    d.node_bound = uint32_t(words);
-    d.prim_bound = P[rt - 1];
-    if (node_capacity < d.node_bound || leaf_capacity < B || voxel_capacity < nmax || prim_capacity < std::max(d.prim_bound, 1u))
+    Job j;
+    j.mode = kModePlain;
+    j.log2 = log2_size;
+    j.rt_req = rt_log2_req;
+    j.voxels = edits;
+    j.n_new = n_new;
+    // one fixed tuning: the scratch bound below holds for it at every allowed size
+    const Tune fixed{8, 4096, 50};
+    Plan p;
+    pyrb_result r = plan_build(j, &fixed, p);
+    if (r != PYRB_OK) return r;
+    const uint32_t prim_need = std::max(p.d.prim_bound, 1u);
+    if (node_capacity < p.d.node_bound || leaf_capacity < p.B || voxel_capacity < p.nmax || prim_capacity < prim_need)
         return fail(PYRB_ERROR_INVALID_ARGUMENT,
                     "pyrb_build_noalloc: output buffers too small (need nodes %u words, leaves %u, keys/attrs %u, "
-                    "prims %u)", d.node_bound, B, nmax, std::max(d.prim_bound, 1u));
-
-    // scratch layout inside the fixed array: zero region, 0xFF region, the rest
-    Layout zl;
-    const uint64_t o_counters = zl.take(kCtrCount * 4);
-    const uint64_t o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
-    const uint64_t o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
-    const uint64_t o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
-    const uint64_t o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
-    const uint64_t o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
-    const uint64_t o_leaf_table = zl.take(uint64_t(d.leaf_cap) * 16);
-    uint64_t o_table[kMaxLevels + 2], o_bstat[kMaxLevels + 2], o_ostat[kMaxLevels + 2];
-    uint32_t cap[kMaxLevels + 2], btiles[kMaxLevels + 2], otiles[kMaxLevels + 2];
-    for (uint32_t lv = 2; lv < log2; ++lv) {
-        cap[lv] = next_pow2((uint64_t(P[lv]) * 100 + lf - 1) / lf, 1024);
-        uint32_t child = lv == 2 ? B : P[lv - 1];
-        btiles[lv] = std::max((child + kNodeBuildTile - 1) / kNodeBuildTile, 1u);
-        otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
-        o_table[lv] = zl.take(uint64_t(cap[lv]) * 16);
-        o_bstat[lv] = zl.take(uint64_t(btiles[lv]) * 8);
-        o_ostat[lv] = zl.take(uint64_t(otiles[lv]) * 8);
-    }
-    const uint64_t zero_bytes = align_up(zl.size, 256);
-    Layout fl;
-    fl.size = zero_bytes;
-    const uint64_t o_chunk_first = fl.take(4), o_roots = fl.take(4), o_prim_start = fl.take(4);
-    const uint64_t ff_bytes = align_up(fl.size, 256) - zero_bytes;
-    Layout ol;
-    ol.size = zero_bytes + ff_bytes;
-    const uint64_t o_seg_entry = ol.take(8), o_seg_tile = ol.take(8);
-    const uint64_t o_k0 = ol.take(uint64_t(nmax) * 4), o_v0 = ol.take(uint64_t(nmax) * 4);
-    const uint64_t o_k1 = ol.take(uint64_t(nmax) * 4), o_v1 = ol.take(uint64_t(nmax) * 4);
-    const uint64_t o_bkey = ol.take(uint64_t(B) * 8), o_bmask = ol.take(uint64_t(B) * 8);
-    const uint64_t o_bfirst = ol.take(uint64_t(B) * 4), o_bslot = ol.take(uint64_t(B) * 4);
-    const uint64_t o_bref = ol.take(uint64_t(B) * 4);
-    uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
-    uint64_t o_set[2][7];
-    for (int s = 0; s < 2; ++s) {
-        uint64_t m = std::max(setn[s], 1u);
-        o_set[s][0] = ol.take(m * 8);
-        o_set[s][1] = ol.take(m * 4);
-        o_set[s][2] = ol.take(m * 4);
-        o_set[s][3] = ol.take(m * 4);
-        o_set[s][4] = ol.take(m * 8);
-        o_set[s][5] = ol.take(m * 8);
-        o_set[s][6] = ol.take(m * kNodeStride * 4);
-    }
-    const uint64_t scratch_bytes = align_up(ol.size, 256);
-    if (scratch_bytes > kStaticScratchBytes)
+                    "prims %u)", p.d.node_bound, p.B, p.nmax, prim_need);
+    if (p.scratch_bytes > kStaticScratchBytes)
         return fail(PYRB_ERROR_INVALID_ARGUMENT,
                     "pyrb_build_noalloc: this build needs %llu bytes of scratch, the fixed array holds %llu",
-                    (unsigned long long)scratch_bytes, (unsigned long long)kStaticScratchBytes);
+                    (unsigned long long)p.scratch_bytes, (unsigned long long)kStaticScratchBytes);
 
     void* base = nullptr;
-    pyrb_result r = static_scratch(&base);
+    r = static_scratch(&base);
     if (r != PYRB_OK) return r;
-    auto at = [&](uint64_t off) { return static_cast<void*>(static_cast<unsigned char*>(base) + off); };
-    d.counters = static_cast<uint32_t*>(at(o_counters));
-    d.hist = static_cast<uint32_t*>(at(o_hist));
-    d.sort_status = static_cast<uint64_t*>(at(o_sort_status));
-    d.uniq_status = static_cast<uint64_t*>(at(o_uniq_status));
-    d.brick_status = static_cast<uint64_t*>(at(o_brick_status));
-    d.leafown_status = static_cast<uint64_t*>(at(o_leafown_status));
-    d.leaf_table = static_cast<uint4*>(at(o_leaf_table));
-    d.chunk_first = static_cast<uint32_t*>(at(o_chunk_first));
-    d.roots = static_cast<uint32_t*>(at(o_roots));
-    d.prim_start = static_cast<uint32_t*>(at(o_prim_start));
-    d.seg_entry = static_cast<uint32_t*>(at(o_seg_entry));
-    d.seg_tile = static_cast<uint32_t*>(at(o_seg_tile));
-    d.kbuf[0] = at(o_k0);
-    d.vbuf[0] = static_cast<uint32_t*>(at(o_v0));
-    d.kbuf[1] = at(o_k1);
-    d.vbuf[1] = static_cast<uint32_t*>(at(o_v1));
-    d.bkey = static_cast<uint64_t*>(at(o_bkey));
-    d.bmask = static_cast<uint64_t*>(at(o_bmask));
-    d.bfirst = static_cast<uint32_t*>(at(o_bfirst));
-    d.bslot = static_cast<uint32_t*>(at(o_bslot));
-    d.bref = static_cast<uint32_t*>(at(o_bref));
-    d.ukey = reinterpret_cast<uint64_t*>(keys);
-    d.uval = reinterpret_cast<uint32_t*>(attrs);
-    d.leaves = reinterpret_cast<uint64_t*>(leaves);
-    d.nodes = reinterpret_cast<uint32_t*>(nodes);
-    d.prims = reinterpret_cast<uint8_t*>(prims);
-    d.aabbs = reinterpret_cast<float*>(aabbs);
-
+    const uint64_t outs[6] = {nodes, leaves, keys, attrs, prims, aabbs};
     std::vector<LevelDesc> levels;
-    for (uint32_t lv = 2; lv < log2; ++lv) {
-        LevelDesc L;
-        std::memset(&L, 0, sizeof(L));
-        L.lv = lv;
-        L.child_bound = lv == 2 ? B : P[lv - 1];
-        L.parent_bound = P[lv];
-        L.build_tiles = btiles[lv];
-        L.own_tiles = otiles[lv];
-        L.need_box = lv + 1 <= rt ? 1u : 0u;
-        L.pcap = cap[lv];
-        L.tile_ctr_build = 12 + 2 * (lv - 2);
-        L.tile_ctr_own = 13 + 2 * (lv - 2);
-        const int ps = (lv - 2) & 1;
-        L.pkey = static_cast<uint64_t*>(at(o_set[ps][0]));
-        L.pcnt = static_cast<uint32_t*>(at(o_set[ps][1]));
-        L.pfirst = static_cast<uint32_t*>(at(o_set[ps][2]));
-        L.pslot = static_cast<uint32_t*>(at(o_set[ps][3]));
-        L.plo = static_cast<uint64_t*>(at(o_set[ps][4]));
-        L.phi = static_cast<uint64_t*>(at(o_set[ps][5]));
-        L.pwords = static_cast<uint32_t*>(at(o_set[ps][6]));
-        L.ptable = static_cast<uint4*>(at(o_table[lv]));
-        L.build_status = static_cast<uint64_t*>(at(o_bstat[lv]));
-        L.own_status = static_cast<uint64_t*>(at(o_ostat[lv]));
-        if (lv == 2) {
-            L.ckey = d.bkey;
-            L.cmask = d.bmask;
-            L.cfirst = d.bfirst;
-            L.cslot = d.bslot;
-            L.ctable = d.leaf_table;
-        } else {
-            const LevelDesc& C = levels.back();
-            L.ckey = C.pkey;
-            L.ccnt = C.pcnt;
-            L.cfirst = C.pfirst;
-            L.cslot = C.pslot;
-            L.clo = C.plo;
-            L.chi = C.phi;
-            L.ctable = C.ptable;
-        }
-        levels.push_back(L);
-    }
-
-    // the array keeps the previous call's contents: clear everything that must start
-    // at zero (counters, histograms, look-back status, dedup tables) and the 0xFF part
-    CU(cudaMemsetAsync(at(0), 0, zero_bytes, st));
-    CU(cudaMemsetAsync(at(zero_bytes), 0xFF, ff_bytes, st));
-    Prof prof(st);
-    launch(k_plan, 1, 1024, 0, st, d);
-    CU(cudaGetLastError());
-    CU((launch_sort<8, 16>(d, st, prof)));
-    launch(k_leaf_insert, leaf_insert_grid(d), kBlock, 0, st, d);
-    launch(k_leaf_own, d.leafown_tiles, kBlock, 0, st, d);
-    const uint32_t lv0 = tail_level(log2, B, P);
-    launch_levels(d, levels, lv0, make_tail(lv0, P, levels, d.leaf_table), st, prof);
-    CU(cudaGetLastError());
+    bind_plan(p, reinterpret_cast<uint64_t>(base), outs, j, levels);
+    // the array keeps the previous call's contents: launch_plan clears everything that
+    // must start at zero (counters, histograms, look-back status, dedup tables) and the
+    // 0xFF part before the first kernel
+    cudaError_t err = cudaSuccess;
+    const uint32_t launches = launch_plan(p, levels, st, &err);
+    if (err != cudaSuccess) return fail(PYRB_ERROR_CUDA, "pyrb_build_noalloc: %s", cudaGetErrorString(err));
     uint32_t ctr[kCtrCount];
-    CU(cudaMemcpyAsync(ctr, d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(ctr, p.d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    if (ctr[kCtrError]) return device_error(ctr[kCtrError]);
-    out->log2_size = log2;
-    out->rt_log2 = rt;
+    if (ctr[kCtrError]) return device_error(ctr);
+    out->log2_size = p.d.log2;
+    out->rt_log2 = p.d.rt_log2;
     out->nodes = nodes;
     out->leaves = leaves;
     out->keys = keys;
@@ -1537,6 +1522,11 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     out->prims = prims;
     out->aabbs = aabbs;
     fill_counts(ctr, out);
+    uint32_t meta[16] = {p.d.log2, p.d.rt_log2, p.passes, p.rb, launches};
+    const uint64_t out_bytes = p.out_bytes();
+    std::memcpy(meta + 5, &p.scratch_bytes, 8);
+    std::memcpy(meta + 7, &out_bytes, 8);
+    fill_stats(ctr, meta);
     return PYRB_OK;
 }
 

@@ -9,6 +9,7 @@ namespace pyrb {
 constexpr uint32_t kErrSpin = 1u;       // a look-back or wait gave up after its poll limit
 constexpr uint32_t kErrTable = 2u;      // a dedup table had no free slot
 constexpr uint32_t kErrBound = 4u;      // a count exceeded its allocated upper bound
+constexpr uint32_t kErrCapacity = 8u;   // a generator count exceeded the chunk capacity (world path)
 
 // Counter block (u32) read back at the end of a build.
 constexpr int kCtrUnique = 0;      // voxel_count
@@ -18,6 +19,7 @@ constexpr int kCtrWords = 3;       // node_words
 constexpr int kCtrRoot = 4;
 constexpr int kCtrPrims = 5;
 constexpr int kCtrError = 6;
+constexpr int kCtrNeed = 7;        // largest generator count above the chunk capacity (world path)
 constexpr int kCtrCursor = 8;      // + lv: first node word of level lv (lv = 2..25)
 constexpr int kCtrParents = 36;    // + lv: P_lv
 constexpr int kCtrUniqueLv = 64;   // + lv: U_lv

@@ -58,9 +58,18 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
         if (c < K) {
             switch (d.mode) {
                 case kModeChunks: size = __ldg(d.offsets + c + 1) - __ldg(d.offsets + c); break;
-                case kModeChunksEdits:
-                    size = min(__ldg(d.gen_counts + c), d.capacity) + (__ldg(d.edit_offsets + c + 1) - __ldg(d.edit_offsets + c));
+                case kModeChunksEdits: {
+                    // a count above the capacity is reported, never cut off silently: the
+                    // host gets PYRB_ERROR_CAPACITY with the largest count and keeps no
+                    // result (reads stay inside the chunk's capacity meanwhile)
+                    const uint32_t g = __ldg(d.gen_counts + c);
+                    if (g > d.capacity) {
+                        atomicMax(d.counters + kCtrNeed, g);
+                        atomicOr(d.counters + kCtrError, kErrCapacity);
+                    }
+                    size = min(g, d.capacity) + (__ldg(d.edit_offsets + c + 1) - __ldg(d.edit_offsets + c));
                     break;
+                }
                 case kModeBatch:
                     size = __ldg(d.voxel_offsets + c + 1) - __ldg(d.voxel_offsets + c);
                     if (d.edit_offsets2) size += __ldg(d.edit_offsets2 + c + 1) - __ldg(d.edit_offsets2 + c);
@@ -1563,6 +1572,19 @@ __global__ void __launch_bounds__(kBlock) k_finalize(BuildDesc d, LevelDesc top)
         }
         d.counters[kCtrRoot] = root;
         d.counters[kCtrWords] = cursor;
+    }
+}
+
+// Diagnostics: one bounded wait that nothing ends. Tile 1 looks back at tile 0,
+// whose status is never published; the wait gives up after kSpinLimit polls and sets
+// kErrSpin, exactly as a wait inside a build would (which 0: the per-digit look-back
+// of the sort passes, 1: the warp look-back of the compaction kernels). status:
+// 2 zeroed words; launched with one warp.
+__global__ void __launch_bounds__(32) k_selftest_wait(uint64_t* status, uint32_t* counters, uint32_t which) {
+    if (which == 0) {
+        if (threadIdx.x == 0) lookback_window<kSortWindow>(status, 1, 1, 0, 1, counters + kCtrError);
+    } else {
+        lookback_warp(status, 1, 0, 1, counters + kCtrError);
     }
 }
 

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libpyrit_b200.so")
 PYRB_OK = 0
 PYRB_ERROR_INVALID_ARGUMENT = -1
 PYRB_ERROR_OUT_OF_MEMORY = -3
+PYRB_ERROR_CAPACITY = -4
 PYRB_ERROR_CUDA = -6
 PYRB_BUILD_HOST_INPUT = 0x1
 
@@ -119,6 +120,10 @@ SIGNATURES = {
     "pyrb_palette_pack": (ctypes.c_int32, [ctypes.POINTER(Exec), _u64, _p, _u32, _u64, _p, _p, _u64]),
     "pyrb_build_noalloc": (ctypes.c_int32, [_p, _u32, _u32, _u64, _u32, _u64, _u32, _u64, _u32, _u64, _u64, _u32,
                                             _u64, _u64, _u32, ctypes.POINTER(BuiltC)]),
+    "pyrb_build_memory": (ctypes.c_int32, [_u32, _u32, _p, _u64, ctypes.POINTER(ctypes.c_uint64),
+                                           ctypes.POINTER(ctypes.c_uint64)]),
+    "pyrb_last_capacity_need": (ctypes.c_uint32, []),
+    "pyrb_selftest_wait_limit": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32]),
 }
 
 _lib = None

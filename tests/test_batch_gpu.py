@@ -104,3 +104,21 @@ def test_mixed_batch_with_large_sort_tiles(radix_bits):
         _check(log2s, chunks, None, rt=3)
     finally:
         gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+
+
+# The batched configuration's own chunk sizes: 2 chunks of 256^3, 3 of 128^3 and 20 of
+# 32^3 / 64^3 from the chunk-mix generator (heightfield tiled per chunk with caves) in
+# one batch. Such a batch gives segments of ~1000 sort tiles next to ones of a single
+# tile, the root of a small chunk three levels below the batch's top, and unique passes
+# split over many tiles; each chunk must still equal its own single build (the
+# reference's batch == single property, tests/cpu_test.zig:1001-1060).
+CONFIG2_LOG2S = [8, 5, 6, 7, 5, 5, 6, 8, 5, 7, 6, 5, 5, 6, 5, 7, 5, 6, 5, 5, 6, 5, 5, 6, 5]
+
+
+@pytest.mark.parametrize("with_edits", [False, True])
+def test_config2_mix_at_full_chunk_sizes(with_edits):
+    log2s = CONFIG2_LOG2S
+    assert log2s.count(8) == 2 and log2s.count(7) == 3 and len(log2s) == 25
+    chunks = [wl.mix_chunk(200 + i, l, 0) for i, l in enumerate(log2s)]
+    edits = [wl.chunk_edits(l, 64, 300 + i) for i, l in enumerate(log2s)] if with_edits else None
+    _check(log2s, chunks, edits, rt=5)

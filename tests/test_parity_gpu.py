@@ -144,9 +144,16 @@ def test_noise256_with_edits_matches_oracle(gb):
     vox = wl.noise_grid(8, 0)
     ed = wl.noise_edits(8, 0)
     pts = np.concatenate([vox, ed])
-    g = gb.build(8, 7, dev(pts)).download()
+    b = gb.build(8, 7, dev(pts))
+    st = gb.last_stats()
+    g = b.download()
     o = orc.gb_build(8, 7, pts)
     assert_same_build(g, o, label="noise256")
+    # the memory the build took is the host-side bound, under the reference's 130 B/voxel
+    # (tests/cpu_test.zig:1559-1629)
+    scratch, outputs = gb.build_memory(8, len(pts))
+    assert (st.scratch_bytes, st.output_bytes) == (scratch, outputs)
+    assert (scratch + outputs) / len(pts) < 130
 
 
 @pytest.mark.parametrize("radix_bits,tile_keys,lf", [(4, 1024, 50), (8, 2048, 70), (11, 4096, 50), (11, 1024, 90),
@@ -304,3 +311,41 @@ def test_world_edit_overlay_matches_worldedit_then_build_chunks(gb, seed):
         packed[c * cap:c * cap + oc[c]] = ov[c * cap:c * cap + oc[c]]
     o = orc.gb_build_chunks(log2, 4, cap, packed, offs)
     assert_same_build(g, o, chunks=True, label="world overlay")
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_world_edit_overlay_with_repeated_coordinates(gb, seed):
+    """Edit lists that name a coordinate several times and edits on generated voxels:
+    every chunk builds as if its edits were applied after its generated voxels in list
+    order (the last entry of a coordinate wins, attribute 0 removes) -- the build of
+    the concatenated lists, byte for byte."""
+    rng = np.random.default_rng(50 + seed)
+    K, log2, cap = 5, 5, 9000
+    n = 1 << log2
+    vox = np.zeros((K * cap, 4), np.uint32)
+    counts = np.zeros(K, np.uint32)
+    segs, edits, eoff = [], [], [0]
+    for c in range(K):
+        g = wl.mix_chunk(500 + c, log2, seed)[:cap // 2] if c != 3 else np.zeros((0, 4), np.uint32)
+        vox[c * cap:c * cap + len(g)] = g
+        counts[c] = len(g)
+        m = int(rng.integers(50, 600))
+        e = np.empty((m, 4), np.uint32)
+        e[:, :3] = rng.integers(0, n // 2, (m, 3))          # a small corner: many repeats
+        if len(g):
+            k = min(m // 3, len(g))
+            e[:k, :3] = g[rng.integers(0, len(g), k), :3]    # edits on generated voxels
+        e[:, 3] = np.where(rng.random(m) < 0.4, 0, rng.integers(1, 9, m))
+        edits.append(e)
+        eoff.append(eoff[-1] + m)
+        segs.append(np.concatenate([g, e]))
+    ed = np.concatenate(edits)
+    eoff = np.array(eoff, np.uint32)
+    got = gb.build_chunks_edits(log2, 4, K, cap, dev(vox), dev(counts), dev(ed), dev(eoff), int(eoff[-1])).download()
+    cap2 = max(len(sg) for sg in segs)
+    packed = np.zeros((K * cap2, 4), np.uint32)
+    for c in range(K):
+        packed[c * cap2:c * cap2 + len(segs[c])] = segs[c]
+    offs = np.concatenate([[0], np.cumsum([len(sg) for sg in segs])]).astype(np.uint32)
+    o = orc.gb_build_chunks(log2, 4, cap2, packed, offs)
+    assert_same_build(got, o, chunks=True, label="repeated edits")

@@ -11,9 +11,11 @@ from gpu_helpers import dev, subdag
 pytestmark = pytest.mark.gpu
 
 
-def _pool(n_chunks=12):
+def _pool(n_chunks=12, log2s=None):
     from pyrit_b200.serve import ChunkPool
-    log2s = np.array([5 if i % 3 else 6 for i in range(n_chunks)], np.uint32)
+    if log2s is None:
+        log2s = [5 if i % 3 else 6 for i in range(n_chunks)]
+    log2s = np.array(log2s, np.uint32)
     vox, offs = wl.mix_chunks_device(log2s, 40, 0)
     return ChunkPool(vox, offs, log2s), vox, offs
 
@@ -30,13 +32,22 @@ def _requests(pool, n, seed=0, rate=None):
     return out
 
 
-def test_results_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("edges", ["small", "full"])
+def test_results_same_alone_and_in_the_mix(edges):
+    """small: a pool of 32^3 / 64^3 chunks; full: the served configuration's edges up to
+    256^3 (every request drawn from 32^3 .. 256^3 chunks), batches of several MB."""
     import torch
     from pyrit_b200 import gpu_build
     from pyrit_b200.serve import ChunkServer
-    pool, vox, offs = _pool()
-    reqs = _requests(pool, 40)
-    srv = ChunkServer(pool, budget_bytes=8 << 30, max_batch_voxels=400_000, max_inflight=2, rt_log2=5)
+    if edges == "small":
+        pool, vox, offs = _pool()
+        reqs = _requests(pool, 40)
+        max_vox = 400_000
+    else:
+        pool, vox, offs = _pool(log2s=[8, 5, 7, 6, 5, 7, 6, 5, 8, 6])
+        reqs = _requests(pool, 24, seed=9)
+        max_vox = 12_000_000
+    srv = ChunkServer(pool, budget_bytes=8 << 30, max_batch_voxels=max_vox, max_inflight=2, rt_log2=5)
     stats = srv.serve(reqs, realtime=False)
     assert stats.batches >= 3 and stats.max_batch_requests >= 2
     host_vox = vox.cpu().numpy().view(np.uint32)

@@ -1,10 +1,11 @@
 """pyrb_build_noalloc: the build variant for callers that cannot allocate device memory
-while they build (frame loops that must not synchronise the device through
-cudaMalloc, code running during CUDA graph stream capture, fixed memory budgets).
+while they build -- a render or frame loop must not call cudaMalloc, which synchronises
+the whole device, and an engine with a fixed memory budget has no allocator to hand over.
 It keeps all scratch in a fixed device array inside the library; the test allocates
 the input and output buffers itself and checks, over two calls in a row, that the
 results equal pyrb_build's bit for bit (the second call also shows that the shared
-array is cleared between calls). This file is collected last on purpose."""
+array is cleared between calls), and at the documented limit (edge 256, about 2^20
+voxels) that they equal the oracle's. This file is collected last on purpose."""
 import ctypes
 
 import numpy as np
@@ -84,6 +85,44 @@ def test_noalloc_matches_pyrb_build_two_calls_in_a_row():
         assert np.array_equal(got["attrs"], ref.attrs)
         assert np.array_equal(got["prims"], ref.prims)
         assert np.array_equal(got["aabbs"], ref.aabbs.view(np.uint32))
+
+
+def _noise_octant_near_limit():
+    """About 10^6 entries at edge 256: the noise grid and its edits inside the octant
+    [0, 128)^3, plus repeats of part of it with new attributes (the last one wins)."""
+    vox, ed = wl.noise_grid(8, 0), wl.noise_edits(8, 0)
+    inside = lambda p: p[(p[:, 0] < 128) & (p[:, 1] < 128) & (p[:, 2] < 128)]
+    base = np.concatenate([inside(vox), inside(ed)])
+    rng = np.random.default_rng(4)
+    rep = base[rng.integers(0, len(base), (1 << 20) - 2 - len(base))].copy()
+    rep[:, 3] = rng.integers(0, 9, len(rep))
+    pts = np.concatenate([base, rep, np.array([[300, 0, 0, 7], [0, 0xFFFFFFFF, 0, 7]], np.uint32)])
+    assert len(pts) == 1 << 20
+    return pts
+
+
+def test_noalloc_at_its_limit_matches_the_oracle_two_calls_in_a_row():
+    from oracle import oracle as orc
+    pts = _noise_octant_near_limit()
+    o = orc.gb_build(8, 5, pts)
+    for _ in range(2):
+        got = _noalloc_build(8, 5, pts)
+        assert got["voxel_count"] == o.voxel_count and got["node_words"] == o.node_words
+        assert got["root"] == o.root and got["prim_count"] == o.prim_count
+        assert np.array_equal(got["nodes"], o.nodes)
+        assert np.array_equal(got["leaves"], o.leaves)
+        assert np.array_equal(got["keys"], o.keys)
+        assert np.array_equal(got["attrs"], o.attrs)
+        assert np.array_equal(got["prims"], o.prims)
+        assert np.array_equal(got["aabbs"], o.aabbs.view(np.uint32))
+
+
+def test_noalloc_without_input_builds_the_empty_geometry():
+    from pyrit_b200 import gpu_build
+    got = _noalloc_build(5, 3, np.zeros((0, 4), np.uint32))  # n_new 0, edits NULL
+    ref = gpu_build.build(5, 3, None, n_new=0).download()
+    assert got["voxel_count"] == 0 and got["node_words"] == ref.node_words == 2
+    assert got["root"] == ref.root and np.array_equal(got["nodes"], ref.nodes)
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit():
