@@ -335,11 +335,13 @@ PYRB_API pyrb_result pyrb_path_edit(const pyrb_exec* e, uint64_t nodes, uint64_t
  * pyrb_build; total for pyrb_build_chunks; count * capacity + edit_total for
  * pyrb_build_chunks_edits; voxel_total + edit_total for a batch) in `count` chunks of
  * edge 2^log2_size, or, when chunk_log2 (host u32[count]) is given, of edges
- * 2^chunk_log2[c] (a pyrb_build_batch; log2_size is ignored). Uses the current tuning.
+ * 2^chunk_log2[c] (a pyrb_build_batch; log2_size is ignored); rt_log2_req as the build
+ * takes it (it sizes the prim outputs). Uses the current tuning.
  * scratch_bytes: freed when the build returns; output_bytes: the six output buffers.
  * The reference bounds its build scratch with a counting Exec (tests/cpu_test.zig:1559-1629). */
-PYRB_API pyrb_result pyrb_build_memory(uint32_t log2_size, uint32_t count, const uint32_t* chunk_log2,
-                                       uint64_t entries, uint64_t* scratch_bytes, uint64_t* output_bytes);
+PYRB_API pyrb_result pyrb_build_memory(uint32_t log2_size, uint32_t rt_log2_req, uint32_t count,
+                                       const uint32_t* chunk_log2, uint64_t entries, uint64_t* scratch_bytes,
+                                       uint64_t* output_bytes);
 
 /* Largest generator count of the calling thread's last PYRB_ERROR_CAPACITY result
  * (the capacity to grow to; src/world.zig:968-996), 0 if there was none. */

@@ -1355,13 +1355,15 @@ PYRB_API pyrb_result pyrb_path_edit(const pyrb_exec* e, uint64_t nodes, uint64_t
     return done(PYRB_OK);
 }
 
-PYRB_API pyrb_result pyrb_build_memory(uint32_t log2_size, uint32_t count, const uint32_t* chunk_log2,
-                                       uint64_t entries, uint64_t* scratch_bytes, uint64_t* output_bytes) {
+PYRB_API pyrb_result pyrb_build_memory(uint32_t log2_size, uint32_t rt_log2_req, uint32_t count,
+                                       const uint32_t* chunk_log2, uint64_t entries, uint64_t* scratch_bytes,
+                                       uint64_t* output_bytes) {
     if (count == 0) return fail(PYRB_ERROR_INVALID_ARGUMENT, "count is 0");
     if (entries >= (uint64_t(1) << 31))
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "too many entries for one build (%llu)", (unsigned long long)entries);
     Job j;
     j.K = count;
+    j.rt_req = rt_log2_req;
     if (chunk_log2) {
         uint32_t lmax = 0;
         for (uint32_t c = 0; c < count; ++c) lmax = std::max(lmax, chunk_log2[c]);

@@ -302,17 +302,19 @@ def downsample(log2_src: int, rt_log2_req: int, src_keys, src_vals, n_src: int, 
     return Built(out, stream)
 
 
-def build_memory(log2_size: int, entries: int, count: int = 1, chunk_log2=None) -> tuple[int, int]:
+def build_memory(log2_size: int, entries: int, count: int = 1, chunk_log2=None, rt_log2_req: int = 3
+                 ) -> tuple[int, int]:
     """(scratch bytes, output bytes) a build of `entries` raw entries would allocate:
     one volume (count 1), `count` chunks of edge 2^log2_size, or a batch of chunks of
-    edges 2^chunk_log2[c]. Host-only; uses the current tuning."""
+    edges 2^chunk_log2[c]; rt_log2_req as the build takes it. Host-only; uses the
+    current tuning."""
     scratch, outs = ctypes.c_uint64(0), ctypes.c_uint64(0)
     lg = None
     if chunk_log2 is not None:
         lg = np.ascontiguousarray(chunk_log2, dtype=np.uint32)
         count = len(lg)
-    native.check(native.lib().pyrb_build_memory(log2_size, count, None if lg is None else lg.ctypes.data, entries,
-                                                ctypes.byref(scratch), ctypes.byref(outs)))
+    native.check(native.lib().pyrb_build_memory(log2_size, rt_log2_req, count, None if lg is None else lg.ctypes.data,
+                                                entries, ctypes.byref(scratch), ctypes.byref(outs)))
     return scratch.value, outs.value
 
 

@@ -120,7 +120,7 @@ SIGNATURES = {
     "pyrb_palette_pack": (ctypes.c_int32, [ctypes.POINTER(Exec), _u64, _p, _u32, _u64, _p, _p, _u64]),
     "pyrb_build_noalloc": (ctypes.c_int32, [_p, _u32, _u32, _u64, _u32, _u64, _u32, _u64, _u32, _u64, _u64, _u32,
                                             _u64, _u64, _u32, ctypes.POINTER(BuiltC)]),
-    "pyrb_build_memory": (ctypes.c_int32, [_u32, _u32, _p, _u64, ctypes.POINTER(ctypes.c_uint64),
+    "pyrb_build_memory": (ctypes.c_int32, [_u32, _u32, _u32, _p, _u64, ctypes.POINTER(ctypes.c_uint64),
                                            ctypes.POINTER(ctypes.c_uint64)]),
     "pyrb_last_capacity_need": (ctypes.c_uint32, []),
     "pyrb_selftest_wait_limit": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32]),

@@ -34,7 +34,7 @@ def test_bernoulli_1024_properties():
     b = gpu_build.build(log2, 7, dev(pts))
     st = gpu_build.last_stats()
     # the memory the build took is the host-side bound, under the reference's 130 B/voxel
-    scratch, outputs = gpu_build.build_memory(log2, len(pts))
+    scratch, outputs = gpu_build.build_memory(log2, len(pts), rt_log2_req=7)
     assert (st.scratch_bytes, st.output_bytes) == (scratch, outputs)
     assert (scratch + outputs) / len(pts) < 130
     h = b.download()

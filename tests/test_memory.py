@@ -16,7 +16,7 @@ DENSE_CONFIGS = [(8, 5_116_905), (10, 162_054_872)]
 
 @pytest.mark.parametrize("log2,entries", DENSE_CONFIGS)
 def test_bytes_per_entry_below_the_reference_cap(log2, entries):
-    scratch, outputs = gpu_build.build_memory(log2, entries)
+    scratch, outputs = gpu_build.build_memory(log2, entries, rt_log2_req=7)
     assert scratch > 0 and outputs > 0
     assert (scratch + outputs) / entries < 130
 

@@ -151,7 +151,7 @@ def test_noise256_with_edits_matches_oracle(gb):
     assert_same_build(g, o, label="noise256")
     # the memory the build took is the host-side bound, under the reference's 130 B/voxel
     # (tests/cpu_test.zig:1559-1629)
-    scratch, outputs = gb.build_memory(8, len(pts))
+    scratch, outputs = gb.build_memory(8, len(pts), rt_log2_req=7)
     assert (st.scratch_bytes, st.output_bytes) == (scratch, outputs)
     assert (scratch + outputs) / len(pts) < 130
 
