@@ -210,14 +210,17 @@ PYRB_API const char* pyrb_result_string(pyrb_result r);
 /* Tuning of the sort and the dedup tables (digit width 4, 8, 9, 10 or 11 bits; keys per
  * sort tile 1024, 2048 or 4096, or 8192 with 8- or 9-bit digits; both 0, the default:
  * chosen per build, 9 bits on 8192 entries where that takes one radix pass less than
- * 8 bits, else 8 bits on 4096; hash load factor in percent, 25..90). Applies to
- * builds started afterwards on any thread. Returns PYRB_ERROR_INVALID_ARGUMENT for
- * unsupported values. */
+ * 8 bits, else 8 bits on 4096; hash load factor in percent, 25..90) and of the way the
+ * voxels are ordered (path: 0 automatic, the default -- a cell grid in device memory
+ * for dense chunks of at most 2^10 edge with at most 4 cells per entry, else the radix
+ * sort; 1 always the sort; 2 the grid wherever the edge allows it). The output never
+ * depends on any of them. Applies to builds started afterwards on any thread. Returns
+ * PYRB_ERROR_INVALID_ARGUMENT for unsupported values. */
 typedef struct pyrb_tuning {
     uint32_t radix_bits;
     uint32_t tile_keys;
     uint32_t load_factor_pct;
-    uint32_t reserved;
+    uint32_t path;
 } pyrb_tuning;
 PYRB_API pyrb_result pyrb_set_tuning(const pyrb_tuning* t);
 PYRB_API void pyrb_get_tuning(pyrb_tuning* t);

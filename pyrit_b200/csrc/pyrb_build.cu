@@ -18,6 +18,7 @@
 #include "pyrit_b200.h"
 #include "pyrb_internal.h"
 #include "pyrb_kernels.cuh"
+#include "pyrb_grid.cuh"
 #include "pyrb_pathedit.cuh"
 
 using namespace pyrb;
@@ -69,6 +70,14 @@ cudaError_t launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
 std::atomic<uint32_t> g_radix_bits{0};  // 0 with g_tile_keys 0: chosen per build (auto_tuning)
 std::atomic<uint32_t> g_tile_keys{0};
 std::atomic<uint32_t> g_load_pct{50};
+// Sort or cell grid for the voxels of a build (pyrb_tuning.path)
+constexpr uint32_t kPathAuto = 0, kPathSort = 1, kPathGrid = 2;
+std::atomic<uint32_t> g_path{kPathAuto};
+// The grid path is taken automatically while the chunks hold at most this many cells
+// per entry (dense volumes: 256^3 noise at 30 % solid has 3.3, terrain chunks 2), and
+// at most kGridMaxCells cells in all (8 B each).
+constexpr uint64_t kGridCellsPerEntry = 4;
+constexpr uint64_t kGridMaxCells = uint64_t(1) << 33;
 
 // ---------------------------------------------------------------------------
 // memory: caller callbacks, else a library-owned stream-ordered pool per device
@@ -387,7 +396,7 @@ void auto_tuning(uint32_t sort_bits, uint32_t* rb, uint32_t* tile_keys) {
 struct Plan {
     BuildDesc d;
     uint32_t K = 1, rb = 8, it = 16, lf = 50, passes = 1, min_log2 = 3, rt = 3, n = 0, nmax = 1, B = 1;
-    bool chunked = false, key64 = false;
+    bool chunked = false, key64 = false, grid = false;
     uint32_t P[kMaxLevels + 2] = {};
     uint32_t cap[kMaxLevels + 2] = {}, btiles[kMaxLevels + 2] = {}, otiles[kMaxLevels + 2] = {};
     uint64_t o_counters = 0, o_hist = 0, o_sort_status = 0, o_uniq_status = 0, o_brick_status = 0,
@@ -395,6 +404,7 @@ struct Plan {
     uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
     uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
     uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bslot = 0, o_bref = 0;
+    uint64_t o_grid = 0, o_grid_off = 0;
     uint64_t o_set[2][7] = {};
     uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
     // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
@@ -409,7 +419,7 @@ struct Plan {
 // Digit width, tile and load factor of a build: the fixed tuning given, else the
 // library's current tuning (64-bit keys: 8-bit digits on 2048-key tiles).
 struct Tune {
-    uint32_t rb, tile_keys, lf;
+    uint32_t rb, tile_keys, lf, path;
 };
 
 pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
@@ -454,18 +464,26 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     const uint32_t nmax = p.nmax = std::max(n, 1u);
 
     // tuning (64-bit keys use 8-bit digits and 2048-key tiles)
-    uint32_t rb, tile_keys, lf;
+    uint32_t rb, tile_keys, lf, path;
     if (fixed) {
         rb = fixed->rb;
         tile_keys = fixed->tile_keys;
         lf = fixed->lf;
+        path = fixed->path;
     } else {
         rb = p.key64 ? 8u : g_radix_bits.load();
         tile_keys = p.key64 ? 2048u : g_tile_keys.load();
         if (rb == 0) auto_tuning(lb + 1, &rb, &tile_keys);
         lf = g_load_pct.load();
+        path = g_path.load();
     }
-    p.rb = rb;
+    // cells of all chunks; the grid path needs 32-bit keys (edges up to 2^10)
+    uint64_t grid_cells = 0;
+    for (uint32_t l = 3; l <= log2 && !p.key64; ++l) grid_cells += per_log2[l] << (3 * l);
+    if (!p.key64 && grid_cells <= kGridMaxCells)
+        p.grid = path == kPathGrid || (path == kPathAuto && grid_cells <= kGridCellsPerEntry * nmax);
+    if (p.grid) tile_keys = 4096;  // the scatter's tiles over the entries
+    p.rb = p.grid ? 0 : rb;
     p.it = tile_keys / kBlock;
     p.lf = lf;
 
@@ -484,12 +502,12 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     d.top = log2 - 1;
     d.chunked = p.chunked ? 1u : 0u;
 
-    // digit plan over lb + 1 bits (the invalid bit on top)
+    // digit plan over lb + 1 bits (the invalid bit on top); none for the grid
     const uint32_t sort_bits = lb + 1;
-    const uint32_t passes = p.passes = (sort_bits + rb - 1) / rb;
+    const uint32_t passes = p.passes = p.grid ? 0 : (sort_bits + rb - 1) / rb;
     d.passes = passes;
-    d.radix = 1u << rb;
-    {
+    d.radix = p.grid ? 0 : 1u << rb;
+    if (passes) {
         uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 0;
         for (uint32_t q = 0; q < passes; ++q) {
             uint32_t b = base + (q < extra ? 1 : 0);
@@ -537,14 +555,23 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     while ((d.leaf_cap >> d.leaf_region_shift) > d.leaf_regions) ++d.leaf_region_shift;
     d.node_bound = uint32_t(words);
     d.prim_bound = P[rt - 1];
+    if (p.grid) {
+        d.use_grid = 1;
+        d.grid_cells = grid_cells;
+        d.grid_tiles = uint32_t(std::max<uint64_t>((grid_cells + 64 * kGridTileBricks - 1) / (64 * kGridTileBricks), 1));
+    }
 
     // ---- scratch layout
     Layout zl;  // zero-initialised region
     p.o_counters = zl.take(kCtrCount * 4);
-    p.o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
-    p.o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
-    p.o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
-    p.o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
+    if (!p.grid) {
+        p.o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
+        p.o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
+        p.o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
+        p.o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
+    } else {
+        p.o_uniq_status = zl.take(uint64_t(d.grid_tiles) * 8);  // voxels | bricks << 31 per compaction tile
+    }
     p.o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
     // a table filled region by region is cleared by its insert kernel, not by the memset
     p.o_leaf_table = d.leaf_regions > 1 ? 0 : zl.take(uint64_t(d.leaf_cap) * 16);
@@ -558,6 +585,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_bstat[lv] = zl.take(uint64_t(p.btiles[lv]) * 8);
         p.o_ostat[lv] = zl.take(uint64_t(p.otiles[lv]) * 8);
     }
+    if (p.grid) p.o_grid = zl.take(grid_cells * 8);
     p.zero_bytes = align_up(zl.size, 256);
     Layout fl;  // 0xFF region follows
     fl.size = p.zero_bytes;
@@ -571,10 +599,14 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     p.o_seg_entry = ol.take(uint64_t(K + 1) * 4);
     p.o_seg_tile = ol.take(uint64_t(K + 1) * 4);
     const uint64_t kbytes = p.key64 ? 8 : 4;
-    p.o_k0 = ol.take(uint64_t(nmax) * kbytes);
-    p.o_v0 = ol.take(uint64_t(nmax) * 4);
-    p.o_k1 = ol.take(uint64_t(nmax) * kbytes);
-    p.o_v1 = ol.take(uint64_t(nmax) * 4);
+    if (!p.grid) {
+        p.o_k0 = ol.take(uint64_t(nmax) * kbytes);
+        p.o_v0 = ol.take(uint64_t(nmax) * 4);
+        p.o_k1 = ol.take(uint64_t(nmax) * kbytes);
+        p.o_v1 = ol.take(uint64_t(nmax) * 4);
+    } else {
+        p.o_grid_off = ol.take(uint64_t(K + 1) * 8);
+    }
     p.o_bkey = ol.take(uint64_t(B) * 8);
     p.o_bmask = ol.take(uint64_t(B) * 8);
     p.o_bfirst = ol.take(uint64_t(B) * 4);
@@ -628,19 +660,29 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     d.region_count = static_cast<uint32_t*>(at(p.o_regions));
     d.region_cursor = d.region_count + kMaxLeafRegions;
     d.region_zeroed = d.region_count + 2 * kMaxLeafRegions;
-    // the sort buffers are dead once the unique voxels are out: N x (kb + 4) bytes from
-    // k0 hold the B region-grouped masks, k1 their brick indices
-    d.pmask = static_cast<uint64_t*>(at(p.o_k0));
-    d.pidx = static_cast<uint32_t*>(at(p.o_k1));
+    // the sort buffers (or the cell grid) are dead once the unique voxels are out: N x
+    // (kb + 4) bytes from k0 hold the B region-grouped masks, k1 their brick indices
+    // (in the grid: 8 B per cell, at least 512 B per brick)
+    if (p.grid) {
+        d.grid = static_cast<uint64_t*>(at(p.o_grid));
+        d.grid_off = static_cast<uint64_t*>(at(p.o_grid_off));
+        d.pmask = d.grid;
+        d.pidx = reinterpret_cast<uint32_t*>(d.grid + p.B);
+    } else {
+        d.pmask = static_cast<uint64_t*>(at(p.o_k0));
+        d.pidx = static_cast<uint32_t*>(at(p.o_k1));
+    }
     d.chunk_first = static_cast<uint32_t*>(at(p.o_chunk_first));
     d.roots = static_cast<uint32_t*>(at(p.o_roots));
     d.prim_start = static_cast<uint32_t*>(at(p.o_prim_start));
     d.seg_entry = static_cast<uint32_t*>(at(p.o_seg_entry));
     d.seg_tile = static_cast<uint32_t*>(at(p.o_seg_tile));
-    d.kbuf[0] = at(p.o_k0);
-    d.vbuf[0] = static_cast<uint32_t*>(at(p.o_v0));
-    d.kbuf[1] = at(p.o_k1);
-    d.vbuf[1] = static_cast<uint32_t*>(at(p.o_v1));
+    if (!p.grid) {
+        d.kbuf[0] = at(p.o_k0);
+        d.vbuf[0] = static_cast<uint32_t*>(at(p.o_v0));
+        d.kbuf[1] = at(p.o_k1);
+        d.vbuf[1] = static_cast<uint32_t*>(at(p.o_v1));
+    }
     d.bkey = static_cast<uint64_t*>(at(p.o_bkey));
     d.bmask = static_cast<uint64_t*>(at(p.o_bmask));
     d.bfirst = static_cast<uint32_t*>(at(p.o_bfirst));
@@ -712,8 +754,16 @@ uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaSt
     ++launches;
     prof.mark("plan");
     if ((*err = cudaGetLastError()) != cudaSuccess) return 0;
-    if ((*err = launch_sort_any(p.rb, p.it, d, st, prof)) != cudaSuccess) return 0;
-    launches += 3 + p.passes;
+    if (p.grid) {
+        launch(k_grid_scatter, d.sort_tiles, kBlock, 0, st, d);
+        prof.mark("grid_scatter");
+        launch(k_grid_compact, d.grid_tiles, kBlock, 0, st, d);
+        prof.mark("grid_compact");
+        launches += 2;
+    } else {
+        if ((*err = launch_sort_any(p.rb, p.it, d, st, prof)) != cudaSuccess) return 0;
+        launches += 3 + p.passes;
+    }
     const uint32_t B = p.B;
     if (d.leaf_regions > 1) {
         launch(k_leaf_part, std::max(std::min((B + kBrickTile - 1) / kBrickTile, 148u * 8u), 1u), kBlock, 0, st, d);
@@ -1068,9 +1118,11 @@ PYRB_API pyrb_result pyrb_set_tuning(const pyrb_tuning* t) {
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "8192-key tiles take 8- or 9-bit digits");
     if (t->load_factor_pct < 25 || t->load_factor_pct > 90)
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "load_factor_pct must lie in [25, 90]");
+    if (t->path > kPathGrid) return fail(PYRB_ERROR_INVALID_ARGUMENT, "path must be 0 (automatic), 1 (sort) or 2 (grid)");
     g_radix_bits = t->radix_bits;
     g_tile_keys = t->tile_keys;
     g_load_pct = t->load_factor_pct;
+    g_path = t->path;
     return PYRB_OK;
 }
 
@@ -1079,7 +1131,7 @@ PYRB_API void pyrb_get_tuning(pyrb_tuning* t) {
     t->radix_bits = g_radix_bits;
     t->tile_keys = g_tile_keys;
     t->load_factor_pct = g_load_pct;
-    t->reserved = 0;
+    t->path = g_path;
 }
 
 // PYRD v1 (src/io.zig:88-129): 52-byte header, then nodes, leaves, attributes.
@@ -1485,7 +1537,7 @@ PYRB_API pyrb_result pyrb_build_noalloc(void* stream, uint32_t log2_size, uint32
     j.voxels = edits;
     j.n_new = n_new;
     // one fixed tuning: the scratch bound below holds for it at every allowed size
-    const Tune fixed{8, 4096, 50};
+    const Tune fixed{8, 4096, 50, kPathSort};
     Plan p;
     pyrb_result r = plan_build(j, &fixed, p);
     if (r != PYRB_OK) return r;

@@ -132,6 +132,17 @@ struct BuildDesc {
     uint32_t prim_bound;
     uint32_t* roots;         // [K] (chunk builds), 0xFFFFFFFF initialised
     uint32_t* prim_start;    // [K]
+
+    // Cell grid of a dense build (use_grid): one 64-bit cell per voxel position of
+    // every chunk in key (Morton) order, chunk after chunk; an entry at a position
+    // leaves (input index + 1) << 32 | attribute there by an atomic max, so the cell
+    // ends up holding the last entry of its position. Replaces the sort and the
+    // unique pass: a streaming compaction of the cells gives the sorted unique voxels.
+    uint32_t use_grid;
+    uint32_t grid_tiles;     // compaction tiles of kGridTileBricks bricks
+    uint64_t grid_cells;     // cells of all chunks (a multiple of 64)
+    uint64_t* grid;          // [grid_cells], zeroed before the build
+    uint64_t* grid_off;      // [K + 1] first cell of every chunk (k_plan)
 };
 
 // One node level: children (bricks at level 2) -> parents of edge 2^(lv+1).

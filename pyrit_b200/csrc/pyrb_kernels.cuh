@@ -49,8 +49,10 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint32_t s_scan[2][1024];
     __shared__ uint32_t s_carry[2];
+    __shared__ uint64_t s_cells[1024];
+    __shared__ uint64_t s_cell_carry;
     const uint32_t K = d.seg_count;
-    if (threadIdx.x == 0) { s_carry[0] = 0; s_carry[1] = 0; }
+    if (threadIdx.x == 0) { s_carry[0] = 0; s_carry[1] = 0; s_cell_carry = 0; }
     __syncthreads();
     for (uint32_t base = 0; base < K; base += 1024) {
         uint32_t c = base + threadIdx.x;
@@ -94,13 +96,32 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
             d.seg_entry[c] = s_carry[0] + s_scan[0][threadIdx.x] - size;
             d.seg_tile[c] = s_carry[1] + s_scan[1][threadIdx.x] - tiles;
         }
+        if (d.use_grid) {
+            // first cell of every chunk in the cell grid (chunk after chunk)
+            const uint32_t l = c < K ? (d.mode == kModeBatch ? __ldg(d.chunk_log2 + c) : d.log2) : 0;
+            const uint64_t cells = c < K ? uint64_t(1) << (3 * l) : 0;
+            s_cells[threadIdx.x] = cells;
+            __syncthreads();
+            for (uint32_t o = 1; o < 1024; o <<= 1) {
+                const uint64_t a = threadIdx.x >= o ? s_cells[threadIdx.x - o] : 0;
+                __syncthreads();
+                s_cells[threadIdx.x] += a;
+                __syncthreads();
+            }
+            if (c < K) d.grid_off[c] = s_cell_carry + s_cells[threadIdx.x] - cells;
+        }
         __syncthreads();
-        if (threadIdx.x == 0) { s_carry[0] += s_scan[0][1023]; s_carry[1] += s_scan[1][1023]; }
+        if (threadIdx.x == 0) {
+            s_carry[0] += s_scan[0][1023];
+            s_carry[1] += s_scan[1][1023];
+            if (d.use_grid) s_cell_carry += s_cells[1023];
+        }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         d.seg_entry[K] = s_carry[0];
         d.seg_tile[K] = s_carry[1];
+        if (d.use_grid) d.grid_off[K] = s_cell_carry;
     }
 }
 

@@ -65,7 +65,10 @@ COUNTS_WORDS = 176
 
 class Tuning(ctypes.Structure):
     _fields_ = [("radix_bits", ctypes.c_uint32), ("tile_keys", ctypes.c_uint32),
-                ("load_factor_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("load_factor_pct", ctypes.c_uint32), ("path", ctypes.c_uint32)]
+
+
+PATH_AUTO, PATH_SORT, PATH_GRID = 0, 1, 2
 
 
 class PathEditJob(ctypes.Structure):

@@ -93,17 +93,17 @@ def test_uniform_batch_equals_chunks_api():
 def test_mixed_batch_with_large_sort_tiles(radix_bits):
     """8192-entry sort tiles over segments of many sizes: full 32^3 chunks span four
     tiles, small chunks share none, empty ones take none."""
-    from pyrit_b200 import gpu_build
+    from pyrit_b200 import gpu_build, native
     rng = np.random.default_rng(11)
     log2s = [5, 3, 5, 4, 5, 3]
     kinds = ["full", "rand", "rand", "empty", "full", "rand"]
     chunks = [_chunk(rng, l, k) for l, k in zip(log2s, kinds)]
     old = gpu_build.get_tuning()
     try:
-        gpu_build.set_tuning(radix_bits, 8192, 50)
+        gpu_build.set_tuning(radix_bits, 8192, 50, native.PATH_SORT)
         _check(log2s, chunks, None, rt=3)
     finally:
-        gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+        gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
 
 
 # The batched configuration's own chunk sizes: 2 chunks of 256^3, 3 of 128^3 and 20 of
@@ -115,10 +115,16 @@ def test_mixed_batch_with_large_sort_tiles(radix_bits):
 CONFIG2_LOG2S = [8, 5, 6, 7, 5, 5, 6, 8, 5, 7, 6, 5, 5, 6, 5, 7, 5, 6, 5, 5, 6, 5, 5, 6, 5]
 
 
+@pytest.mark.parametrize("path", ["sort", "grid"])
 @pytest.mark.parametrize("with_edits", [False, True])
-def test_config2_mix_at_full_chunk_sizes(with_edits):
+def test_config2_mix_at_full_chunk_sizes(with_edits, path):
+    from pyrit_b200 import gpu_build, native
     log2s = CONFIG2_LOG2S
     assert log2s.count(8) == 2 and log2s.count(7) == 3 and len(log2s) == 25
     chunks = [wl.mix_chunk(200 + i, l, 0) for i, l in enumerate(log2s)]
     edits = [wl.chunk_edits(l, 64, 300 + i) for i, l in enumerate(log2s)] if with_edits else None
-    _check(log2s, chunks, edits, rt=5)
+    gpu_build.set_tuning(0, 0, 50, native.PATH_SORT if path == "sort" else native.PATH_GRID)
+    try:
+        _check(log2s, chunks, edits, rt=5)
+    finally:
+        gpu_build.set_tuning(0, 0, 50, native.PATH_AUTO)

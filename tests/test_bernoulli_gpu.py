@@ -14,16 +14,26 @@ from gpu_helpers import assert_same_build, dev
 pytestmark = pytest.mark.gpu
 
 
-def test_bernoulli_256_matches_oracle():
+@pytest.fixture(params=["sort", "grid"])
+def path(request):
+    """The sparse worst case on both paths: the radix sort (the automatic choice at 6.6
+    cells per entry) and the cell grid forced."""
+    from pyrit_b200 import gpu_build, native
+    gpu_build.set_tuning(0, 0, 50, native.PATH_SORT if request.param == "sort" else native.PATH_GRID)
+    yield request.param
+    gpu_build.set_tuning(0, 0, 50, native.PATH_AUTO)
+
+
+def test_bernoulli_256_matches_oracle(path):
     from pyrit_b200 import gpu_build
     vox = wl.bernoulli_grid(8, 1)
     ed = wl.uniform_edits(8, 16000, 1)
     pts = np.concatenate([vox, ed])
     g = gpu_build.build(8, 5, dev(pts)).download()
-    assert_same_build(g, orc.gb_build(8, 5, pts), label="bernoulli256")
+    assert_same_build(g, orc.gb_build(8, 5, pts), label="bernoulli256 " + path)
 
 
-def test_bernoulli_1024_properties():
+def test_bernoulli_1024_properties(path):
     import torch
     from pyrit_b200 import gpu_build
     log2, seed = 10, 0

@@ -13,12 +13,17 @@ from gpu_helpers import assert_same_build, dev
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def gb():
+@pytest.fixture(scope="module", params=["sort", "grid"])
+def gb(request):
+    """Every test of this module runs twice: voxels ordered by the radix sort, and by the
+    cell grid (where the edge allows it); the output must not depend on the path."""
     import torch
     assert torch.cuda.is_available(), "GPU tests need a CUDA device"
-    from pyrit_b200 import gpu_build
-    return gpu_build
+    from pyrit_b200 import gpu_build, native
+    path = native.PATH_SORT if request.param == "sort" else native.PATH_GRID
+    gpu_build.set_tuning(0, 0, 50, path)
+    yield gpu_build
+    gpu_build.set_tuning(0, 0, 50, native.PATH_AUTO)
 
 
 def _scene_points(log2, seed=21, dups=200):
@@ -165,10 +170,10 @@ def test_tuning_variants_are_bit_exact(gb, radix_bits, tile_keys, lf):
     o = orc.gb_build(6, 4, pts)
     old = gb.get_tuning()
     try:
-        gb.set_tuning(radix_bits, tile_keys, lf)
+        gb.set_tuning(radix_bits, tile_keys, lf, old.path)
         g = gb.build(6, 4, dev(pts)).download()
     finally:
-        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
     assert_same_build(g, o, label=f"tuning {radix_bits}/{tile_keys}/{lf}")
 
 
@@ -180,10 +185,10 @@ def test_large_sort_tiles_match_oracle(gb, radix_bits):
     o = orc.gb_build(7, 5, pts)
     old = gb.get_tuning()
     try:
-        gb.set_tuning(radix_bits, 8192, 50)
+        gb.set_tuning(radix_bits, 8192, 50, old.path)
         g = gb.build(7, 5, dev(pts)).download()
     finally:
-        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
     assert len(pts) % 8192 != 0
     assert_same_build(g, o, label=f"tiles 8192, {radix_bits} bits")
 
@@ -210,10 +215,10 @@ def test_brick_runs_across_tiles(gb, last_attr, tuning):
     o = orc.gb_build(5, 3, pts)
     old = gb.get_tuning()
     try:
-        gb.set_tuning(tuning[0], tuning[1], 50)
+        gb.set_tuning(tuning[0], tuning[1], 50, old.path)
         g = gb.build(5, 3, dev(pts)).download()
     finally:
-        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
     assert_same_build(g, o, label=f"duplicate runs, last attr {last_attr}, tuning {tuning}")
 
 
@@ -241,10 +246,10 @@ def test_leaf_table_regions_with_repeated_masks(gb, lf):
     o = orc.gb_build(9, 5, pts)
     old = gb.get_tuning()
     try:
-        gb.set_tuning(8, 4096, lf)
+        gb.set_tuning(8, 4096, lf, old.path)
         g = gb.build(9, 5, dev(pts)).download()
     finally:
-        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
     assert len(o.leaves) == 4
     assert_same_build(g, o, label=f"leaf regions, load factor {lf}")
 

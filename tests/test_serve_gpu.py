@@ -46,7 +46,7 @@ def test_results_same_alone_and_in_the_mix(edges):
     else:
         pool, vox, offs = _pool(log2s=[8, 5, 7, 6, 5, 7, 6, 5, 8, 6])
         reqs = _requests(pool, 24, seed=9)
-        max_vox = 12_000_000
+        max_vox = 4_000_000   # a 256^3 chunk (~8.8 M voxels) forms a batch alone, smaller ones share
     srv = ChunkServer(pool, budget_bytes=8 << 30, max_batch_voxels=max_vox, max_inflight=2, rt_log2=5)
     stats = srv.serve(reqs, realtime=False)
     assert stats.batches >= 3 and stats.max_batch_requests >= 2
