@@ -15,9 +15,10 @@ sort, unique, bricks/leaves, all node levels, prims) of that input.
           PyrVoxel input from pinned memory on a copy stream and reads its counts
           back; uploads overlap the previous build. The one-call-at-a-time figure
           (pyrb_geometry_build + PYRB_BUILD_HOST_INPUT) is reported beside it.
-  roofline  the onesweep scatter pass (dominant kernel): algorithmic bytes per launch
-          (16 B per entry: key+value read and written) / mean launch time from
-          per-stage CUDA events, against the measured HBM copy bandwidth.
+  roofline  the dominant HBM kernel of the build (largest share of its per-stage CUDA
+          event time): algorithmic bytes per launch / mean launch time, against the
+          measured HBM copy bandwidth; "kernels" lists every HBM kernel the same way
+          (byte formulas in kernel_roofline).
   cpu_baseline  the reference's CPU builder (restated in oracle/: hash-map overlay
           merge + buildPoints, src/dag_builder.zig) on one host core, one build.
 
@@ -195,28 +196,34 @@ def stage_profile(log2, rt, dpts, sptr, flush, steps):
     return {k: statistics.mean(v) for k, v in stage.items()}
 
 
-def kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak):
+def kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak, cells=0):
     """Algorithmic bytes / CUDA-event time of the build's HBM kernels against `peak`
     (GB/s). Bytes per launch (the roofline basis of the design notes):
+      grid_scatter  n_in (16 + 8)                read PyrVoxels, one 8-byte cell update each
+      grid_compact  8 cells + 12 n_u + 20 B      read every cell, write keys, attributes, bricks
       encode_hist   n_in (16 + kb + 4)           read PyrVoxels, write key + value
       sort_pass     n_in 2 (kb + 4)              read and write key + value
       unique_brick  n_in (kb + 4) + 12 n_u + 20 B
       leaf_part     20 B; leaf_insert 28 B; leaf_own 16 B + 8 L
       node level l  20 C + 28 P + 4 W            children C, parents P, words W written
-    with B bricks, L leaves, W = 2 U + C U / P for U unique parents."""
+    with B bricks, L leaves, W = 2 U + C U / P for U unique parents. Each entry also
+    carries "share": its part of the build's summed stage time (a sort pass: all passes)."""
     B = int(st.brick_count)
     out = {}
+    total_ms = sum(stage_ms.values()) or 1.0
 
-    def add(name, ms, nbytes):
+    def add(name, ms, nbytes, launches=1):
         if ms and ms > 0:
             gbs = nbytes / (ms / 1e3) / 1e9
             out[name] = {"ms": round(ms, 4), "alg_bytes": int(nbytes), "gbs": round(gbs, 1),
-                         "frac": round(gbs / peak, 4)}
+                         "frac": round(gbs / peak, 4), "share": round(launches * ms / total_ms, 4)}
 
+    add("grid_scatter", stage_ms.get("grid_scatter"), n_in * 24)
+    add("grid_compact", stage_ms.get("grid_compact"), 8 * cells + 12 * n_u + 20 * B)
     add("encode_hist", stage_ms.get("encode_hist"), n_in * (16 + key_bytes + 4))
     sort_keys = [k for k in stage_ms if k.startswith("sort_pass")]
     if sort_keys:
-        add("sort_pass", statistics.mean(stage_ms[k] for k in sort_keys), n_in * 2 * (key_bytes + 4))
+        add("sort_pass", statistics.mean(stage_ms[k] for k in sort_keys), n_in * 2 * (key_bytes + 4), len(sort_keys))
     add("unique_brick", stage_ms.get("unique_brick"), n_in * (key_bytes + 4) + 12 * n_u + 20 * B)
     add("leaf_part", stage_ms.get("leaf_part"), 20 * B)
     add("leaf_insert", stage_ms.get("leaf_insert"), 28 * B)
@@ -370,13 +377,17 @@ def run_ours(args):
 
     # per-stage profile (CUDA events after every launch of the build)
     stage_ms = stage_profile(LOG2, RT, dpts, sptr, flush, min(args.steps, 20))
-    sort_keys = [k for k in stage_ms if k.startswith("sort_pass")]
-    sort_ms = statistics.mean(stage_ms[k] for k in sort_keys)
     key_bytes = 4 if 3 * LOG2 + 1 <= 32 else 8
-    sort_bytes = 2 * (key_bytes + 4) * n_in
     peak, peak_kind = load_peaks()
-    achieved = sort_bytes / (sort_ms / 1e3) / 1e9
-    traffic = committed_traffic("k_sort_pass", args.workload)
+    # the dominant HBM kernel (largest share of the build's stage time)
+    kernels = kernel_roofline(stage_ms, st, n_in, n_u, sizes["leaves"], key_bytes, peak,
+                              cells=(1 << (3 * LOG2)) if st.sort_passes == 0 else 0)
+    dom = max(kernels, key=lambda k: kernels[k]["share"])
+    dom_kernel = {"grid_scatter": "k_grid_scatter", "grid_compact": "k_grid_compact", "sort_pass": "k_sort_pass",
+                  "encode_hist": "k_encode_hist", "unique_brick": "k_unique"}.get(dom, dom)
+    dom_bytes, dom_ms = kernels[dom]["alg_bytes"], kernels[dom]["ms"]
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = committed_traffic(dom_kernel, args.workload)
 
     # whole-build algorithmic bytes (read input once; write keys+attrs, leaves, nodes, prims)
     alg_bytes = 16 * n_in + 12 * n_u + 8 * sizes["leaves"] + 4 * sizes["node_words"] + 40 * sizes["prims"]
@@ -478,13 +489,16 @@ def run_ours(args):
                        "bricks": st.brick_count, "leaves": sizes["leaves"], "node_words": sizes["node_words"],
                        "prims": sizes["prims"], "sort_passes": st.sort_passes, "radix_bits": st.radix_bits,
                        "l2": "flushed between steps (512 MiB write outside the timed events)",
-                       "key_bits": 8 * key_bytes, "dedup_per_level": dedup,
+                       "key_bits": 8 * key_bytes, "path": "sort" if st.sort_passes else "cell grid",
+                       "dedup_per_level": dedup,
                        "scratch_bytes": int(st.scratch_bytes), "output_bytes_bound": int(st.output_bytes),
                        "parallelism": "replicas" if world > 1 else "single"},
             "hbm_gbs": hbm_gbs,
-            "roofline": {"bound": "hbm", "kernel": "k_sort_pass", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": dom_kernel, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": sort_bytes, "mean_launch_ms": sort_ms},
+                         "algorithmic_bytes_per_launch": dom_bytes, "mean_launch_ms": dom_ms,
+                         "share_of_build": kernels[dom]["share"]},
+            "kernels": kernels,
             "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
             "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": 16 * n_in,
                     "d2h_bytes_per_step": 4 * native.COUNTS_WORDS,
@@ -553,7 +567,8 @@ def run_worst_case(args, reps=3):
     stage_ms = stage_profile(LOG2, RT, dpts, sptr, flush, reps)
     peak, peak_kind = load_peaks()
     key_bytes = 4 if 3 * LOG2 + 1 <= 32 else 8
-    kernels = kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak)
+    kernels = kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak,
+                              cells=(1 << (3 * LOG2)) if st.sort_passes == 0 else 0)
     dedup = {str(lv): {"parents": int(st.level_parents[lv]), "unique": int(st.level_unique[lv]),
                        "ratio": (st.level_parents[lv] / st.level_unique[lv]) if st.level_unique[lv] else None}
              for lv in range(2, LOG2)}
