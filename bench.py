@@ -708,6 +708,18 @@ def run_batched(args, emit=True):
     native.check(L.pyrb_build_finish(counts.data_ptr(), ctypes.byref(o)))
     n_u = o.voxel_count
     t_batched = min(times)
+    # per-stage CUDA events of one more batched build
+    L.pyrb_profile_enable(1)
+    try:
+        batched_once()
+        torch.cuda.synchronize()
+        ms = (ctypes.c_float * 256)()
+        names = ctypes.create_string_buffer(256 * 32)
+        k = L.pyrb_profile_read(ms, names, 32, 256)
+        batch_stages = {names.raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode(): round(ms[i], 4)
+                        for i in range(min(k, 256))}
+    finally:
+        L.pyrb_profile_enable(0)
 
     # chunk install: attribute palettes over the batch (scan + pack), device time
     bd = batch_desc(K)
@@ -787,7 +799,8 @@ def run_batched(args, emit=True):
            "n_gpus": world, "scaling": "weak", "chunks_per_gpu": K, "palette": palette, "path_edit": path_edit,
            "per_chunk_voxels_checked": "nodes[root + 1] of every chunk of the batch equals the voxel count of its "
                                        "plain build in the loop (%d chunks, %d empty)" % (K, K - len(nz)),
-           "tuning": {k: best[k] for k in ("radix_bits", "tile_keys", "load_factor_pct")},
+           "tuning": {k: best.get(k) for k in ("radix_bits", "tile_keys", "load_factor_pct", "path")},
+           "stages_ms": batch_stages,
            "edges": {str(1 << l): int((log2s == l).sum()) for l in (5, 6, 7, 8)}}
     if dist:
         dist.barrier()
@@ -834,7 +847,7 @@ def serve_autotune(vox, offs, log2s, budget_s, chunks=64):
 
     best, _ = autotune.sweep(once, reps=2, budget_s=budget_s)
     autotune.apply(best)
-    return {x: best[x] for x in ("radix_bits", "tile_keys", "load_factor_pct")}
+    return {x: best.get(x) for x in ("radix_bits", "tile_keys", "load_factor_pct", "path")}
 
 
 def run_served(args, emit=True):

@@ -1,11 +1,13 @@
-"""Autotuner of the build's sort and dedup parameters.
+"""Autotuner of the build's ordering path, sort and dedup parameters.
 
-Sweeps the radix digit width (4, 8, 9, 10, 11 bits), the keys per sort tile (1024,
-2048, 4096; 8192 with 8- or 9-bit digits) and the dedup hash-table load factor (50 %,
-70 %) on a caller-supplied
-workload, times every setting with CUDA events, applies the fastest through
-pyrb_set_tuning and can persist it as JSON. None of the parameters changes the
-output (the build is bit-exact for all of them); they only change speed and memory.
+Sweeps the way voxels are ordered (the cell grid, or the radix sort with its digit
+width of 4, 8, 9, 10, 11 bits and keys per sort tile of 1024, 2048, 4096, or 8192
+with 8- or 9-bit digits) and the dedup hash-table load factor (50 %, 70 %) on a
+caller-supplied workload, times every setting with CUDA events, applies the fastest
+through pyrb_set_tuning and can persist it as JSON. None of the parameters changes
+the output (the build is bit-exact for all of them); they only change speed and
+memory. The grid settings come first (two of them); the sort settings follow while
+the time budget lasts.
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ import json
 import os
 import time
 
-from . import gpu_build
+from . import gpu_build, native
 
 RADIX_BITS = (4, 8, 9, 10, 11)
 TILE_KEYS = (1024, 2048, 4096, 8192)
@@ -39,16 +41,17 @@ def sweep(run_once, reps: int = 3, radix_bits=RADIX_BITS, tile_keys=TILE_KEYS, l
     results = []
     if budget_s <= 0:   # no sweep: report the current setting
         cur = {"radix_bits": old.radix_bits, "tile_keys": old.tile_keys, "load_factor_pct": old.load_factor_pct,
-               "ms": None}
+               "path": old.path, "ms": None}
         return cur, [cur]
     t_start = time.time()
+    settings = [(0, 0, lf, native.PATH_GRID) for lf in load_factors] + [
+        (rb, tk, lf, native.PATH_SORT) for rb, tk, lf in itertools.product(radix_bits, tile_keys, load_factors)
+        if supported(rb, tk)]
     try:
-        for rb, tk, lf in itertools.product(radix_bits, tile_keys, load_factors):
-            if not supported(rb, tk):
-                continue
+        for rb, tk, lf, path in settings:
             if time.time() - t_start > budget_s:
                 break
-            gpu_build.set_tuning(rb, tk, lf)
+            gpu_build.set_tuning(rb, tk, lf, path)
             run_once()  # warm-up of this setting
             torch.cuda.synchronize()
             times = []
@@ -56,15 +59,17 @@ def sweep(run_once, reps: int = 3, radix_bits=RADIX_BITS, tile_keys=TILE_KEYS, l
                 a, b = run_once()
                 torch.cuda.synchronize()
                 times.append(a.elapsed_time(b))
-            results.append({"radix_bits": rb, "tile_keys": tk, "load_factor_pct": lf, "ms": min(times)})
+            results.append({"radix_bits": rb, "tile_keys": tk, "load_factor_pct": lf, "path": path,
+                            "ms": min(times)})
     finally:
-        gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct)
+        gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
     best = min(results, key=lambda r: r["ms"])
     return best, results
 
 
 def apply(setting: dict) -> None:
-    gpu_build.set_tuning(setting["radix_bits"], setting["tile_keys"], setting["load_factor_pct"])
+    gpu_build.set_tuning(setting["radix_bits"], setting["tile_keys"], setting["load_factor_pct"],
+                         setting.get("path", native.PATH_AUTO))
 
 
 def save(setting: dict, path: str | None = None) -> str:
