@@ -404,7 +404,7 @@ struct Plan {
     uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
     uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
     uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bslot = 0, o_bref = 0;
-    uint64_t o_grid = 0, o_grid_off = 0;
+    uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0;
     uint64_t o_set[2][7] = {};
     uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
     // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
@@ -569,8 +569,6 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
         p.o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
         p.o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
-    } else {
-        p.o_uniq_status = zl.take(uint64_t(d.grid_tiles) * 8);  // voxels | bricks << 31 per compaction tile
     }
     p.o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
     // a table filled region by region is cleared by its insert kernel, not by the memset
@@ -606,6 +604,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_v1 = ol.take(uint64_t(nmax) * 4);
     } else {
         p.o_grid_off = ol.take(uint64_t(K + 1) * 8);
+        p.o_grid_count = ol.take(uint64_t(d.grid_tiles) * 8);
     }
     p.o_bkey = ol.take(uint64_t(B) * 8);
     p.o_bmask = ol.take(uint64_t(B) * 8);
@@ -666,6 +665,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     if (p.grid) {
         d.grid = static_cast<uint64_t*>(at(p.o_grid));
         d.grid_off = static_cast<uint64_t*>(at(p.o_grid_off));
+        d.grid_count = static_cast<uint64_t*>(at(p.o_grid_count));
         d.pmask = d.grid;
         d.pidx = reinterpret_cast<uint32_t*>(d.grid + p.B);
     } else {
@@ -757,9 +757,13 @@ uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaSt
     if (p.grid) {
         launch(k_grid_scatter, d.sort_tiles, kBlock, 0, st, d);
         prof.mark("grid_scatter");
-        launch(k_grid_compact, d.grid_tiles, kBlock, 0, st, d);
-        prof.mark("grid_compact");
-        launches += 2;
+        launch(k_grid_count, d.grid_tiles, kBlock, 0, st, d);
+        prof.mark("grid_count");
+        launch(k_grid_scan, 1, kGridScanThreads, 0, st, d);
+        prof.mark("grid_scan");
+        launch(k_grid_write, d.grid_tiles, kBlock, 0, st, d);
+        prof.mark("grid_write");
+        launches += 4;
     } else {
         if ((*err = launch_sort_any(p.rb, p.it, d, st, prof)) != cudaSuccess) return 0;
         launches += 3 + p.passes;

@@ -12,18 +12,20 @@
 //                   with the largest index: the last one in input order, which is the
 //                   entry a stable sort puts last among equal keys. Entries out of
 //                   range are dropped, as their invalid key is.
-//   k_grid_compact  one streaming pass over the cells in key order, 64 bricks of 64
-//                   cells per tile: a cell is a voxel if some entry reached it and its
-//                   winner's attribute is not 0 (attribute 0 deletes). Ballots give each
-//                   brick's 64-bit mask directly; voxel and brick positions come from
-//                   one decoupled look-back over the tiles (both counts packed in one
-//                   status word). Output: the sorted unique keys and attributes, the
-//                   brick records and the per-chunk first voxel, exactly what the sort
-//                   path's k_unique writes.
+//   k_grid_count    the compaction, in three passes without waits between tiles:
+//   k_grid_scan     a cell is a voxel if its attribute word is not 0 (a cell no entry
+//   k_grid_write    reached is all zero; attribute 0 deletes). Tiles of 64 bricks of 64
+//                   cells: ballots give each brick's 64-bit mask directly. The count pass
+//                   writes every tile's voxels and non-empty bricks, one block scans
+//                   them, and the write pass reads the cells again and writes at the
+//                   final positions: the sorted unique keys and attributes, the brick
+//                   records and the per-chunk first voxel, exactly what the sort path's
+//                   k_unique writes. (A single pass with a decoupled look-back measured
+//                   barrier-bound: every block waited for its tile's look-back.)
 //
-// Bytes: 8 per cell for the zeroing, the atomics' line traffic and the read, against
-// 2 (kb + 4) per entry and pass of a sort: the grid wins while a chunk has at most a
-// few cells per entry (the host picks the path, see plan_build).
+// Bytes: 8 per cell for the zeroing, the atomics' line traffic and each of the two
+// reads, against 2 (kb + 4) per entry and pass of a sort: the grid wins while a chunk
+// has at most a few cells per entry (the host picks the path, see plan_build).
 #pragma once
 
 #include "pyrb_kernels.cuh"
@@ -66,54 +68,132 @@ __device__ __forceinline__ uint32_t grid_chunk(const BuildDesc& d, uint64_t cell
     return lo;
 }
 
-__global__ void __launch_bounds__(kBlock) k_grid_compact(BuildDesc d) {
+// The attribute words of a warp's kGridWarpBricks bricks: cells lane and 32 + lane of
+// each (a voxel is a cell whose attribute is not 0: a cell no entry reached is all
+// zero, and attribute 0 deletes). Only the low half of every 64-bit cell is loaded.
+__device__ __forceinline__ void grid_load_attrs(const BuildDesc& d, uint64_t wb0, uint64_t nbricks, uint32_t* a0,
+                                                uint32_t* a1) {
+    const unsigned lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < kGridWarpBricks; ++k) {
+        const uint64_t b = wb0 + k;
+        const uint32_t* cell = reinterpret_cast<const uint32_t*>(d.grid + (b << 6));
+        a0[k] = b < nbricks ? __ldcg(cell + 2 * lane) : 0u;
+        a1[k] = b < nbricks ? __ldcg(cell + 2 * (32 + lane)) : 0u;
+    }
+}
+
+// Pass 1 of the compaction: voxels and non-empty bricks of every tile, packed
+// (voxels | bricks << 32) into grid_count[tile]. No dependency between tiles.
+__global__ void __launch_bounds__(kBlock) k_grid_count(BuildDesc d) {
     grid_dep_wait();
-    __shared__ uint32_t s_tile;
-    __shared__ uint64_t s_scan[2 * kWarps + 2];
-    __shared__ uint64_t s_base;
+    __shared__ uint64_t s_sum[kWarps];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint64_t nbricks = d.grid_cells >> 6;
+    const uint64_t wb0 = uint64_t(tile) * kGridTileBricks + uint64_t(warp) * kGridWarpBricks;
+    uint32_t a0[kGridWarpBricks], a1[kGridWarpBricks];
+    grid_load_attrs(d, wb0, nbricks, a0, a1);
+    uint32_t vox = 0, bricks = 0;
+#pragma unroll
+    for (int k = 0; k < kGridWarpBricks; ++k) {
+        const uint32_t n = __popc(__ballot_sync(kFull, a0[k] != 0)) + __popc(__ballot_sync(kFull, a1[k] != 0));
+        vox += n;
+        bricks += n ? 1u : 0u;
+    }
+    if (lane == 0) s_sum[warp] = uint64_t(vox) | (uint64_t(bricks) << 32);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t t = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) t += s_sum[w];
+        d.grid_count[tile] = t;
+    }
+}
+
+// Pass 2: exclusive scan of the tile counts in place (one block, chunks of 8 per
+// thread); the totals are the build's voxel and brick counts.
+constexpr int kGridScanThreads = 1024, kGridScanPer = 8;
+__global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
+    grid_dep_wait();
+    __shared__ uint64_t s_w[kGridScanThreads / 32];
+    __shared__ uint64_t s_carry;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = kGridScanThreads / 32;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const uint32_t T = d.grid_tiles;
+    for (uint32_t base = 0; base < T; base += kGridScanThreads * kGridScanPer) {
+        const uint32_t i0 = base + threadIdx.x * kGridScanPer;
+        uint64_t v[kGridScanPer], sum = 0;
+#pragma unroll
+        for (int j = 0; j < kGridScanPer; ++j) {
+            v[j] = i0 + j < T ? d.grid_count[i0 + j] : 0;
+            sum += v[j];
+        }
+        uint64_t x = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(kFull, x, o);
+            if (lane >= unsigned(o)) x += y;
+        }
+        if (lane == 31) s_w[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            const uint64_t w = lane < unsigned(NW) ? s_w[lane] : 0;
+            uint64_t sw = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t y = __shfl_up_sync(kFull, sw, o);
+                if (lane >= unsigned(o)) sw += y;
+            }
+            if (lane < unsigned(NW)) s_w[lane] = sw - w;  // exclusive warp offsets
+        }
+        __syncthreads();
+        uint64_t run = s_carry + s_w[warp] + x - sum;
+#pragma unroll
+        for (int j = 0; j < kGridScanPer; ++j) {
+            if (i0 + j < T) d.grid_count[i0 + j] = run;
+            run += v[j];
+        }
+        __syncthreads();
+        if (threadIdx.x == kGridScanThreads - 1) s_carry = run;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        d.counters[kCtrUnique] = uint32_t(s_carry);
+        d.counters[kCtrBricks] = uint32_t(s_carry >> 32);
+    }
+}
+
+// Pass 3: every tile again, now with its first voxel and brick from the scan: sorted
+// unique keys and attributes, brick records, first voxel of every chunk.
+__global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
+    grid_dep_wait();
+    __shared__ uint64_t s_sum[kWarps];
     __shared__ uint32_t s_rcount[kMaxLeafRegions];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = dyn_tile(d.counters, 8, &s_tile);
-    if (tile >= d.grid_tiles) return;
+    const uint32_t tile = blockIdx.x;
     const bool regions = d.leaf_regions > 1;
     if (threadIdx.x < kMaxLeafRegions) s_rcount[threadIdx.x] = 0;
     const uint64_t nbricks = d.grid_cells >> 6;
     const uint64_t wb0 = uint64_t(tile) * kGridTileBricks + uint64_t(warp) * kGridWarpBricks;
-
-    // all loads first (16 per lane in flight), cells lane and 32 + lane of each brick;
-    // the grid is read once, so the loads stream past L1
-    uint64_t c0[kGridWarpBricks], c1[kGridWarpBricks];
+    uint32_t a0[kGridWarpBricks], a1[kGridWarpBricks];
+    grid_load_attrs(d, wb0, nbricks, a0, a1);
+    uint32_t vox = 0, bricks = 0;
 #pragma unroll
     for (int k = 0; k < kGridWarpBricks; ++k) {
-        const uint64_t b = wb0 + k;
-        const uint64_t* cell = d.grid + (b << 6);
-        c0[k] = b < nbricks ? __ldcs(reinterpret_cast<const unsigned long long*>(cell + lane)) : 0ull;
-        c1[k] = b < nbricks ? __ldcs(reinterpret_cast<const unsigned long long*>(cell + 32 + lane)) : 0ull;
+        const uint32_t n = __popc(__ballot_sync(kFull, a0[k] != 0)) + __popc(__ballot_sync(kFull, a1[k] != 0));
+        vox += n;
+        bricks += n ? 1u : 0u;
     }
-    // a voxel: some entry reached the cell and its winner's attribute is not 0
-    unsigned m0[kGridWarpBricks], m1[kGridWarpBricks];
-    uint32_t wvox = 0, wbricks = 0;
-#pragma unroll
-    for (int k = 0; k < kGridWarpBricks; ++k) {
-        m0[k] = __ballot_sync(kFull, (c0[k] >> 32) != 0 && uint32_t(c0[k]) != 0);
-        m1[k] = __ballot_sync(kFull, (c1[k] >> 32) != 0 && uint32_t(c1[k]) != 0);
-        const uint32_t n = __popc(m0[k]) + __popc(m1[k]);
-        wvox += n;
-        wbricks += n ? 1u : 0u;
-    }
-    // tile scan of (voxels | bricks << 31) over the warps, then the look-back
-    uint64_t total;
-    const uint64_t wexcl = block_excl_scan64(lane == 0 ? (uint64_t(wvox) | (uint64_t(wbricks) << 31)) : 0, s_scan, &total);
-    const uint64_t wofs = __shfl_sync(kFull, wexcl, 0);
-    if (warp == 0) {
-        if (lane == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | total);
-        const uint64_t ex = lookback_warp(d.uniq_status, tile, 0, total, d.counters + kCtrError);
-        if (lane == 0) s_base = ex;
-    }
+    if (lane == 0) s_sum[warp] = uint64_t(vox) | (uint64_t(bricks) << 32);
     __syncthreads();
-    const uint64_t base = s_base;
-    uint64_t vpos = (base & 0x7FFFFFFFull) + (wofs & 0x7FFFFFFFull);
-    uint64_t bpos = (base >> 31) + (wofs >> 31);
+    uint64_t wofs = d.grid_count[tile];  // the tile's first voxel | first brick << 32
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w)
+        if (w < int(warp)) wofs += s_sum[w];
+    uint64_t vpos = uint32_t(wofs), bpos = wofs >> 32;
     const unsigned lt = lanemask_lt();
     uint32_t seg = 0;
     uint64_t seg_lo = 0, seg_hi = 0;
@@ -124,7 +204,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_compact(BuildDesc d) {
     }
 #pragma unroll
     for (int k = 0; k < kGridWarpBricks; ++k) {
-        const unsigned lo = m0[k], hi = m1[k];
+        const unsigned lo = __ballot_sync(kFull, a0[k] != 0), hi = __ballot_sync(kFull, a1[k] != 0);
         if (!(lo | hi)) continue;                       // warp-uniform
         const uint64_t cell = (wb0 + k) << 6;
         while (cell >= seg_hi) {                         // bricks never straddle chunks
@@ -138,7 +218,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_compact(BuildDesc d) {
             const uint64_t p = vpos + __popc(lo & lt);
             if (p < d.n_total) {
                 d.ukey[p] = key0 + lane;
-                d.uval[p] = uint32_t(c0[k]);
+                d.uval[p] = a0[k];
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);
             }
@@ -147,7 +227,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_compact(BuildDesc d) {
             const uint64_t p = vpos + n0 + __popc(hi & lt);
             if (p < d.n_total) {
                 d.ukey[p] = key0 + 32 + lane;
-                d.uval[p] = uint32_t(c1[k]);
+                d.uval[p] = a1[k];
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);
             }
@@ -171,11 +251,6 @@ __global__ void __launch_bounds__(kBlock) k_grid_compact(BuildDesc d) {
         __syncthreads();
         if (threadIdx.x < d.leaf_regions && s_rcount[threadIdx.x])
             atomicAdd(d.region_count + threadIdx.x, s_rcount[threadIdx.x]);
-    }
-    if (tile == d.grid_tiles - 1 && threadIdx.x == 0) {
-        const uint64_t t = base + total;
-        d.counters[kCtrUnique] = uint32_t(t & 0x7FFFFFFFull);
-        d.counters[kCtrBricks] = uint32_t(t >> 31);
     }
 }
 
