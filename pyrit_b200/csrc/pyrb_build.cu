@@ -404,7 +404,7 @@ struct Plan {
     uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
     uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
     uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bslot = 0, o_bref = 0;
-    uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0;
+    uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0, o_chunk_vstart = 0;
     uint64_t o_set[2][7] = {};
     uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
     // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
@@ -605,6 +605,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     } else {
         p.o_grid_off = ol.take(uint64_t(K + 1) * 8);
         p.o_grid_count = ol.take(uint64_t(d.grid_tiles) * 8);
+        p.o_chunk_vstart = ol.take(uint64_t(K) * 4);
     }
     p.o_bkey = ol.take(uint64_t(B) * 8);
     p.o_bmask = ol.take(uint64_t(B) * 8);
@@ -666,6 +667,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
         d.grid = static_cast<uint64_t*>(at(p.o_grid));
         d.grid_off = static_cast<uint64_t*>(at(p.o_grid_off));
         d.grid_count = static_cast<uint64_t*>(at(p.o_grid_count));
+        d.chunk_vstart = static_cast<uint32_t*>(at(p.o_chunk_vstart));
         d.pmask = d.grid;
         d.pidx = reinterpret_cast<uint32_t*>(d.grid + p.B);
     } else {
@@ -764,6 +766,11 @@ uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaSt
         launch(k_grid_write, d.grid_tiles, kBlock, 0, st, d);
         prof.mark("grid_write");
         launches += 4;
+        if (d.chunked) {
+            launch(k_grid_chunks, std::max(std::min((p.K + kBlock - 1) / kBlock, 1024u), 1u), kBlock, 0, st, d);
+            prof.mark("grid_chunks");
+            ++launches;
+        }
     } else {
         if ((*err = launch_sort_any(p.rb, p.it, d, st, prof)) != cudaSuccess) return 0;
         launches += 3 + p.passes;

@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_count(BuildDesc d) {
 
 // Pass 2: exclusive scan of the tile counts in place (one block, chunks of 8 per
 // thread); the totals are the build's voxel and brick counts.
-constexpr int kGridScanThreads = 1024, kGridScanPer = 8;
+constexpr int kGridScanThreads = 1024, kGridScanPer = 16;
 __global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint64_t s_w[kGridScanThreads / 32];
@@ -204,14 +204,17 @@ __global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
     }
 #pragma unroll
     for (int k = 0; k < kGridWarpBricks; ++k) {
-        const unsigned lo = __ballot_sync(kFull, a0[k] != 0), hi = __ballot_sync(kFull, a1[k] != 0);
-        if (!(lo | hi)) continue;                       // warp-uniform
+        if (wb0 + k >= nbricks) break;                   // warp-uniform
         const uint64_t cell = (wb0 + k) << 6;
         while (cell >= seg_hi) {                         // bricks never straddle chunks
             ++seg;
             seg_lo = seg_hi;
             seg_hi = __ldg(d.grid_off + seg + 1);
         }
+        // the voxels before a chunk's first cell (k_grid_chunks turns them into its first voxel)
+        if (d.chunked && cell == seg_lo && lane == 0) d.chunk_vstart[seg] = uint32_t(vpos);
+        const unsigned lo = __ballot_sync(kFull, a0[k] != 0), hi = __ballot_sync(kFull, a1[k] != 0);
+        if (!(lo | hi)) continue;                       // warp-uniform
         const uint64_t key0 = (uint64_t(seg) << d.lb) | (cell - seg_lo);  // key of the brick's first cell
         const uint32_t n0 = __popc(lo);
         if ((lo >> lane) & 1) {
@@ -239,7 +242,6 @@ __global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
                 d.bmask[bpos] = mask;
                 d.bfirst[bpos] = uint32_t(vpos);
                 if (regions) atomicAdd(&s_rcount[leaf_region(d, mask)], 1u);
-                if (d.chunked) atomicMin(d.chunk_first + seg, uint32_t(vpos));
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);
             }
@@ -251,6 +253,17 @@ __global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
         __syncthreads();
         if (threadIdx.x < d.leaf_regions && s_rcount[threadIdx.x])
             atomicAdd(d.region_count + threadIdx.x, s_rcount[threadIdx.x]);
+    }
+}
+
+// First voxel of every chunk of a chunk build (chunkFirst, gbuild.zig:237-242): the
+// voxels before its first cell, or 0xFFFFFFFF for a chunk without voxels.
+__global__ void __launch_bounds__(kBlock) k_grid_chunks(BuildDesc d) {
+    grid_dep_wait();
+    const uint32_t total = d.counters[kCtrUnique];
+    for (uint32_t c = blockIdx.x * kBlock + threadIdx.x; c < d.seg_count; c += gridDim.x * kBlock) {
+        const uint32_t v = d.chunk_vstart[c], next = c + 1 < d.seg_count ? d.chunk_vstart[c + 1] : total;
+        d.chunk_first[c] = next > v ? v : 0xFFFFFFFFu;
     }
 }
 

@@ -144,6 +144,7 @@ struct BuildDesc {
     uint64_t* grid;          // [grid_cells], zeroed before the build
     uint64_t* grid_off;      // [K + 1] first cell of every chunk (k_plan)
     uint64_t* grid_count;    // [grid_tiles] voxels | bricks << 32 per tile, then their exclusive scan
+    uint32_t* chunk_vstart;  // [K] voxels before the first cell of every chunk (chunk builds)
 };
 
 // One node level: children (bricks at level 2) -> parents of edge 2^(lv+1).
