@@ -41,6 +41,10 @@ __device__ __forceinline__ void red_max_u64(uint64_t* p, uint64_t v) {
 
 // Entries -> cells. Tiles follow the per-segment tiling of the sort path (tile_span),
 // so the entry index (the order that decides) and the chunk are those of the sort.
+// PyrVoxel segments (every mode but old keys and downsampling) take the fast loop:
+// the chunk's voxel and edit lists are resolved once per tile, and each thread keeps
+// kScatterBatch 16-byte loads in flight before it encodes and updates their cells.
+constexpr int kScatterBatch = 4;
 __global__ void __launch_bounds__(kBlock) k_grid_scatter(BuildDesc d) {
     grid_dep_wait();
     const uint32_t tile = blockIdx.x;
@@ -49,12 +53,71 @@ __global__ void __launch_bounds__(kBlock) k_grid_scatter(BuildDesc d) {
     const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
     uint64_t* cells = d.grid + __ldg(d.grid_off + sp.seg);
     const uint32_t inv = 1u << d.lb;
+    // the segment's entries: src[0, nv) then esrc[0, ...)
+    const uint4* src = nullptr;
+    const uint4* esrc = nullptr;
+    uint32_t nv = 0, log2c = d.log2;
+    bool fast = true;
+    switch (d.mode) {
+        case kModePlain:
+            fast = d.n_old == 0;
+            src = d.voxels;
+            nv = d.n_new;
+            break;
+        case kModeChunks:
+            src = d.voxels + uint64_t(sp.seg) * d.capacity;
+            nv = d.capacity;  // offsets[] never exceed it
+            break;
+        case kModeChunksEdits:
+            src = d.voxels + uint64_t(sp.seg) * d.capacity;
+            nv = min(__ldg(d.gen_counts + sp.seg), d.capacity);
+            esrc = d.edits + __ldg(d.edit_offsets + sp.seg);
+            break;
+        case kModeBatch: {
+            const uint32_t vo = __ldg(d.voxel_offsets + sp.seg);
+            src = d.voxels + (d.voxel_starts ? __ldg(d.voxel_starts + sp.seg) : uint64_t(vo));
+            nv = __ldg(d.voxel_offsets + sp.seg + 1) - vo;
+            esrc = d.edit_offsets2 ? d.edits + __ldg(d.edit_offsets2 + sp.seg) : nullptr;
+            log2c = __ldg(d.chunk_log2 + sp.seg);
+            break;
+        }
+        default:
+            fast = false;
+            break;
+    }
+    const uint32_t j0 = sp.start - seg_begin;
+    if (!fast) {
 #pragma unroll 4
-    for (uint32_t idx = threadIdx.x; idx < sp.count; idx += kBlock) {
-        const uint32_t e = sp.start + idx;
-        uint32_t key = 0, val = 0;
-        load_raw(d, sp.seg, e - seg_begin, key, val);
-        if (!(key & inv)) red_max_u64(cells + key, (uint64_t(e + 1) << 32) | val);
+        for (uint32_t idx = threadIdx.x; idx < sp.count; idx += kBlock) {
+            const uint32_t e = sp.start + idx;
+            uint32_t key = 0, val = 0;
+            load_raw(d, sp.seg, e - seg_begin, key, val);
+            if (!(key & inv)) red_max_u64(cells + key, (uint64_t(e + 1) << 32) | val);
+        }
+        return;
+    }
+    for (uint32_t base = 0; base < sp.count; base += kScatterBatch * kBlock) {
+        uint4 v[kScatterBatch];
+#pragma unroll
+        for (int k = 0; k < kScatterBatch; ++k) {
+            const uint32_t idx = base + k * kBlock + threadIdx.x;
+            const uint32_t j = j0 + idx;
+            // past the voxel list: the edits, if the segment has any (else the entry is
+            // dropped, as load_raw drops a chunk entry past its capacity)
+            v[k] = make_uint4(0xFFFFFFFFu, 0, 0, 0);
+            if (idx < sp.count) {
+                if (j < nv) v[k] = __ldcs(src + j);
+                else if (esrc) v[k] = __ldcs(esrc + (j - nv));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kScatterBatch; ++k) {
+            const uint32_t idx = base + k * kBlock + threadIdx.x;
+            uint32_t key, val;
+            encode_voxel(v[k], log2c, d.lb, key, val);
+            if (idx < sp.count && !(key & inv))
+                red_max_u64(cells + key, (uint64_t(sp.start + idx + 1) << 32) | val);
+        }
     }
 }
 
@@ -168,7 +231,9 @@ __global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
 
 // Pass 3: every tile again, now with its first voxel and brick from the scan: sorted
 // unique keys and attributes, brick records, first voxel of every chunk.
-__global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
+// 5 tiles per SM (48 registers): the tiles write as soon as their loads arrive, so
+// more of them in flight keep more loads outstanding
+__global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint64_t s_sum[kWarps];
     __shared__ uint32_t s_rcount[kMaxLeafRegions];
@@ -193,7 +258,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
 #pragma unroll
     for (int w = 0; w < kWarps; ++w)
         if (w < int(warp)) wofs += s_sum[w];
-    uint64_t vpos = uint32_t(wofs), bpos = wofs >> 32;
+    uint32_t vpos = uint32_t(wofs), bpos = uint32_t(wofs >> 32);
     const unsigned lt = lanemask_lt();
     uint32_t seg = 0;
     uint64_t seg_lo = 0, seg_hi = 0;
@@ -212,13 +277,13 @@ __global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
             seg_hi = __ldg(d.grid_off + seg + 1);
         }
         // the voxels before a chunk's first cell (k_grid_chunks turns them into its first voxel)
-        if (d.chunked && cell == seg_lo && lane == 0) d.chunk_vstart[seg] = uint32_t(vpos);
+        if (d.chunked && cell == seg_lo && lane == 0) d.chunk_vstart[seg] = vpos;
         const unsigned lo = __ballot_sync(kFull, a0[k] != 0), hi = __ballot_sync(kFull, a1[k] != 0);
         if (!(lo | hi)) continue;                       // warp-uniform
         const uint64_t key0 = (uint64_t(seg) << d.lb) | (cell - seg_lo);  // key of the brick's first cell
         const uint32_t n0 = __popc(lo);
         if ((lo >> lane) & 1) {
-            const uint64_t p = vpos + __popc(lo & lt);
+            const uint32_t p = vpos + __popc(lo & lt);
             if (p < d.n_total) {
                 d.ukey[p] = key0 + lane;
                 d.uval[p] = a0[k];
@@ -227,7 +292,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
             }
         }
         if ((hi >> lane) & 1) {
-            const uint64_t p = vpos + n0 + __popc(hi & lt);
+            const uint32_t p = vpos + n0 + __popc(hi & lt);
             if (p < d.n_total) {
                 d.ukey[p] = key0 + 32 + lane;
                 d.uval[p] = a1[k];
@@ -240,7 +305,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_write(BuildDesc d) {
             if (bpos < d.brick_bound) {
                 d.bkey[bpos] = key0 >> 6;
                 d.bmask[bpos] = mask;
-                d.bfirst[bpos] = uint32_t(vpos);
+                d.bfirst[bpos] = vpos;
                 if (regions) atomicAdd(&s_rcount[leaf_region(d, mask)], 1u);
             } else {
                 atomicOr(d.counters + kCtrError, kErrBound);
