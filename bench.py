@@ -569,6 +569,28 @@ def run_worst_case(args, reps=3):
     n_u, leaves = o.voxel_count, o.leaf_count
     st = gpu_build.last_stats()
     stage_ms = stage_profile(LOG2, RT, dpts, sptr, flush, reps)
+    # both ways of ordering the voxels, forced (the automatic choice is timed above)
+    paths = {}
+    old = gpu_build.get_tuning()
+    try:
+        for name, code in (("sort", native.PATH_SORT), ("grid", native.PATH_GRID)):
+            gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, code)
+            L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(build_async()))
+            tt = []
+            for s in range(reps):
+                flush.fill_(s & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                q = build_async()
+                b.record(stream)
+                L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(q))
+                torch.cuda.synchronize()
+                tt.append(a.elapsed_time(b))
+            paths[name] = {"ms_per_build": statistics.median(tt),
+                           "stages_ms": {k: round(v, 4) for k, v in
+                                         stage_profile(LOG2, RT, dpts, sptr, flush, 1).items()}}
+    finally:
+        gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
     peak, peak_kind = load_peaks()
     key_bytes = 4 if 3 * LOG2 + 1 <= 32 else 8
     kernels = kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak,
@@ -583,6 +605,7 @@ def run_worst_case(args, reps=3):
             "leaves": leaves, "ms_per_build": t, "voxels_per_s": n_u / (t / 1e3),
             "sort_passes": int(st.sort_passes), "radix_bits": int(st.radix_bits),
             "peak_gbs": peak, "peak_kind": peak_kind, "kernels": kernels, "dedup_per_level": dedup,
+            "path": "sort" if st.sort_passes else "cell grid", "paths_forced": paths,
             "scratch_plus_output_bytes_per_entry": (st.scratch_bytes + st.output_bytes) / n_in,
             "how": "pyrb_build_async on the resident input, CUDA events around each build (median of %d), "
                    "per-stage events from pyrb_profile_enable" % reps}
@@ -909,7 +932,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["noise256", "bernoulli1024", "bernoulli512", "batched", "served"], default="noise256")
+    ap.add_argument("--workload", choices=["noise256", "bernoulli1024", "bernoulli512", "batched", "served", "worst"],
+                    default="noise256")
     ap.add_argument("--rates", type=float, nargs="+", default=[20000.0])
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--max-batch-voxels", type=int, default=64 << 20)
@@ -928,6 +952,12 @@ def main():
         return 0
     if args.workload == "served":
         run_served(args)
+        return 0
+    if args.workload == "worst":
+        import torch
+        torch.cuda.set_device(_env_int("LOCAL_RANK", 0))
+        print(json.dumps({"metric": METRIC + " (worst case)", "unit": "voxels/s", "n_gpus": 1,
+                          "worst_case": run_worst_case(args)}), flush=True)
         return 0
     return run_ours(args)
 
