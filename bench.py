@@ -880,7 +880,8 @@ def serve_autotune(vox, offs, log2s, budget_s, chunks=64):
 def run_served(args, emit=True):
     """Poisson arrivals of chunk-build requests (a chunk of the 1024-chunk mix plus 0..64
     random edits) at --rate per second for --duration seconds, served by continuous
-    batching with a 40 GB budget for dedup tables and the DAG arena."""
+    batching (the library's native served loop, pyrb_server_*) with a 40 GB budget for
+    dedup tables, scratch and the DAG arena."""
     import torch
     from pyrit_b200 import workloads as wl
     from pyrit_b200.serve import ChunkPool, ChunkServer, Request
@@ -909,6 +910,7 @@ def run_served(args, emit=True):
         srv.release_all()
         st = srv.serve(reqs, realtime=True)
         srv.release_all()
+        srv.close()
         s = st.summary()
         s["offered_req_per_s"] = rate
         s["offered_voxels_per_s"] = float(np.mean(pool.sizes[chunks]) * rate)
@@ -936,7 +938,7 @@ def main():
                     default="noise256")
     ap.add_argument("--rates", type=float, nargs="+", default=[20000.0])
     ap.add_argument("--duration", type=float, default=10.0)
-    ap.add_argument("--max-batch-voxels", type=int, default=64 << 20)
+    ap.add_argument("--max-batch-voxels", type=int, default=32 << 20)
     ap.add_argument("--chunks", type=int, default=1024)
     ap.add_argument("--batched-reps", type=int, default=3)
     ap.add_argument("--tune-budget", type=float, default=15.0)

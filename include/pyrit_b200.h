@@ -358,6 +358,67 @@ PYRB_API uint32_t pyrb_last_capacity_need(void);
  * build error ... look-back wait limit". Synchronises the exec's stream. */
 PYRB_API pyrb_result pyrb_selftest_wait_limit(const pyrb_exec* e, uint32_t which);
 
+/* Served chunk builds: continuous batching of chunk-build requests on one GPU, the
+ * served form beside the reference's streaming world job (World.gpuWorkImpl on its
+ * worker thread, src/world.zig:937-1025, admission by free device memory :814-821,
+ * LRU eviction of unused chunks, src/world_plan.zig:273-292). Requests name a chunk of
+ * a device-resident pool of chunk voxel lists plus up to max_edits overlay edits
+ * (host {x, y, z, attribute}; attribute 0 removes; the last entry of a coordinate
+ * wins). A worker thread keeps up to max_inflight batches enqueued on the server's own
+ * stream; whenever one completes, the requests that arrived meanwhile form the next
+ * pyrb_build_batch (at most max_batch_requests and max_batch_entries voxels + edits;
+ * a larger request runs alone). All scratch and results live in one device arena of
+ * budget_bytes: a batch is admitted when the build's exact need (pyrb_build_memory)
+ * fits, after evicting the least recently completed batches (those whose results were
+ * all released first). A result stays valid until released or, when the arena is
+ * full, evicted: copy out what must outlive that. Each result is bit-identical to the
+ * same chunk built alone. */
+typedef struct pyrb_server pyrb_server;
+typedef struct pyrb_server_config {
+    const uint32_t* pool_log2;    /* host u32[pool_count]: edge 2^log2 of every pool chunk, log2 in [3, 10] */
+    const uint64_t* pool_starts;  /* host u64[pool_count]: first PyrVoxel of chunk c in pool_voxels */
+    const uint32_t* pool_sizes;   /* host u32[pool_count]: PyrVoxels of chunk c (chunk-local coordinates) */
+    uint64_t pool_voxels;         /* device PyrVoxel[]; must stay valid while the server lives */
+    uint32_t pool_count;
+    uint32_t rt_log2;             /* RT prim level of every build */
+    uint64_t budget_bytes;        /* device arena for every batch's scratch and the results */
+    uint64_t max_batch_entries;   /* voxels + edits of one batch */
+    uint32_t max_batch_requests;
+    uint32_t max_edits;           /* per request */
+    uint32_t max_inflight;        /* batches enqueued on the GPU at once */
+    uint32_t reserved;
+} pyrb_server_config;
+typedef struct pyrb_server_result {
+    uint64_t id;                  /* the submitted id */
+    int32_t status;               /* PYRB_OK, or the error of its batch */
+    uint32_t root;                /* node offset of the chunk's root in batch.nodes; 0xFFFFFFFF: no voxels */
+    uint32_t first_voxel;         /* its first key / attribute in batch.keys / batch.attrs */
+    uint32_t first_prim;          /* its first prim in batch.prims / batch.aabbs */
+    uint32_t voxel_count;
+    uint32_t reserved;
+    pyrb_built batch;             /* buffers of the batch that built it (shared; owned by the server) */
+    double latency_ms;            /* submit -> the server saw its batch complete (host clock) */
+} pyrb_server_result;
+typedef struct pyrb_server_stats {
+    uint64_t requests, batches, failed_batches, evictions, voxels, peak_bytes, arena_used;
+    uint32_t max_batch_requests, pending, inflight, reserved;
+} pyrb_server_stats;
+/* Creates the server on the current device (allocates the arena and the staging
+ * buffers once, starts the worker thread). */
+PYRB_API pyrb_result pyrb_server_create(const pyrb_server_config* cfg, pyrb_server** out);
+/* Queues a request (any thread). */
+PYRB_API pyrb_result pyrb_server_submit(pyrb_server* s, uint64_t id, uint32_t chunk, const uint32_t* edits,
+                                        uint32_t n_edits);
+/* Copies up to `cap` finished results (in completion order) and removes them from the queue. */
+PYRB_API uint32_t pyrb_server_poll(pyrb_server* s, pyrb_server_result* out, uint32_t cap);
+/* The caller no longer needs result `id`; a batch is freed once all its results are released. */
+PYRB_API pyrb_result pyrb_server_release(pyrb_server* s, uint64_t id);
+PYRB_API void pyrb_server_get_stats(pyrb_server* s, pyrb_server_stats* out);
+/* Waits (up to timeout_ms) until no request is pending or on the GPU. */
+PYRB_API pyrb_result pyrb_server_drain(pyrb_server* s, uint32_t timeout_ms);
+/* Stops the worker, waits for the GPU, frees everything (results included). */
+PYRB_API void pyrb_server_destroy(pyrb_server* s);
+
 /* Library version (major << 16 | minor). */
 PYRB_API uint32_t pyrb_version(void);
 

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 
-CUDA_SOURCES = ["pyrb_build.cu"]
+CUDA_SOURCES = ["pyrb_build.cu", "pyrb_server.cpp"]
 # every header next to the sources: a change to any of them rebuilds the library
 CUDA_HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")) and not f.startswith("workloads"))
 WORKLOAD_SOURCES = ["workloads.cpp", "workloads_gpu.cu"]

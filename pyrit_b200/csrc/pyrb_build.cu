@@ -898,6 +898,11 @@ pyrb_result run_build(const pyrb_exec* e, const Job& job, pyrb_built* out, uint3
 
 }  // namespace
 
+namespace pyrb {
+// The calling thread's error message, for the library's other translation units.
+pyrb_result set_error(pyrb_result r, const char* msg) { return fail(r, "%s", msg); }
+}  // namespace pyrb
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------

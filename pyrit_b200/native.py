@@ -71,6 +71,29 @@ class Tuning(ctypes.Structure):
 PATH_AUTO, PATH_SORT, PATH_GRID = 0, 1, 2
 
 
+class ServerConfig(ctypes.Structure):
+    """pyrb_server_config."""
+    _fields_ = [("pool_log2", ctypes.c_void_p), ("pool_starts", ctypes.c_void_p), ("pool_sizes", ctypes.c_void_p),
+                ("pool_voxels", ctypes.c_uint64), ("pool_count", ctypes.c_uint32), ("rt_log2", ctypes.c_uint32),
+                ("budget_bytes", ctypes.c_uint64), ("max_batch_entries", ctypes.c_uint64),
+                ("max_batch_requests", ctypes.c_uint32), ("max_edits", ctypes.c_uint32),
+                ("max_inflight", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class ServerResult(ctypes.Structure):
+    """pyrb_server_result."""
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("root", ctypes.c_uint32),
+                ("first_voxel", ctypes.c_uint32), ("first_prim", ctypes.c_uint32), ("voxel_count", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("batch", BuiltC), ("latency_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    """pyrb_server_stats."""
+    _fields_ = [(n, ctypes.c_uint64) for n in ("requests", "batches", "failed_batches", "evictions", "voxels",
+                                               "peak_bytes", "arena_used")] + [
+        (n, ctypes.c_uint32) for n in ("max_batch_requests", "pending", "inflight", "reserved")]
+
+
 class PathEditJob(ctypes.Structure):
     """pyrb_path_edit_job (the reference's PathEditJob, src/device/types.zig:613-658)."""
     _fields_ = [(n, ctypes.c_uint32) for n in (
@@ -127,6 +150,13 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_uint64)]),
     "pyrb_last_capacity_need": (ctypes.c_uint32, []),
     "pyrb_selftest_wait_limit": (ctypes.c_int32, [ctypes.POINTER(Exec), _u32]),
+    "pyrb_server_create": (ctypes.c_int32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "pyrb_server_submit": (ctypes.c_int32, [_p, _u64, _u32, _p, _u32]),
+    "pyrb_server_poll": (ctypes.c_uint32, [_p, ctypes.POINTER(ServerResult), _u32]),
+    "pyrb_server_release": (ctypes.c_int32, [_p, _u64]),
+    "pyrb_server_get_stats": (None, [_p, ctypes.POINTER(ServerStats)]),
+    "pyrb_server_drain": (ctypes.c_int32, [_p, _u32]),
+    "pyrb_server_destroy": (None, [_p]),
 }
 
 _lib = None

@@ -3,27 +3,26 @@
 The reference streams a world by building batches of chunks on a worker thread
 (World.gpuWorkImpl, src/world.zig:937-1025), admitting work by its free-VRAM margin
 (World.vramFree, src/world.zig:814-821) and evicting unused chunks from its pools
-(src/world_plan.zig:273-292). This is the same loop for a stream of independent
-chunk-build requests:
+(src/world_plan.zig:273-292). The library's native served loop (pyrb_server_*, C++:
+pyrit_b200/csrc/pyrb_server.cpp) does the same for a stream of independent chunk-build
+requests:
 
-* requests (a pool chunk plus 0..64 overlay edits) arrive over time;
-* whenever fewer than `max_inflight` batches are on the GPU, every pending request
-  (up to `max_batch_voxels`) forms the next batch, which is ONE pyrb_build_batch_async
-  launch sequence on the server's stream -- requests that arrive while others build
-  join the next batch (continuous batching);
-* admission is by memory accounting: all scratch (dedup tables, sort buffers) and all
-  results are sub-allocated from one fixed device arena of `budget_bytes` (first fit
-  with coalescing); a batch is launched only when its estimated need fits into the
-  largest free range, evicting the least recently used results first;
-* latency of a request = device completion time of its batch (CUDA events on the
-  server stream, relative to an event at t=0) minus its arrival time.
+* requests (a pool chunk plus 0..64 overlay edits) are submitted as they arrive;
+* a worker thread keeps up to `max_inflight` batches on the GPU; whenever one completes,
+  the requests that arrived meanwhile (up to `max_batch_voxels` voxels + edits) form the
+  next batch, ONE pyrb_build_batch_async launch sequence on the server's stream --
+  requests that arrive while others build join the next batch (continuous batching);
+* all scratch (dedup tables, grid cells, sort buffers) and all results are sub-allocated
+  from one fixed device arena of `budget_bytes` (first fit with coalescing); a batch is
+  admitted when the build's exact need fits the largest free range, after evicting the
+  least recently completed results;
+* latency of a request = submit -> the worker saw its batch complete (host clock).
 
-The chunk data, the dedup tables, the node/leaf/attribute arena and all per-request
-outputs stay on the device; the host only forms batches and reads counts.
+The chunk data, the dedup tables, the arena and all per-request outputs stay on the
+device; this module only submits requests and collects results.
 """
 from __future__ import annotations
 
-import collections
 import ctypes
 import time
 from dataclasses import dataclass, field
@@ -43,7 +42,7 @@ class Request:
 
 @dataclass
 class RequestResult:
-    batch: int
+    batch: native.BuiltC    # buffers of the batch that built the request (server-owned)
     root: int
     first_voxel: int
     first_prim: int
@@ -84,247 +83,96 @@ class ChunkPool:
         return len(self.log2s)
 
 
-class RangeArena:
-    """First-fit range allocator with coalescing over one fixed device buffer (the
-    reference's pool allocator, src/range_alloc.zig:25-58). Ranges freed while a batch
-    is being enqueued are held back until that batch has completed on the GPU."""
+class _ArenaView:
+    """Peak and current use of the server's device arena (bytes)."""
 
-    ALIGN = 256
+    def __init__(self, server):
+        self._s = server
 
-    def __init__(self, nbytes: int):
-        import torch
-        self.size = nbytes // self.ALIGN * self.ALIGN
-        self.buf = torch.empty(self.size, dtype=torch.uint8, device="cuda")
-        self.base = self.buf.data_ptr()
-        self.free = [(0, self.size)]        # sorted (offset, length)
-        self.live = {}                      # address -> length
-        self.used = 0
-        self.peak = 0
-        self.defer_to = None                # list collecting deferred frees
+    @property
+    def peak(self) -> int:
+        return int(self._s.stats().peak_bytes)
 
-    def alloc(self, nbytes: int) -> int:
-        n = (max(nbytes, 1) + self.ALIGN - 1) // self.ALIGN * self.ALIGN
-        for i, (off, ln) in enumerate(self.free):
-            if ln >= n:
-                if ln == n:
-                    self.free.pop(i)
-                else:
-                    self.free[i] = (off + n, ln - n)
-                addr = self.base + off
-                self.live[addr] = n
-                self.used += n
-                self.peak = max(self.peak, self.used)
-                return addr
-        return 0
-
-    def release(self, addr: int) -> None:
-        n = self.live.pop(addr)
-        self.used -= n
-        off = addr - self.base
-        import bisect
-        i = bisect.bisect_left(self.free, (off, 0))
-        # coalesce with the neighbours
-        if i > 0 and self.free[i - 1][0] + self.free[i - 1][1] == off:
-            i -= 1
-            off, n = self.free[i][0], self.free[i][1] + n
-            self.free.pop(i)
-        if i < len(self.free) and off + n == self.free[i][0]:
-            n += self.free[i][1]
-            self.free.pop(i)
-        self.free.insert(i, (off, n))
-
-    def free_cb(self, addr: int) -> None:
-        if self.defer_to is not None:
-            self.defer_to.append(addr)
-        else:
-            self.release(addr)
-
-    def largest_free(self) -> int:
-        return max((ln for _, ln in self.free), default=0)
-
-
-class _Slot:
-    """Preallocated pinned staging and device buffers of one in-flight batch."""
-
-    def __init__(self, max_chunks, max_edits):
-        import torch
-        K, E = max_chunks, max_edits
-
-        def pin(n, dt):
-            return torch.zeros(n, dtype=dt).pin_memory()
-
-        def dev(n, dt):
-            return torch.zeros(n, dtype=dt, device="cuda")
-
-        self.h_log2, self.d_log2 = pin(K, torch.int32), dev(K, torch.int32)
-        self.h_voff, self.d_voff = pin(K + 1, torch.int32), dev(K + 1, torch.int32)
-        self.h_eoff, self.d_eoff = pin(K + 1, torch.int32), dev(K + 1, torch.int32)
-        self.h_starts, self.d_starts = pin(K, torch.int64), dev(K, torch.int64)
-        self.h_edits, self.d_edits = pin(4 * max(E, 1), torch.int32), dev(4 * max(E, 1), torch.int32)
-        self.roots, self.first, self.fprim = pin(K, torch.int32), pin(K, torch.int32), pin(K, torch.int32)
-        self.counts = pin(native.COUNTS_WORDS, torch.int32)
-        self.log2_np = np.zeros(K, np.uint32)
-
-
-class _Batch:
-    def __init__(self, bid, reqs, built, done, slot, entries, reserve, deferred):
-        self.bid, self.reqs, self.built, self.done, self.slot = bid, reqs, built, done, slot
-        self.entries, self.reserve, self.bytes = entries, reserve, reserve
-        self.deferred = deferred   # scratch ranges to release once the batch is done
+    @property
+    def used(self) -> int:
+        return int(self._s.stats().arena_used)
 
 
 class ChunkServer:
-    # scratch + output bound per entry of a batch build (sort buffers, unique keys and
-    # attributes, bricks, dedup tables, node bound), a safe over-estimate
-    BYTES_PER_ENTRY = 96
-    BYTES_FIXED = 4 << 20
+    """Continuous batching over a device-resident chunk pool, by the library's native
+    served loop (pyrb_server_*: a worker thread, a first-fit device arena of
+    `budget_bytes` for all scratch and results, admission by the build's exact memory
+    need, LRU eviction). This class submits requests at their arrival times, polls the
+    finished results and keeps the statistics."""
 
-    def __init__(self, pool: ChunkPool, budget_bytes: int = 40 << 30, max_batch_voxels: int = 128 << 20,
+    def __init__(self, pool: ChunkPool, budget_bytes: int = 40 << 30, max_batch_voxels: int = 32 << 20,
                  max_inflight: int = 2, rt_log2: int = 5, stream=None, max_batch_requests: int = 1024,
                  max_edits_per_request: int = 64):
-        import torch
         self.pool = pool
-        self.max_batch_requests = max_batch_requests
-        self.max_edits = max_edits_per_request
-        self.free_slots = [_Slot(max_batch_requests, max_batch_requests * max_edits_per_request)
-                           for _ in range(max_inflight)]
-        # all scratch (dedup tables, sort buffers) and every result live in one fixed arena
-        self.arena = RangeArena(budget_bytes)
-        self._alloc_cb = native.ALLOC_FN(lambda ctx, n: self._alloc(n))
-        self._free_cb = native.FREE_FN(lambda ctx, a: self.arena.free_cb(a))
-        self.budget = budget_bytes
-        self.max_batch_voxels = max_batch_voxels
-        self.max_inflight = max_inflight
-        self.rt = rt_log2
-        self.stream = stream or torch.cuda.Stream()
-        self.ex = native.Exec()
-        self.ex.stream = ctypes.c_void_p(self.stream.cuda_stream)
         self.L = native.lib()
-        self.resident = collections.OrderedDict()   # bid -> _Batch (LRU order)
-        self.resident_bytes = 0
+        self.max_edits = max_edits_per_request
+        self._log2 = np.ascontiguousarray(pool.log2s, dtype=np.uint32)
+        self._starts = np.ascontiguousarray(pool.starts, dtype=np.uint64)
+        self._sizes = np.ascontiguousarray(pool.sizes, dtype=np.uint32)
+        cfg = native.ServerConfig(pool_log2=self._log2.ctypes.data, pool_starts=self._starts.ctypes.data,
+                                  pool_sizes=self._sizes.ctypes.data, pool_voxels=pool.voxels.data_ptr(),
+                                  pool_count=len(self._log2), rt_log2=rt_log2, budget_bytes=budget_bytes,
+                                  max_batch_entries=max_batch_voxels, max_batch_requests=max_batch_requests,
+                                  max_edits=max_edits_per_request, max_inflight=max_inflight)
+        h = ctypes.c_void_p()
+        native.check(self.L.pyrb_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.budget = budget_bytes
+        self.arena = _ArenaView(self)
         self.results: dict[int, RequestResult] = {}
         self.requests: dict[int, Request] = {}
         self.keep_results = True
-        self.ex.alloc = self._alloc_cb
-        self.ex.free = self._free_cb
-        self._evictions = 0
+        self._buf = (native.ServerResult * 4096)()
 
-    def _alloc(self, nbytes: int) -> int:
-        a = self.arena.alloc(nbytes)
-        while not a and self.resident:      # make room: evict least recently used results
-            self._evict_one()
-            self._evictions += 1
-            a = self.arena.alloc(nbytes)
-        return a
+    def stats(self) -> native.ServerStats:
+        st = native.ServerStats()
+        self.L.pyrb_server_get_stats(self.h, ctypes.byref(st))
+        return st
 
-    # -- memory accounting ---------------------------------------------------
-    def _used(self, inflight):
-        return self.arena.used
+    def close(self):
+        if self.h:
+            self.L.pyrb_server_destroy(self.h)
+            self.h = None
 
-    def _evict_one(self):
-        bid, b = self.resident.popitem(last=False)
-        self.resident_bytes -= b.bytes
-        saved, self.arena.defer_to = self.arena.defer_to, None   # a finished batch: release at once
+    def __del__(self):
         try:
-            self.L.pyrb_built_free(ctypes.byref(self.ex), ctypes.byref(b.built))
-        finally:
-            self.arena.defer_to = saved
-        for r in b.reqs:
-            self.results.pop(r.rid, None)
-        return b
+            self.close()
+        except Exception:
+            pass
 
     def release_all(self):
-        while self.resident:
-            self._evict_one()
+        for rid in list(self.results):
+            self.L.pyrb_server_release(self.h, rid)
+        self.results.clear()
 
-    # -- one batch -------------------------------------------------------------
-    def _launch(self, bid, reqs):
-        pool = self.pool
-        slot = self.free_slots.pop()
-        K = len(reqs)
-        chunk = np.fromiter((r.chunk for r in reqs), dtype=np.int64, count=K)
-        log2s = slot.log2_np[:K]
-        log2s[:] = pool.log2s[chunk]
-        voff = slot.h_voff.numpy()[:K + 1].view(np.uint32)
-        voff[0] = 0
-        np.cumsum(pool.sizes[chunk], out=voff[1:])
-        slot.h_log2.numpy()[:K] = log2s.view(np.int32)
-        slot.h_starts.numpy()[:K] = pool.starts[chunk].view(np.int64)
-        eoff = slot.h_eoff.numpy()[:K + 1].view(np.uint32)
-        eoff[0] = 0
-        np.cumsum(np.fromiter((len(r.edits) for r in reqs), dtype=np.uint32, count=K), out=eoff[1:])
-        ne = int(eoff[K])
-        if ne:
-            he = slot.h_edits.numpy()[:4 * ne].reshape(ne, 4).view(np.uint32)
-            o = 0
-            for r in reqs:
-                m = len(r.edits)
-                if m:
-                    he[o:o + m] = r.edits
-                    o += m
-        import torch
-        with torch.cuda.stream(self.stream):
-            slot.d_log2[:K].copy_(slot.h_log2[:K], non_blocking=True)
-            slot.d_voff[:K + 1].copy_(slot.h_voff[:K + 1], non_blocking=True)
-            slot.d_eoff[:K + 1].copy_(slot.h_eoff[:K + 1], non_blocking=True)
-            slot.d_starts[:K].copy_(slot.h_starts[:K], non_blocking=True)
-            if ne:
-                slot.d_edits[:4 * ne].copy_(slot.h_edits[:4 * ne], non_blocking=True)
-        bd = native.Batch(count=K, log2_host=log2s.ctypes.data, log2=slot.d_log2.data_ptr(),
-                          voxels=pool.voxels.data_ptr(), voxel_offsets=slot.d_voff.data_ptr(),
-                          edits=slot.d_edits.data_ptr() if ne else 0, edit_offsets=slot.d_eoff.data_ptr() if ne else 0,
-                          voxel_total=int(voff[K]), edit_total=ne, voxel_starts=slot.d_starts.data_ptr())
-        built = native.BuiltC()
-        deferred = []
-        self.arena.defer_to = deferred
-        try:
-            rc = self.L.pyrb_build_batch_async(ctypes.byref(self.ex), ctypes.byref(bd), self.rt,
-                                               slot.roots.data_ptr(), slot.first.data_ptr(),
-                                               slot.fprim.data_ptr(), slot.counts.data_ptr(), ctypes.byref(built))
-        finally:
-            self.arena.defer_to = None
-        if rc != native.PYRB_OK:
-            self.free_slots.append(slot)
-            for a in deferred:       # nothing was enqueued that uses them
-                self.arena.release(a)
-            if rc == native.PYRB_ERROR_OUT_OF_MEMORY:
-                return None
-            native.check(rc)
-        done = torch.cuda.Event(enable_timing=True)
-        done.record(self.stream)
-        entries = int(voff[K]) + ne
-        reserve = self.BYTES_PER_ENTRY * entries + self.BYTES_FIXED
-        return _Batch(bid, reqs, built, done, slot, entries, reserve, deferred)
+    def _submit(self, r: Request):
+        e = np.ascontiguousarray(r.edits, dtype=np.uint32).reshape(-1, 4)
+        native.check(self.L.pyrb_server_submit(self.h, r.rid & 0xFFFFFFFFFFFFFFFF, r.chunk,
+                                               e.ctypes.data if len(e) else None, len(e)))
 
-    def _retire(self, b, t0_event, stats):
-        slot = b.slot
-        native.check(self.L.pyrb_build_finish(ctypes.c_void_p(slot.counts.data_ptr()), ctypes.byref(b.built)))
-        st = native.Stats()
-        self.L.pyrb_last_stats(ctypes.byref(st))
-        b.bytes = int(st.output_bytes)          # scratch is released, the outputs stay resident
-        done_ms = t0_event.elapsed_time(b.done)
-        K = len(b.reqs)
-        roots = slot.roots.numpy()[:K].view(np.uint32).copy()
-        first = slot.first.numpy()[:K].view(np.uint32).copy()
-        fprim = slot.fprim.numpy()[:K].view(np.uint32).copy()
-        arrivals = np.fromiter((r.arrival for r in b.reqs), dtype=np.float64, count=K)
-        lats = done_ms - arrivals * 1e3
-        stats.latencies_ms.extend(lats.tolist())
-        if self.keep_results:
-            for k, r in enumerate(b.reqs):
-                self.results[r.rid] = RequestResult(b.bid, int(roots[k]), int(first[k]), int(fprim[k]), float(lats[k]))
-        stats.voxels += b.built.voxel_count
-        self.free_slots.append(slot)
-        b.slot = None
-        for a in b.deferred:
-            self.arena.release(a)
-        b.deferred = []
-        self.resident[b.bid] = b
-        self.resident_bytes += b.bytes
+    def _collect(self, stats: ServeStats) -> int:
+        k = self.L.pyrb_server_poll(self.h, self._buf, len(self._buf))
+        for j in range(k):
+            res = self._buf[j]
+            rid = int(res.id)
+            rid = rid - (1 << 64) if rid >= 1 << 63 else rid
+            if res.status != native.PYRB_OK:
+                raise native.PyrbError(res.status, f"request {rid} failed")
+            stats.latencies_ms.append(res.latency_ms)
+            if self.keep_results:
+                self.results[rid] = RequestResult(native.BuiltC.from_buffer_copy(res.batch), int(res.root),
+                                                  int(res.first_voxel), int(res.first_prim), float(res.latency_ms))
+            else:
+                self.L.pyrb_server_release(self.h, res.id)
+        return k
 
-    # -- the serving loop ------------------------------------------------------
+    # -- the serving loop: arrivals on the host clock, batching in the library -----
     def serve(self, requests: list[Request], realtime: bool = True) -> ServeStats:
-        import torch
         stats = ServeStats(requests=len(requests))
         too_many = [r.rid for r in requests if len(r.edits) > self.max_edits]
         if too_many:
@@ -332,58 +180,26 @@ class ChunkServer:
         if self.keep_results:
             for r in requests:
                 self.requests[r.rid] = r
+        before = self.stats()
         order = sorted(requests, key=lambda r: r.arrival)
-        pending = collections.deque()
-        inflight = collections.deque()
-        t0_event = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        t0_event.record(self.stream)
+        n, i, done = len(order), 0, 0
         t0 = time.perf_counter()
-        nxt, bid = 0, 0
-        while nxt < len(order) or pending or inflight:
+        while done < n:
             now = (time.perf_counter() - t0) if realtime else float("inf")
-            while nxt < len(order) and order[nxt].arrival <= now:
-                pending.append(order[nxt])
-                nxt += 1
-            while inflight and inflight[0].done.query():
-                self._retire(inflight.popleft(), t0_event, stats)
-            launched = False
-            if pending and len(inflight) < self.max_inflight:
-                reqs, vox = [], 0
-                while pending and len(reqs) < self.max_batch_requests and (
-                        not reqs or vox + int(self.pool.sizes[pending[0].chunk]) <= self.max_batch_voxels):
-                    r = pending.popleft()
-                    reqs.append(r)
-                    vox += int(self.pool.sizes[r.chunk]) + len(r.edits)
-                need = self.BYTES_PER_ENTRY * vox + self.BYTES_FIXED
-                while self.resident and self.arena.largest_free() < need:
-                    self._evict_one()
-                    stats.evictions += 1
-                b = self._launch(bid, reqs) if (self.arena.largest_free() >= need or not inflight) else None
-                if b is not None:
-                    bid += 1
-                    inflight.append(b)
-                    stats.batches += 1
-                    stats.max_batch_requests = max(stats.max_batch_requests, len(reqs))
-                    stats.peak_bytes = max(stats.peak_bytes, self.arena.peak)
-                    launched = True
-                else:
-                    if not inflight:
-                        raise RuntimeError(f"a batch of {vox} voxels does not fit into the {self.budget}-byte arena")
-                    for r in reversed(reqs):
-                        pending.appendleft(r)
-            if not launched and inflight and (not pending or len(inflight) >= self.max_inflight):
-                # nothing to launch: wait for the oldest batch (realtime: poll, new requests may arrive)
-                if realtime:
-                    time.sleep(20e-6)
-                else:
-                    inflight[0].done.synchronize()
-        end = torch.cuda.Event(enable_timing=True)
-        end.record(self.stream)
-        end.synchronize()
-        stats.duration_s = t0_event.elapsed_time(end) / 1e3
-        stats.evictions += self._evictions
-        self._evictions = 0
+            while i < n and order[i].arrival <= now:
+                self._submit(order[i])
+                i += 1
+            k = self._collect(stats)
+            done += k
+            if k == 0 and (i == n or not realtime):
+                time.sleep(20e-6)
+        stats.duration_s = time.perf_counter() - t0
+        after = self.stats()
+        stats.batches = int(after.batches - before.batches)
+        stats.voxels = int(after.voxels - before.voxels)
+        stats.evictions = int(after.evictions - before.evictions)
+        stats.peak_bytes = int(after.peak_bytes)
+        stats.max_batch_requests = int(after.max_batch_requests)
         return stats
 
     # -- access to a served result (tests) -------------------------------------
@@ -391,9 +207,7 @@ class ChunkServer:
         """Host copy of the whole batch buffers holding request `rid` plus its result."""
         from .gpu_build import Built
         res = self.results[rid]
-        b = self.resident[res.batch]
-        torch_stream = self.stream.cuda_stream
-        view = Built(b.built, torch_stream)
+        view = Built(res.batch, None)
         host = view.download()
         view._c = None  # the server owns the buffers
         return res, host
