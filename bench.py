@@ -902,8 +902,8 @@ def run_served(args, emit=True):
         nedits = rng.integers(0, 65, n)
         reqs = [Request(i, int(chunks[i]), wl.chunk_edits(int(log2s[chunks[i]]), int(nedits[i]), 5000 + i),
                         float(arr[i])) for i in range(n)]
-        srv = ChunkServer(pool, budget_bytes=40 << 30, max_batch_voxels=args.max_batch_voxels, max_inflight=2,
-                          rt_log2=5)
+        srv = ChunkServer(pool, budget_bytes=40 << 30, max_batch_voxels=args.max_batch_voxels,
+                          max_inflight=args.max_inflight, rt_log2=5)
         srv.keep_results = False
         # warm-up on a few requests (not timed)
         srv.serve([Request(-1 - i, int(chunks[i]), reqs[i].edits, 0.0) for i in range(4)], realtime=False)
@@ -920,7 +920,7 @@ def run_served(args, emit=True):
                           "higher_is_better": True, "data": "synthetic",
                           "config": {"workload": "Poisson chunk requests from the 1024-chunk mix + 0..64 edits",
                                      "duration_s": args.duration, "budget_gb": 40,
-                                     "max_batch_voxels": args.max_batch_voxels},
+                                     "max_batch_voxels": args.max_batch_voxels, "max_inflight": args.max_inflight},
                           "tuning": tuning, "served": out}), flush=True)
     del vox
     torch.cuda.empty_cache()
@@ -939,6 +939,7 @@ def main():
     ap.add_argument("--rates", type=float, nargs="+", default=[20000.0])
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--max-batch-voxels", type=int, default=32 << 20)
+    ap.add_argument("--max-inflight", type=int, default=2)
     ap.add_argument("--chunks", type=int, default=1024)
     ap.add_argument("--batched-reps", type=int, default=3)
     ap.add_argument("--tune-budget", type=float, default=15.0)
