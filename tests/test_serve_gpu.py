@@ -76,7 +76,7 @@ def test_lru_eviction_under_small_budget():
     from pyrit_b200.serve import ChunkServer
     pool, vox, offs = _pool(6)
     reqs = _requests(pool, 30, seed=3)
-    budget = 30 << 20   # a few batches' results: older ones must be evicted to admit more
+    budget = 16 << 20   # a few batches' results: older ones must be evicted to admit more
     srv = ChunkServer(pool, budget_bytes=budget, max_batch_voxels=150_000, max_inflight=2, rt_log2=5)
     stats = srv.serve(reqs, realtime=False)
     assert stats.evictions > 0
