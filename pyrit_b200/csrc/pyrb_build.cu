@@ -77,6 +77,8 @@ std::atomic<uint32_t> g_path{kPathAuto};
 // per entry (dense volumes: 256^3 noise at 30 % solid has 3.3, terrain chunks 2), and
 // at most kGridMaxCells cells in all (8 B each).
 constexpr uint64_t kGridCellsPerEntry = 4;
+// A node level takes tiles of one item per thread below this many large tiles (2 per SM)
+constexpr uint32_t kSmallLevelTiles = 296;
 constexpr uint64_t kGridMaxCells = uint64_t(1) << 33;
 
 // ---------------------------------------------------------------------------
@@ -244,9 +246,15 @@ uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels,
     uint32_t launches = 0;
     for (const LevelDesc& L : levels) {
         if (L.lv >= lv0) break;
-        launch(k_node_build, L.build_tiles, kBlock, node_build_smem_bytes(L.lv == 2), st, d, L);
+        if (L.build_nb == 1)
+            launch(k_node_build<1>, L.build_tiles, kBlock, node_build_smem_bytes(L.lv == 2, 1), st, d, L);
+        else
+            launch(k_node_build<kNBIT>, L.build_tiles, kBlock, node_build_smem_bytes(L.lv == 2), st, d, L);
         prof.mark("node_build", L.lv);
-        launch(k_node_own, L.own_tiles, kBlock, 0, st, d, L);
+        if (L.own_it == 1)
+            launch(k_node_own<1>, L.own_tiles, kBlock, 0, st, d, L);
+        else
+            launch(k_node_own<kNodeIT>, L.own_tiles, kBlock, 0, st, d, L);
         prof.mark("node_own", L.lv);
         launches += 2;
         if (L.lv + 1 == d.rt_log2) {
@@ -399,6 +407,7 @@ struct Plan {
     bool chunked = false, key64 = false, grid = false;
     uint32_t P[kMaxLevels + 2] = {};
     uint32_t cap[kMaxLevels + 2] = {}, btiles[kMaxLevels + 2] = {}, otiles[kMaxLevels + 2] = {};
+    uint32_t bnb[kMaxLevels + 2] = {}, oit[kMaxLevels + 2] = {};
     uint64_t o_counters = 0, o_hist = 0, o_sort_status = 0, o_uniq_status = 0, o_brick_status = 0,
              o_leafown_status = 0, o_leaf_table = 0, o_regions = 0;
     uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
@@ -577,8 +586,11 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     for (uint32_t lv = 2; lv < log2; ++lv) {
         p.cap[lv] = next_pow2((uint64_t(P[lv]) * 100 + lf - 1) / lf, 1024);
         uint32_t child = lv == 2 ? B : P[lv - 1];
-        p.btiles[lv] = std::max((child + kNodeBuildTile - 1) / kNodeBuildTile, 1u);
-        p.otiles[lv] = std::max((P[lv] + kNodeTile - 1) / kNodeTile, 1u);
+        // levels too small for two waves of large tiles take tiles of one item per thread
+        p.bnb[lv] = child >= kSmallLevelTiles * kNodeBuildTile ? kNBIT : 1;
+        p.oit[lv] = P[lv] >= kSmallLevelTiles * kNodeTile ? kNodeIT : 1;
+        p.btiles[lv] = std::max((child + kBlock * p.bnb[lv] - 1) / (kBlock * p.bnb[lv]), 1u);
+        p.otiles[lv] = std::max((P[lv] + kBlock * p.oit[lv] - 1) / (kBlock * p.oit[lv]), 1u);
         p.o_table[lv] = zl.take(uint64_t(p.cap[lv]) * 16);
         p.o_bstat[lv] = zl.take(uint64_t(p.btiles[lv]) * 8);
         p.o_ostat[lv] = zl.take(uint64_t(p.otiles[lv]) * 8);
@@ -706,6 +718,8 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
         L.parent_bound = p.P[lv];
         L.build_tiles = p.btiles[lv];
         L.own_tiles = p.otiles[lv];
+        L.build_nb = p.bnb[lv];
+        L.own_it = p.oit[lv];
         L.need_box = lv + 1 <= d.rt_log2 ? 1u : 0u;
         L.pcap = p.cap[lv];
         L.tile_ctr_build = 12 + 2 * (lv - 2);

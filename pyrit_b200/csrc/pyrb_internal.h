@@ -158,6 +158,8 @@ struct LevelDesc {
     uint32_t pcap;           // table capacity (power of two)
     uint32_t tile_ctr_build; // counter index of the dynamic tile ids
     uint32_t tile_ctr_own;
+    uint32_t build_nb;       // children per thread of the build kernel (4, or 1 for small levels)
+    uint32_t own_it;         // parents per thread of the owner kernel (8, or 1 for small levels)
     // children
     const uint64_t* ckey;    // lv == 2: brick keys (voxel key >> 6)
     const uint32_t* ccnt;    // lv >  2

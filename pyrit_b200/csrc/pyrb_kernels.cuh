@@ -1037,22 +1037,28 @@ __device__ __forceinline__ uint32_t brick_ref(const BuildDesc& d, uint32_t b) {
 // a halo of up to 7 children of the tile's last parent), heads found with warp
 // ballots, positions by a look-back scan, then every thread builds parents from
 // shared memory.
+// Parents per thread of the node-owner kernel and children per thread of the node
+// build: large levels take 8 and 4 (tiles of 2048 parents / 1024 children), levels
+// small enough to leave most SMs idle with those take 1 (tiles of 256), so that their
+// tiles spread over the whole GPU (plan_build picks per level).
 constexpr int kNodeIT = 8;
-constexpr int kNodeTile = kBlock * kNodeIT;     // tile of the node-owner kernel
+constexpr int kNodeTile = kBlock * kNodeIT;     // tile of the node-owner kernel (large levels)
 constexpr int kNBIT = 4;
-constexpr int kNodeBuildTile = kBlock * kNBIT;  // children per node-build tile
+constexpr int kNodeBuildTile = kBlock * kNBIT;  // children per node-build tile (large levels)
 constexpr int kNodeHalo = 8;
 // Level 2 stages the children's brick masks (its parents' boxes come from them) rather
 // than their boxes: 28 instead of 36 bytes per child, 6 tiles per SM instead of 5.
-constexpr size_t node_build_smem_bytes(bool bricks) {
-    return size_t(kNodeBuildTile + kNodeHalo) * (bricks ? 8 + 8 + 4 + 4 + 4 : 8 + 8 + 8 + 4 + 4 + 4) +
-           size_t(kNodeBuildTile) * 4 + 64;
+constexpr size_t node_build_smem_bytes(bool bricks, int nb = kNBIT) {
+    return size_t(kBlock * nb + kNodeHalo) * (bricks ? 8 + 8 + 4 + 4 + 4 : 8 + 8 + 8 + 4 + 4 + 4) +
+           size_t(kBlock * nb) * 4 + 64;
 }
 
+template <int NB>
 __global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc L) {
     grid_dep_wait();
     extern __shared__ uint64_t smem64[];
-    constexpr int N = kNodeBuildTile + kNodeHalo;
+    constexpr int kTile = kBlock * NB;
+    constexpr int N = kTile + kNodeHalo;
     uint64_t* skey = smem64;
     uint64_t* slo = skey + N;                        // level 2: the brick masks
     uint64_t* shi = L.lv == 2 ? slo : slo + N;
@@ -1068,10 +1074,10 @@ __global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc
     const uint32_t tile = dyn_tile(d.counters, L.tile_ctr_build, &s_tile);
     const uint32_t C = L.lv == 2 ? min(d.counters[kCtrBricks], d.brick_bound)
                                  : min(d.counters[kCtrParents + L.lv - 1], L.child_bound);
-    const uint32_t ntiles = (C + kNodeBuildTile - 1) / kNodeBuildTile;
+    const uint32_t ntiles = (C + kTile - 1) / kTile;
     if (tile >= ntiles) return;
-    const uint32_t t0 = tile * kNodeBuildTile;
-    const uint32_t own_n = min(uint32_t(kNodeBuildTile), C - t0);
+    const uint32_t t0 = tile * kTile;
+    const uint32_t own_n = min(uint32_t(kTile), C - t0);
     const uint32_t tn = min(uint32_t(N), C - t0);
     // stage the children: coalesced loads; references of bricks from the dense
     // leaf-reference array, of nodes by one gather per child from the level's table
@@ -1107,12 +1113,12 @@ __global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc
     }
     if (threadIdx.x == 0) s_prev = t0 > 0 ? L.ckey[t0 - 1] : ~0ull;
     __syncthreads();
-    // heads of this tile's own children (warp chunks of 32 * kNBIT)
-    unsigned hb[kNBIT];
+    // heads of this tile's own children (warp chunks of 32 * NB)
+    unsigned hb[NB];
     uint32_t wc = 0;
 #pragma unroll
-    for (int j = 0; j < kNBIT; ++j) {
-        const uint32_t i = warp * 32 * kNBIT + j * 32 + lane;
+    for (int j = 0; j < NB; ++j) {
+        const uint32_t i = warp * 32 * NB + j * 32 + lane;
         bool head = false;
         if (i < own_n) {
             const uint64_t pk = i == 0 ? s_prev : skey[i - 1];
@@ -1131,8 +1137,8 @@ __global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc
     }
     uint32_t run = wexcl;
 #pragma unroll
-    for (int j = 0; j < kNBIT; ++j) {
-        const uint32_t i = warp * 32 * kNBIT + j * 32 + lane;
+    for (int j = 0; j < NB; ++j) {
+        const uint32_t i = warp * 32 * NB + j * 32 + lane;
         if ((hb[j] >> lane) & 1) shead[run + __popc(hb[j] & lanemask_lt())] = i;
         run += __popc(hb[j]);
     }
@@ -1183,6 +1189,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc
 }
 
 // Owners of level lv get word offsets (scan of their lengths) and write their words.
+template <int NIT>
 __global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
     grid_dep_wait();
     __shared__ uint32_t s_tile;
@@ -1191,14 +1198,15 @@ __global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = dyn_tile(d.counters, L.tile_ctr_own, &s_tile);
     const uint32_t P = min(d.counters[kCtrParents + L.lv], L.parent_bound);
-    const uint32_t ntiles = (P + kNodeTile - 1) / kNodeTile;
+    constexpr uint32_t kTile = kBlock * NIT;
+    const uint32_t ntiles = (P + kTile - 1) / kTile;
     if (tile >= ntiles) return;
     const uint32_t cursor = d.counters[kCtrCursor + L.lv];
-    const uint32_t wstart = tile * kNodeTile + warp * 32 * kNodeIT;
-    uint32_t len[kNodeIT], slot[kNodeIT];
+    const uint32_t wstart = tile * kTile + warp * 32 * NIT;
+    uint32_t len[NIT], slot[NIT];
     uint64_t wsum = 0;  // words | count << 31
 #pragma unroll
-    for (int j = 0; j < kNodeIT; ++j) {
+    for (int j = 0; j < NIT; ++j) {
         uint32_t i = wstart + j * 32 + lane;
         len[j] = 0;
         slot[j] = 0;
@@ -1222,7 +1230,7 @@ __global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
     __syncthreads();
     uint32_t run = uint32_t(s_base & 0x7FFFFFFFu) + uint32_t(wexcl & 0x7FFFFFFFu);
 #pragma unroll
-    for (int j = 0; j < kNodeIT; ++j) {
+    for (int j = 0; j < NIT; ++j) {
         uint32_t i = wstart + j * 32 + lane;
         uint32_t x = len[j];
 #pragma unroll
