@@ -196,12 +196,23 @@ def stage_profile(log2, rt, dpts, sptr, flush, steps):
     return {k: statistics.mean(v) for k, v in stage.items()}
 
 
+def path_name(stage_ms):
+    """How the build ordered its voxels, from its stages."""
+    if "bucket_count" in stage_ms:
+        return "brick buckets"
+    return "cell grid" if "grid_scatter" in stage_ms else "sort"
+
+
 def kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak, cells=0):
     """Algorithmic bytes / CUDA-event time of the build's HBM kernels against `peak`
     (GB/s). Bytes per launch (the roofline basis of the design notes):
       grid_scatter  n_in (16 + 8)                read PyrVoxels, one 8-byte cell update each
       grid_count    8 cells                      read every cell (its 32-byte sector holds 4)
       grid_write    8 cells + 12 n_u + 20 B      read every cell, write keys, attributes, bricks
+      bucket_count  n_in (16 + 4)                read PyrVoxels, add to the brick's counter
+      bucket_scatter n_in (16 + 4 + 9)           read PyrVoxels, take a slot, write the 9-byte record
+      bucket_tile_count  9 n_in + 4 nb           read the records and the bucket bounds (nb bricks)
+      bucket_tile_write  9 n_in + 4 nb + 12 n_u + 20 B
       encode_hist   n_in (16 + kb + 4)           read PyrVoxels, write key + value
       sort_pass     n_in 2 (kb + 4)              read and write key + value
       unique_brick  n_in (kb + 4) + 12 n_u + 20 B
@@ -222,6 +233,11 @@ def kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak, cells=0):
     add("grid_scatter", stage_ms.get("grid_scatter"), n_in * 24)
     add("grid_count", stage_ms.get("grid_count"), 8 * cells)
     add("grid_write", stage_ms.get("grid_write"), 8 * cells + 12 * n_u + 20 * B)
+    nb = cells // 64
+    add("bucket_count", stage_ms.get("bucket_count"), n_in * 20)
+    add("bucket_scatter", stage_ms.get("bucket_scatter"), n_in * 29)
+    add("bucket_tile_count", stage_ms.get("bucket_tile_count"), 9 * n_in + 4 * nb)
+    add("bucket_tile_write", stage_ms.get("bucket_tile_write"), 9 * n_in + 4 * nb + 12 * n_u + 20 * B)
     add("encode_hist", stage_ms.get("encode_hist"), n_in * (16 + key_bytes + 4))
     sort_keys = [k for k in stage_ms if k.startswith("sort_pass")]
     if sort_keys:
@@ -230,14 +246,22 @@ def kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak, cells=0):
     add("leaf_part", stage_ms.get("leaf_part"), 20 * B)
     add("leaf_insert", stage_ms.get("leaf_insert"), 28 * B)
     add("leaf_own", stage_ms.get("leaf_own"), 16 * B + 8 * leaves)
+    def node_bytes(lv):
+        C = B if lv == 2 else int(st.level_parents[lv - 1])
+        P, U = int(st.level_parents[lv]), int(st.level_unique[lv])
+        W = 2 * U + (C * U // P if P else 0)
+        return 20 * C + 28 * P + 4 * W
+
     for lv in range(2, 24):
         nb, no = stage_ms.get("node_build:%d" % lv), stage_ms.get("node_own:%d" % lv)
         if nb is None or no is None:
             continue
-        C = B if lv == 2 else int(st.level_parents[lv - 1])
-        P, U = int(st.level_parents[lv]), int(st.level_unique[lv])
-        W = 2 * U + (C * U // P if P else 0)
-        add("node_dedup:%d" % lv, nb + no, 20 * C + 28 * P + 4 * W)
+        add("node_dedup:%d" % lv, nb + no, node_bytes(lv))
+    # the small levels in one cooperative launch: all of its levels' node bytes
+    for k, ms in stage_ms.items():
+        if k.startswith("levels:"):
+            lv0 = int(k.split(":")[1])
+            add(k, ms, sum(node_bytes(lv) for lv in range(lv0, 24) if st.level_parents[lv]))
     return out
 
 
@@ -381,12 +405,16 @@ def run_ours(args):
     stage_ms = stage_profile(LOG2, RT, dpts, sptr, flush, min(args.steps, 20))
     key_bytes = 4 if 3 * LOG2 + 1 <= 32 else 8
     peak, peak_kind = load_peaks()
-    # the dominant HBM kernel (largest share of the build's stage time; a node level is
-    # two kernels and latency-bound, it is listed but not taken)
+    # the dominant kernel: the largest share of the build's stage time (a per-level
+    # node dedup is a pair of kernels, listed in "kernels" but not a candidate)
     kernels = kernel_roofline(stage_ms, st, n_in, n_u, sizes["leaves"], key_bytes, peak,
                               cells=(1 << (3 * LOG2)) if st.sort_passes == 0 else 0)
     names = {"grid_scatter": "k_grid_scatter", "grid_count": "k_grid_count", "grid_write": "k_grid_write",
-             "sort_pass": "k_sort_pass", "encode_hist": "k_encode_hist", "unique_brick": "k_unique"}
+             "sort_pass": "k_sort_pass", "encode_hist": "k_encode_hist", "unique_brick": "k_unique",
+             "leaf_insert": "k_leaf_insert", "leaf_own": "k_leaf_own", "bucket_count": "k_bkt_count",
+             "bucket_scatter": "k_bkt_scatter", "bucket_tile_count": "k_grid_count<bucket>",
+             "bucket_tile_write": "k_grid_write<bucket>"}
+    names.update({k: "k_levels_coop" for k in kernels if k.startswith("levels:")})
     dom = max((k for k in kernels if k in names), key=lambda k: kernels[k]["share"])
     dom_kernel = names[dom]
     dom_bytes, dom_ms = kernels[dom]["alg_bytes"], kernels[dom]["ms"]
@@ -493,7 +521,7 @@ def run_ours(args):
                        "bricks": st.brick_count, "leaves": sizes["leaves"], "node_words": sizes["node_words"],
                        "prims": sizes["prims"], "sort_passes": st.sort_passes, "radix_bits": st.radix_bits,
                        "l2": "flushed between steps (512 MiB write outside the timed events)",
-                       "key_bits": 8 * key_bytes, "path": "sort" if st.sort_passes else "cell grid",
+                       "key_bits": 8 * key_bytes, "path": path_name(stage_ms),
                        "dedup_per_level": dedup,
                        "scratch_bytes": int(st.scratch_bytes), "output_bytes_bound": int(st.output_bytes),
                        "parallelism": "replicas" if world > 1 else "single"},
@@ -573,7 +601,7 @@ def run_worst_case(args, reps=3):
     paths = {}
     old = gpu_build.get_tuning()
     try:
-        for name, code in (("sort", native.PATH_SORT), ("grid", native.PATH_GRID)):
+        for name, code in (("sort", native.PATH_SORT), ("grid", native.PATH_GRID), ("bucket", native.PATH_BUCKET)):
             gpu_build.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, code)
             L.pyrb_built_free(ctypes.byref(ex), ctypes.byref(build_async()))
             tt = []
@@ -605,7 +633,7 @@ def run_worst_case(args, reps=3):
             "leaves": leaves, "ms_per_build": t, "voxels_per_s": n_u / (t / 1e3),
             "sort_passes": int(st.sort_passes), "radix_bits": int(st.radix_bits),
             "peak_gbs": peak, "peak_kind": peak_kind, "kernels": kernels, "dedup_per_level": dedup,
-            "path": "sort" if st.sort_passes else "cell grid", "paths_forced": paths,
+            "path": path_name(stage_ms), "paths_forced": paths,
             "scratch_plus_output_bytes_per_entry": (st.scratch_bytes + st.output_bytes) / n_in,
             "how": "pyrb_build_async on the resident input, CUDA events around each build (median of %d), "
                    "per-stage events from pyrb_profile_enable" % reps}

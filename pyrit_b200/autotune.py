@@ -1,13 +1,13 @@
 """Autotuner of the build's ordering path, sort and dedup parameters.
 
-Sweeps the way voxels are ordered (the cell grid, or the radix sort with its digit
-width of 4, 8, 9, 10, 11 bits and keys per sort tile of 1024, 2048, 4096, or 8192
-with 8- or 9-bit digits) and the dedup hash-table load factor (50 %, 70 %) on a
+Sweeps the way voxels are ordered (the cell grid, the brick buckets, or the radix sort
+with its digit width of 4, 8, 9, 10, 11 bits and keys per sort tile of 1024, 2048,
+4096, or 8192 with 8- or 9-bit digits) and the dedup hash-table load factor (50 %, 70 %) on a
 caller-supplied workload, times every setting with CUDA events, applies the fastest
 through pyrb_set_tuning and can persist it as JSON. None of the parameters changes
 the output (the build is bit-exact for all of them); they only change speed and
-memory. The grid settings come first (two of them); the sort settings follow while
-the time budget lasts.
+memory. The grid and bucket settings come first (four of them); the sort settings
+follow while the time budget lasts.
 """
 from __future__ import annotations
 
@@ -44,7 +44,7 @@ def sweep(run_once, reps: int = 3, radix_bits=RADIX_BITS, tile_keys=TILE_KEYS, l
                "path": old.path, "ms": None}
         return cur, [cur]
     t_start = time.time()
-    settings = [(0, 0, lf, native.PATH_GRID) for lf in load_factors] + [
+    settings = [(0, 0, lf, path) for path in (native.PATH_GRID, native.PATH_BUCKET) for lf in load_factors] + [
         (rb, tk, lf, native.PATH_SORT) for rb, tk, lf in itertools.product(radix_bits, tile_keys, load_factors)
         if supported(rb, tk)]
     try:

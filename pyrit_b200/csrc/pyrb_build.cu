@@ -19,6 +19,7 @@
 #include "pyrb_internal.h"
 #include "pyrb_kernels.cuh"
 #include "pyrb_grid.cuh"
+#include "pyrb_bucket.cuh"
 #include "pyrb_pathedit.cuh"
 
 using namespace pyrb;
@@ -71,7 +72,7 @@ std::atomic<uint32_t> g_radix_bits{0};  // 0 with g_tile_keys 0: chosen per buil
 std::atomic<uint32_t> g_tile_keys{0};
 std::atomic<uint32_t> g_load_pct{50};
 // Sort or cell grid for the voxels of a build (pyrb_tuning.path)
-constexpr uint32_t kPathAuto = 0, kPathSort = 1, kPathGrid = 2;
+constexpr uint32_t kPathAuto = 0, kPathSort = 1, kPathGrid = 2, kPathBucket = 3;
 std::atomic<uint32_t> g_path{kPathAuto};
 // The grid path is taken automatically while the chunks hold at most this many cells
 // per entry (dense volumes: 256^3 noise at 30 % solid has 3.3, terrain chunks 2), and
@@ -80,6 +81,9 @@ constexpr uint64_t kGridCellsPerEntry = 4;
 // A node level takes tiles of one item per thread below this many large tiles (2 per SM)
 constexpr uint32_t kSmallLevelTiles = 296;
 constexpr uint64_t kGridMaxCells = uint64_t(1) << 33;
+// Sparser builds take the brick buckets while their brick counters (4 B per brick
+// position) stay well inside the L2: up to 2^24 bricks (64 MB, a 1024^3 volume).
+constexpr uint64_t kBucketMaxBricks = uint64_t(1) << 24;
 
 // ---------------------------------------------------------------------------
 // memory: caller callbacks, else a library-owned stream-ordered pool per device
@@ -429,7 +433,7 @@ void auto_tuning(uint32_t sort_bits, uint32_t* rb, uint32_t* tile_keys) {
 struct Plan {
     BuildDesc d;
     uint32_t K = 1, rb = 8, it = 16, lf = 50, passes = 1, min_log2 = 3, rt = 3, n = 0, nmax = 1, B = 1;
-    bool chunked = false, key64 = false, grid = false;
+    bool chunked = false, key64 = false, grid = false, bucket = false;
     uint32_t P[kMaxLevels + 2] = {};
     uint32_t cap[kMaxLevels + 2] = {}, btiles[kMaxLevels + 2] = {}, otiles[kMaxLevels + 2] = {};
     uint32_t bnb[kMaxLevels + 2] = {}, oit[kMaxLevels + 2] = {};
@@ -439,6 +443,7 @@ struct Plan {
     uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
     uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bslot = 0, o_bref = 0;
     uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0, o_chunk_vstart = 0;
+    uint64_t o_bcount = 0, o_brec = 0, o_bloc = 0, o_bsum = 0;
     uint64_t o_set[2][7] = {};
     uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
     // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
@@ -516,8 +521,10 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     for (uint32_t l = 3; l <= log2 && !p.key64; ++l) grid_cells += per_log2[l] << (3 * l);
     if (!p.key64 && grid_cells <= kGridMaxCells)
         p.grid = path == kPathGrid || (path == kPathAuto && grid_cells <= kGridCellsPerEntry * nmax);
-    if (p.grid) tile_keys = 4096;  // the scatter's tiles over the entries
-    p.rb = p.grid ? 0 : rb;
+    if (!p.key64 && !p.grid && (grid_cells >> 6) <= kBucketMaxBricks)
+        p.bucket = path == kPathBucket || path == kPathAuto;
+    if (p.grid || p.bucket) tile_keys = 4096;  // the scatter's tiles over the entries
+    p.rb = (p.grid || p.bucket) ? 0 : rb;
     p.it = tile_keys / kBlock;
     p.lf = lf;
 
@@ -538,9 +545,9 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
 
     // digit plan over lb + 1 bits (the invalid bit on top); none for the grid
     const uint32_t sort_bits = lb + 1;
-    const uint32_t passes = p.passes = p.grid ? 0 : (sort_bits + rb - 1) / rb;
+    const uint32_t passes = p.passes = (p.grid || p.bucket) ? 0 : (sort_bits + rb - 1) / rb;
     d.passes = passes;
-    d.radix = p.grid ? 0 : 1u << rb;
+    d.radix = passes ? 1u << rb : 0;
     if (passes) {
         uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 0;
         for (uint32_t q = 0; q < passes; ++q) {
@@ -589,16 +596,19 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     while ((d.leaf_cap >> d.leaf_region_shift) > d.leaf_regions) ++d.leaf_region_shift;
     d.node_bound = uint32_t(words);
     d.prim_bound = P[rt - 1];
-    if (p.grid) {
-        d.use_grid = 1;
+    if (p.grid || p.bucket) {
+        d.use_grid = p.grid ? 1u : 0u;
+        d.use_bucket = p.bucket ? 1u : 0u;
         d.grid_cells = grid_cells;
         d.grid_tiles = uint32_t(std::max<uint64_t>((grid_cells + 64 * kGridTileBricks - 1) / (64 * kGridTileBricks), 1));
+        d.bucket_scan_tiles = uint32_t(std::max<uint64_t>(((grid_cells >> 6) + kBucketScanTile - 1) / kBucketScanTile, 1));
     }
 
     // ---- scratch layout
     Layout zl;  // zero-initialised region
     p.o_counters = zl.take(kCtrCount * 4);
-    if (!p.grid) {
+    if (p.bucket) p.o_bcount = zl.take((grid_cells >> 6) * 4);
+    if (!p.grid && !p.bucket) {
         p.o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
         p.o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
         p.o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
@@ -634,7 +644,12 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     p.o_seg_entry = ol.take(uint64_t(K + 1) * 4);
     p.o_seg_tile = ol.take(uint64_t(K + 1) * 4);
     const uint64_t kbytes = p.key64 ? 8 : 4;
-    if (!p.grid) {
+    if (p.bucket) {
+        p.o_brec = ol.take(uint64_t(nmax) * 8);
+        p.o_bloc = ol.take(uint64_t(nmax));
+        p.o_bsum = ol.take(uint64_t(d.bucket_scan_tiles) * 8);
+    }
+    if (!p.grid && !p.bucket) {
         p.o_k0 = ol.take(uint64_t(nmax) * kbytes);
         p.o_v0 = ol.take(uint64_t(nmax) * 4);
         p.o_k1 = ol.take(uint64_t(nmax) * kbytes);
@@ -700,13 +715,24 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     // the sort buffers (or the cell grid) are dead once the unique voxels are out: N x
     // (kb + 4) bytes from k0 hold the B region-grouped masks, k1 their brick indices
     // (in the grid: 8 B per cell, at least 512 B per brick)
-    if (p.grid) {
-        d.grid = static_cast<uint64_t*>(at(p.o_grid));
+    if (p.grid || p.bucket) {
         d.grid_off = static_cast<uint64_t*>(at(p.o_grid_off));
         d.grid_count = static_cast<uint64_t*>(at(p.o_grid_count));
         d.chunk_vstart = static_cast<uint32_t*>(at(p.o_chunk_vstart));
+    }
+    if (p.grid) {
+        d.grid = static_cast<uint64_t*>(at(p.o_grid));
         d.pmask = d.grid;
         d.pidx = reinterpret_cast<uint32_t*>(d.grid + p.B);
+    } else if (p.bucket) {
+        d.bcount = static_cast<uint32_t*>(at(p.o_bcount));
+        d.brec = static_cast<uint64_t*>(at(p.o_brec));
+        d.bloc = static_cast<uint8_t*>(at(p.o_bloc));
+        d.bsum = static_cast<uint64_t*>(at(p.o_bsum));
+        // dead once the bricks are out: the records hold the region-grouped masks (8 B
+        // per entry >= per brick), the counters their brick indices (4 B per brick position)
+        d.pmask = d.brec;
+        d.pidx = d.bcount;
     } else {
         d.pmask = static_cast<uint64_t*>(at(p.o_k0));
         d.pidx = static_cast<uint32_t*>(at(p.o_k1));
@@ -716,7 +742,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     d.prim_start = static_cast<uint32_t*>(at(p.o_prim_start));
     d.seg_entry = static_cast<uint32_t*>(at(p.o_seg_entry));
     d.seg_tile = static_cast<uint32_t*>(at(p.o_seg_tile));
-    if (!p.grid) {
+    if (!p.grid && !p.bucket) {
         d.kbuf[0] = at(p.o_k0);
         d.vbuf[0] = static_cast<uint32_t*>(at(p.o_v0));
         d.kbuf[1] = at(p.o_k1);
@@ -795,14 +821,35 @@ uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaSt
     ++launches;
     prof.mark("plan");
     if ((*err = cudaGetLastError()) != cudaSuccess) return 0;
-    if (p.grid) {
+    if (p.bucket) {
+        launch(k_bkt_count, d.sort_tiles, kBlock, 0, st, d);
+        prof.mark("bucket_count");
+        launch(k_bkt_scan_tiles, d.bucket_scan_tiles, kBlock, 0, st, d);
+        launch(k_bkt_scan_top, 1, kGridScanThreads, 0, st, d);
+        launch(k_bkt_scan_apply, d.bucket_scan_tiles, kBlock, 0, st, d);
+        prof.mark("bucket_scan");
+        launch(k_bkt_scatter, d.sort_tiles, kBlock, 0, st, d);
+        prof.mark("bucket_scatter");
+        launch(k_grid_count<true>, d.grid_tiles, kBlock, 0, st, d);
+        prof.mark("bucket_tile_count");
+        launch(k_grid_scan, 1, kGridScanThreads, 0, st, d);
+        prof.mark("grid_scan");
+        launch(k_grid_write<true>, d.grid_tiles, kBlock, 0, st, d);
+        prof.mark("bucket_tile_write");
+        launches += 8;
+        if (d.chunked) {
+            launch(k_grid_chunks, std::max(std::min((p.K + kBlock - 1) / kBlock, 1024u), 1u), kBlock, 0, st, d);
+            prof.mark("grid_chunks");
+            ++launches;
+        }
+    } else if (p.grid) {
         launch(k_grid_scatter, d.sort_tiles, kBlock, 0, st, d);
         prof.mark("grid_scatter");
-        launch(k_grid_count, d.grid_tiles, kBlock, 0, st, d);
+        launch(k_grid_count<false>, d.grid_tiles, kBlock, 0, st, d);
         prof.mark("grid_count");
         launch(k_grid_scan, 1, kGridScanThreads, 0, st, d);
         prof.mark("grid_scan");
-        launch(k_grid_write, d.grid_tiles, kBlock, 0, st, d);
+        launch(k_grid_write<false>, d.grid_tiles, kBlock, 0, st, d);
         prof.mark("grid_write");
         launches += 4;
         if (d.chunked) {
@@ -1173,7 +1220,8 @@ PYRB_API pyrb_result pyrb_set_tuning(const pyrb_tuning* t) {
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "8192-key tiles take 8- or 9-bit digits");
     if (t->load_factor_pct < 25 || t->load_factor_pct > 90)
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "load_factor_pct must lie in [25, 90]");
-    if (t->path > kPathGrid) return fail(PYRB_ERROR_INVALID_ARGUMENT, "path must be 0 (automatic), 1 (sort) or 2 (grid)");
+    if (t->path > kPathBucket)
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "path must be 0 (automatic), 1 (sort), 2 (grid) or 3 (bucket)");
     g_radix_bits = t->radix_bits;
     g_tile_keys = t->tile_keys;
     g_load_pct = t->load_factor_pct;

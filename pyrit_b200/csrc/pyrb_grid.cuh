@@ -39,19 +39,16 @@ __device__ __forceinline__ void red_max_u64(uint64_t* p, uint64_t v) {
     asm volatile("red.relaxed.gpu.global.max.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Entries -> cells. Tiles follow the per-segment tiling of the sort path (tile_span),
-// so the entry index (the order that decides) and the chunk are those of the sort.
-// PyrVoxel segments (every mode but old keys and downsampling) take the fast loop:
-// the chunk's voxel and edit lists are resolved once per tile, and each thread keeps
-// kScatterBatch 16-byte loads in flight before it encodes and updates their cells.
+// Every entry of a tile with a valid key, in the per-segment tiling of the sort path
+// (tile_span), so the entry index (the order that decides) and the chunk are those of
+// the sort: f(entry index, local key, value). PyrVoxel segments (every mode but old
+// keys and downsampling) take the fast loop: the chunk's voxel and edit lists are
+// resolved once per tile, and each thread keeps kScatterBatch 16-byte loads in flight
+// before it encodes them.
 constexpr int kScatterBatch = 4;
-__global__ void __launch_bounds__(kBlock) k_grid_scatter(BuildDesc d) {
-    grid_dep_wait();
-    const uint32_t tile = blockIdx.x;
-    if (tile >= d.seg_tile[d.seg_count]) return;
-    const TileSpan sp = tile_span(d, tile);
+template <typename F>
+__device__ __forceinline__ void for_tile_entries(const BuildDesc& d, const TileSpan& sp, F&& f) {
     const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg);
-    uint64_t* cells = d.grid + __ldg(d.grid_off + sp.seg);
     const uint32_t inv = 1u << d.lb;
     // the segment's entries: src[0, nv) then esrc[0, ...)
     const uint4* src = nullptr;
@@ -92,7 +89,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_scatter(BuildDesc d) {
             const uint32_t e = sp.start + idx;
             uint32_t key = 0, val = 0;
             load_raw(d, sp.seg, e - seg_begin, key, val);
-            if (!(key & inv)) red_max_u64(cells + key, (uint64_t(e + 1) << 32) | val);
+            if (!(key & inv)) f(e, key, val);
         }
         return;
     }
@@ -115,10 +112,21 @@ __global__ void __launch_bounds__(kBlock) k_grid_scatter(BuildDesc d) {
             const uint32_t idx = base + k * kBlock + threadIdx.x;
             uint32_t key, val;
             encode_voxel(v[k], log2c, d.lb, key, val);
-            if (idx < sp.count && !(key & inv))
-                red_max_u64(cells + key, (uint64_t(sp.start + idx + 1) << 32) | val);
+            if (idx < sp.count && !(key & inv)) f(sp.start + idx, key, val);
         }
     }
+}
+
+// Entries -> cells: an atomic max of (entry index + 1) << 32 | value.
+__global__ void __launch_bounds__(kBlock) k_grid_scatter(BuildDesc d) {
+    grid_dep_wait();
+    const uint32_t tile = blockIdx.x;
+    if (tile >= d.seg_tile[d.seg_count]) return;
+    const TileSpan sp = tile_span(d, tile);
+    uint64_t* cells = d.grid + __ldg(d.grid_off + sp.seg);
+    for_tile_entries(d, sp, [&](uint32_t e, uint32_t key, uint32_t val) {
+        red_max_u64(cells + key, (uint64_t(e + 1) << 32) | val);
+    });
 }
 
 // Chunk holding cell `cell` (grid_off non-decreasing, grid_off[0] = 0 <= cell).
@@ -146,8 +154,43 @@ __device__ __forceinline__ void grid_load_attrs(const BuildDesc& d, uint64_t wb0
     }
 }
 
+// The attribute words of a warp's bricks from the brick buckets (sparse builds): the
+// warp rebuilds its bricks' 64 cells each in shared memory (the same atomic max of
+// (entry index + 1) << 32 | value as the global grid) and reads them back.
+__device__ __forceinline__ void bucket_load_attrs(const BuildDesc& d, uint64_t wb0, uint64_t nbricks, uint64_t* cells,
+                                                  uint32_t* a0, uint32_t* a1) {
+    const unsigned lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < kGridWarpBricks * 64 / 32; ++i) cells[i * 32 + lane] = 0;
+    // bucket boundaries: lane k < 9 holds the start of brick k (lane 8: the end of brick 7)
+    uint32_t c = 0;
+    if (lane <= uint32_t(kGridWarpBricks)) {
+        const uint64_t b = min(wb0 + lane, nbricks);
+        c = b == 0 ? 0u : __ldcg(d.bcount + b - 1);
+    }
+    uint32_t bound[kGridWarpBricks + 1];
+#pragma unroll
+    for (int k = 0; k <= kGridWarpBricks; ++k) bound[k] = __shfl_sync(kFull, c, k);
+    __syncwarp();
+    for (uint32_t j = bound[0] + lane; j < bound[kGridWarpBricks]; j += 32) {
+        uint32_t k = 0;
+#pragma unroll
+        for (int q = 1; q < kGridWarpBricks; ++q) k += j >= bound[q] ? 1u : 0u;
+        atomicMax(reinterpret_cast<unsigned long long*>(cells + k * 64 + __ldcs(d.bloc + j)),
+                  (unsigned long long)__ldcs(d.brec + j));
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < kGridWarpBricks; ++k) {
+        a0[k] = uint32_t(cells[k * 64 + lane]);
+        a1[k] = uint32_t(cells[k * 64 + 32 + lane]);
+    }
+}
+
 // Pass 1 of the compaction: voxels and non-empty bricks of every tile, packed
 // (voxels | bricks << 32) into grid_count[tile]. No dependency between tiles.
+// kBucket: the cells come from the brick buckets (sparse builds), else from the grid.
+template <bool kBucket>
 __global__ void __launch_bounds__(kBlock) k_grid_count(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint64_t s_sum[kWarps];
@@ -156,7 +199,12 @@ __global__ void __launch_bounds__(kBlock) k_grid_count(BuildDesc d) {
     const uint64_t nbricks = d.grid_cells >> 6;
     const uint64_t wb0 = uint64_t(tile) * kGridTileBricks + uint64_t(warp) * kGridWarpBricks;
     uint32_t a0[kGridWarpBricks], a1[kGridWarpBricks];
-    grid_load_attrs(d, wb0, nbricks, a0, a1);
+    if constexpr (kBucket) {
+        __shared__ uint64_t s_cells[kGridTileBricks * 64];
+        bucket_load_attrs(d, wb0, nbricks, s_cells + warp * kGridWarpBricks * 64, a0, a1);
+    } else {
+        grid_load_attrs(d, wb0, nbricks, a0, a1);
+    }
     uint32_t vox = 0, bricks = 0;
 #pragma unroll
     for (int k = 0; k < kGridWarpBricks; ++k) {
@@ -174,24 +222,24 @@ __global__ void __launch_bounds__(kBlock) k_grid_count(BuildDesc d) {
     }
 }
 
-// Pass 2: exclusive scan of the tile counts in place (one block, chunks of 8 per
+// Pass 2: exclusive scan of the tile counts in place (one block, chunks of 16 per
 // thread); the totals are the build's voxel and brick counts.
 constexpr int kGridScanThreads = 1024, kGridScanPer = 16;
-__global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
-    grid_dep_wait();
+// Exclusive scan of a[0, T) in place by one block of kGridScanThreads; returns the
+// total (valid in every thread).
+__device__ __forceinline__ uint64_t block_scan_inplace(uint64_t* a, uint32_t T) {
     __shared__ uint64_t s_w[kGridScanThreads / 32];
     __shared__ uint64_t s_carry;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = kGridScanThreads / 32;
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
-    const uint32_t T = d.grid_tiles;
     for (uint32_t base = 0; base < T; base += kGridScanThreads * kGridScanPer) {
         const uint32_t i0 = base + threadIdx.x * kGridScanPer;
         uint64_t v[kGridScanPer], sum = 0;
 #pragma unroll
         for (int j = 0; j < kGridScanPer; ++j) {
-            v[j] = i0 + j < T ? d.grid_count[i0 + j] : 0;
+            v[j] = i0 + j < T ? a[i0 + j] : 0;
             sum += v[j];
         }
         uint64_t x = sum;
@@ -216,16 +264,22 @@ __global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
         uint64_t run = s_carry + s_w[warp] + x - sum;
 #pragma unroll
         for (int j = 0; j < kGridScanPer; ++j) {
-            if (i0 + j < T) d.grid_count[i0 + j] = run;
+            if (i0 + j < T) a[i0 + j] = run;
             run += v[j];
         }
         __syncthreads();
         if (threadIdx.x == kGridScanThreads - 1) s_carry = run;
         __syncthreads();
     }
+    return s_carry;
+}
+
+__global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
+    grid_dep_wait();
+    const uint64_t total = block_scan_inplace(d.grid_count, d.grid_tiles);
     if (threadIdx.x == 0) {
-        d.counters[kCtrUnique] = uint32_t(s_carry);
-        d.counters[kCtrBricks] = uint32_t(s_carry >> 32);
+        d.counters[kCtrUnique] = uint32_t(total);
+        d.counters[kCtrBricks] = uint32_t(total >> 32);
     }
 }
 
@@ -233,6 +287,7 @@ __global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
 // unique keys and attributes, brick records, first voxel of every chunk.
 // 5 tiles per SM (48 registers): the tiles write as soon as their loads arrive, so
 // more of them in flight keep more loads outstanding
+template <bool kBucket>
 __global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint64_t s_sum[kWarps];
@@ -244,7 +299,12 @@ __global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     const uint64_t nbricks = d.grid_cells >> 6;
     const uint64_t wb0 = uint64_t(tile) * kGridTileBricks + uint64_t(warp) * kGridWarpBricks;
     uint32_t a0[kGridWarpBricks], a1[kGridWarpBricks];
-    grid_load_attrs(d, wb0, nbricks, a0, a1);
+    if constexpr (kBucket) {
+        __shared__ uint64_t s_cells[kGridTileBricks * 64];
+        bucket_load_attrs(d, wb0, nbricks, s_cells + warp * kGridWarpBricks * 64, a0, a1);
+    } else {
+        grid_load_attrs(d, wb0, nbricks, a0, a1);
+    }
     uint32_t vox = 0, bricks = 0;
 #pragma unroll
     for (int k = 0; k < kGridWarpBricks; ++k) {

@@ -146,6 +146,16 @@ struct BuildDesc {
     uint64_t* grid_off;      // [K + 1] first cell of every chunk (k_plan)
     uint64_t* grid_count;    // [grid_tiles] voxels | bricks << 32 per tile, then their exclusive scan
     uint32_t* chunk_vstart;  // [K] voxels before the first cell of every chunk (chunk builds)
+
+    // Brick buckets of a sparse build (use_bucket): the entries of every brick position
+    // gathered together (a counting pass, a scan, a scatter), each tile of 64 bricks
+    // then rebuilt as a cell grid in shared memory for the grid path's compaction.
+    uint32_t use_bucket;
+    uint32_t bucket_scan_tiles;  // tiles of kBucketScanTile counters
+    uint32_t* bcount;        // [bricks] entries per brick position, then the end of its bucket
+    uint64_t* brec;          // [n_total] (input index + 1) << 32 | value, bucket by bucket
+    uint8_t* bloc;           // [n_total] the entry's cell in its brick (key & 63)
+    uint64_t* bsum;          // [bucket_scan_tiles] counter sums, then their exclusive scan
 };
 
 // One node level: children (bricks at level 2) -> parents of edge 2^(lv+1).

@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
             d.seg_entry[c] = s_carry[0] + s_scan[0][threadIdx.x] - size;
             d.seg_tile[c] = s_carry[1] + s_scan[1][threadIdx.x] - tiles;
         }
-        if (d.use_grid) {
+        if (d.use_grid | d.use_bucket) {
             // first cell of every chunk in the cell grid (chunk after chunk)
             const uint32_t l = c < K ? (d.mode == kModeBatch ? __ldg(d.chunk_log2 + c) : d.log2) : 0;
             const uint64_t cells = c < K ? uint64_t(1) << (3 * l) : 0;
@@ -114,14 +114,14 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
         if (threadIdx.x == 0) {
             s_carry[0] += s_scan[0][1023];
             s_carry[1] += s_scan[1][1023];
-            if (d.use_grid) s_cell_carry += s_cells[1023];
+            if (d.use_grid | d.use_bucket) s_cell_carry += s_cells[1023];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         d.seg_entry[K] = s_carry[0];
         d.seg_tile[K] = s_carry[1];
-        if (d.use_grid) d.grid_off[K] = s_cell_carry;
+        if (d.use_grid | d.use_bucket) d.grid_off[K] = s_cell_carry;
     }
 }
 

@@ -331,8 +331,8 @@ def last_stats() -> native.Stats:
 
 def set_tuning(radix_bits: int = 0, tile_keys: int = 0, load_factor_pct: int = 50, path: int = 0) -> None:
     """Digit width and keys per sort tile (0 and 0: chosen per build, the default), the
-    dedup table load factor and the path (0 automatic, 1 sort, 2 cell grid), for builds
-    started afterwards."""
+    dedup table load factor and the path (0 automatic, 1 sort, 2 cell grid, 3 brick
+    buckets), for builds started afterwards."""
     t = native.Tuning(radix_bits=radix_bits, tile_keys=tile_keys, load_factor_pct=load_factor_pct, path=path)
     native.check(native.lib().pyrb_set_tuning(ctypes.byref(t)))
 

@@ -68,7 +68,7 @@ class Tuning(ctypes.Structure):
                 ("load_factor_pct", ctypes.c_uint32), ("path", ctypes.c_uint32)]
 
 
-PATH_AUTO, PATH_SORT, PATH_GRID = 0, 1, 2
+PATH_AUTO, PATH_SORT, PATH_GRID, PATH_BUCKET = 0, 1, 2, 3
 
 
 class ServerConfig(ctypes.Structure):

@@ -115,7 +115,7 @@ def test_mixed_batch_with_large_sort_tiles(radix_bits):
 CONFIG2_LOG2S = [8, 5, 6, 7, 5, 5, 6, 8, 5, 7, 6, 5, 5, 6, 5, 7, 5, 6, 5, 5, 6, 5, 5, 6, 5]
 
 
-@pytest.mark.parametrize("path", ["sort", "grid"])
+@pytest.mark.parametrize("path", ["sort", "grid", "bucket"])
 @pytest.mark.parametrize("with_edits", [False, True])
 def test_config2_mix_at_full_chunk_sizes(with_edits, path):
     from pyrit_b200 import gpu_build, native
@@ -123,7 +123,8 @@ def test_config2_mix_at_full_chunk_sizes(with_edits, path):
     assert log2s.count(8) == 2 and log2s.count(7) == 3 and len(log2s) == 25
     chunks = [wl.mix_chunk(200 + i, l, 0) for i, l in enumerate(log2s)]
     edits = [wl.chunk_edits(l, 64, 300 + i) for i, l in enumerate(log2s)] if with_edits else None
-    gpu_build.set_tuning(0, 0, 50, native.PATH_SORT if path == "sort" else native.PATH_GRID)
+    gpu_build.set_tuning(0, 0, 50, {"sort": native.PATH_SORT, "grid": native.PATH_GRID,
+                                    "bucket": native.PATH_BUCKET}[path])
     try:
         _check(log2s, chunks, edits, rt=5)
     finally:

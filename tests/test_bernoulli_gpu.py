@@ -14,12 +14,13 @@ from gpu_helpers import assert_same_build, dev
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=["sort", "grid"])
+@pytest.fixture(params=["sort", "grid", "bucket"])
 def path(request):
-    """The sparse worst case on both paths: the radix sort (the automatic choice at 6.6
-    cells per entry) and the cell grid forced."""
+    """The sparse worst case on every path: the brick buckets (the automatic choice at
+    6.6 cells per entry), the radix sort and the cell grid forced."""
     from pyrit_b200 import gpu_build, native
-    gpu_build.set_tuning(0, 0, 50, native.PATH_SORT if request.param == "sort" else native.PATH_GRID)
+    gpu_build.set_tuning(0, 0, 50, {"sort": native.PATH_SORT, "grid": native.PATH_GRID,
+                                    "bucket": native.PATH_BUCKET}[request.param])
     yield request.param
     gpu_build.set_tuning(0, 0, 50, native.PATH_AUTO)
 

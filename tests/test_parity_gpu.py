@@ -13,14 +13,15 @@ from gpu_helpers import assert_same_build, dev
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=["sort", "grid"])
+@pytest.fixture(scope="module", params=["sort", "grid", "bucket"])
 def gb(request):
-    """Every test of this module runs twice: voxels ordered by the radix sort, and by the
-    cell grid (where the edge allows it); the output must not depend on the path."""
+    """Every test of this module runs three times: voxels ordered by the radix sort, by
+    the cell grid and by the brick buckets (the last two where the edge allows them);
+    the output must not depend on the path."""
     import torch
     assert torch.cuda.is_available(), "GPU tests need a CUDA device"
     from pyrit_b200 import gpu_build, native
-    path = native.PATH_SORT if request.param == "sort" else native.PATH_GRID
+    path = {"sort": native.PATH_SORT, "grid": native.PATH_GRID, "bucket": native.PATH_BUCKET}[request.param]
     gpu_build.set_tuning(0, 0, 50, path)
     yield gpu_build
     gpu_build.set_tuning(0, 0, 50, native.PATH_AUTO)
