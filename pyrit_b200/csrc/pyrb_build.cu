@@ -233,40 +233,20 @@ uint32_t leaf_insert_grid(const BuildDesc& d) {
     return std::max(std::min((d.brick_bound + kBlock - 1) / kBlock, 148u * 8u), 1u);
 }
 
-// First level built by the cooperative kernel of the small levels (children bound <=
-// kCoopMaxChildren from there on); log2 means none (the top level is too wide, e.g.
-// many chunks).
-constexpr uint32_t kCoopMaxChildren = 300000;
+// First level built by the single-CTA tail kernel (children bound <= kTailMaxChildren
+// from there on); log2 means no tail (the top level is too wide, e.g. many chunks).
 uint32_t tail_level(uint32_t log2, uint32_t B, const uint32_t* P) {
     for (uint32_t lv = 2; lv < log2; ++lv) {
         const uint32_t child = lv == 2 ? B : P[lv - 1];
-        if (child <= kCoopMaxChildren) return lv;
+        if (child <= kTailMaxChildren) return lv;
     }
     return log2;
 }
 
-// Blocks of the cooperative level kernel: two per SM (all resident at once: the
-// occupancy of the kernel allows more), computed once per device.
-uint32_t coop_blocks() {
-    static std::mutex mu;
-    static int cached[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return 1;
-    std::lock_guard<std::mutex> lk(mu);
-    if (!cached[dev]) {
-        int sms = 0, per_sm = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_levels_coop, kBlock, node_build_smem_bytes(false, 1));
-        cached[dev] = std::max(1, sms * std::min(per_sm, 2));
-    }
-    return uint32_t(cached[dev]);
-}
-
-// Node levels, prims and the final counts. Levels below lv0 run as per-level
-// kernels; the rest (and the finalisation) in the cooperative kernel k_levels_coop.
-uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels, uint32_t lv0, cudaStream_t st,
-                       Prof& prof) {
+// Node levels, prims and the final counts. Levels below lv0 run as multi-CTA
+// kernels; the rest (and the finalisation) in k_tail.
+uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels, uint32_t lv0, const TailDesc& T,
+                       cudaStream_t st, Prof& prof) {
     uint32_t launches = 0;
     for (const LevelDesc& L : levels) {
         if (L.lv >= lv0) break;
@@ -288,36 +268,31 @@ uint32_t launch_levels(const BuildDesc& d, const std::vector<LevelDesc>& levels,
         }
     }
     if (lv0 < d.log2) {
-        // the small levels: one cooperative launch over the SMs (no programmatic
-        // serialisation: it starts once the previous kernel has finished)
-        LevelsDesc S;
-        std::memset(&S, 0, sizeof(S));
-        S.lv0 = lv0;
-        uint32_t tiles = 1;
-        for (const LevelDesc& L : levels) {
-            if (L.lv < lv0) continue;
-            S.lv[S.nlev++] = L;
-            tiles = std::max({tiles, L.build_tiles, L.own_tiles});
-        }
-        const uint32_t grid = std::min(tiles, coop_blocks());
-        const size_t smem = node_build_smem_bytes(false, 1);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3(kBlock);
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, k_levels_coop, d, S);
-        prof.mark("levels", lv0);
+        static std::once_flag once;
+        std::call_once(once, [] {
+            cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tail_smem_bytes()));
+        });
+        launch(k_tail, 1, kTailThreads, tail_smem_bytes(), st, d, T);
+        prof.mark("tail", lv0);
     } else {
         launch(k_finalize, 1, kBlock, 0, st, d, levels.back());
         prof.mark("finalize");
     }
     return launches + 1;
+}
+
+TailDesc make_tail(uint32_t lv0, const uint32_t* P, const std::vector<LevelDesc>& levels, const uint4* leaf_table) {
+    TailDesc T;
+    std::memset(&T, 0, sizeof(T));
+    T.lv0 = lv0;
+    for (int i = 0; i < kMaxLevels + 2; ++i) T.parent_bound[i] = P[i];
+    for (const LevelDesc& L : levels) {
+        const int ps = (L.lv - 2) & 1;
+        T.set[ps] = RecordSet{L.pkey, L.pcnt, L.pfirst, L.pslot, L.plo, L.phi, L.pwords};
+        if (L.lv + 1 == lv0) T.ctable0 = L.ptable;
+    }
+    if (lv0 == 2) T.ctable0 = leaf_table;
+    return T;
 }
 
 thread_local uint32_t g_capacity_need = 0;
@@ -876,7 +851,7 @@ uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaSt
     prof.mark("leaf_own");
     launches += 2;
     const uint32_t lv0 = tail_level(d.log2, B, p.P);
-    launches += launch_levels(d, levels, lv0, st, prof);
+    launches += launch_levels(d, levels, lv0, make_tail(lv0, p.P, levels, d.leaf_table), st, prof);
     if (d.mode == kModeBatch && p.min_log2 < d.log2) {
         launch(k_batch_roots, std::max(std::min((p.K + 255) / 256, 1024u), 1u), 256, 0, st, d, d.log2);
         prof.mark("batch_roots");

@@ -24,7 +24,6 @@ constexpr int kCtrCursor = 8;      // + lv: first node word of level lv (lv = 2.
 constexpr int kCtrParents = 36;    // + lv: P_lv
 constexpr int kCtrUniqueLv = 64;   // + lv: U_lv
 constexpr int kCtrTiles = 96;      // dynamic tile counters, one per launch
-constexpr int kCtrBarrier = 156;   // grid barrier of the cooperative level kernel: arrivals, generation
 constexpr int kCtrCount = 160;
 constexpr uint32_t kMaxLeafRegions = 64;
 #ifndef PYRB_LEAF_REGION_LOG
@@ -196,12 +195,30 @@ struct LevelDesc {
 constexpr uint32_t kNodeStride = 10;
 constexpr uint32_t kNoRef = 0xFFFFFFFFu;
 
-// The small levels, from lv0 to the top, built by one cooperative kernel.
-struct LevelsDesc {
-    uint32_t lv0;
-    uint32_t nlev;
-    LevelDesc lv[kMaxLevels];   // lv[k] is level lv0 + k
+// The upper levels, once a level has at most kTailMaxChildren children, are built by
+// one CTA (k_tail) that keeps each level's dedup table in shared memory.
+constexpr uint32_t kTailThreads = 1024;
+constexpr uint32_t kTailMaxChildren = 4096;
+constexpr uint32_t kTailSlots = 8192;
+
+// One record set of parents (levels alternate between two sets).
+struct RecordSet {
+    uint64_t* key;
+    uint32_t* cnt;
+    uint32_t* first;
+    uint32_t* slot;    // k_tail: node word offset of the parent (its reference)
+    uint64_t* lo;
+    uint64_t* hi;
+    uint32_t* words;   // [bound][kNodeStride]
 };
+
+struct TailDesc {
+    uint32_t lv0;                    // first level built by the tail (children <= kTailMaxChildren)
+    uint32_t parent_bound[kMaxLevels + 2];
+    RecordSet set[2];                // parents of level lv live in set[(lv - 2) & 1]
+    const uint4* ctable0;            // references of lv0's children: leaf table (lv0 == 2) or level lv0-1 table
+};
+
 
 
 }  // namespace pyrb

@@ -1330,6 +1330,257 @@ __global__ void __launch_bounds__(kBlock) k_prims(BuildDesc d, LevelDesc L) {
     prims_range(d, L, blockIdx.x * kBlock + threadIdx.x, gridDim.x * kBlock);
 }
 
+// ---------------------------------------------------------------------------
+// Upper levels in one CTA. Each level: stage the children in shared memory, find
+// heads (block scan), build the parents' words into global memory, dedup them in a
+// shared-memory table (owner = minimum parent index), give the owners word offsets
+// (block scan of their lengths), write their words, and turn every parent's slot
+// into its node offset, which the next level uses as the child reference. Prims
+// (level rt_log2 - 1), roots and the final counts are written here as well.
+// Same output as k_node_build/k_node_own/k_prims/k_finalize per level.
+// ---------------------------------------------------------------------------
+constexpr size_t tail_smem_bytes() {
+    return size_t(kTailMaxChildren) * (8 + 4 + 4) + size_t(kTailSlots) * (4 + 4 + 4) + size_t(kTailMaxChildren) * (4 + 4) +
+           64 * 8;
+}
+
+__device__ __forceinline__ uint32_t tail_scan(uint32_t v, uint32_t* sm, uint32_t* total) {
+    // exclusive scan over kTailThreads threads (32 warps)
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= unsigned(o)) x += y;
+    }
+    if (lane == 31) sm[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = sm[lane], s = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(kFull, s, o);
+            if (lane >= unsigned(o)) s += y;
+        }
+        sm[32 + lane] = s - w;
+        if (lane == 31) sm[64] = s;
+    }
+    __syncthreads();
+    uint32_t r = sm[32 + warp] + x - v;
+    *total = sm[64];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) {
+    grid_dep_wait();
+    extern __shared__ uint64_t tsm64[];
+    uint64_t* skey = tsm64;                                            // children keys
+    uint32_t* sref = reinterpret_cast<uint32_t*>(skey + kTailMaxChildren);
+    uint32_t* scnt = sref + kTailMaxChildren;
+    uint32_t* tkey = scnt + kTailMaxChildren;                          // table: parent index + 1
+    uint32_t* towner = tkey + kTailSlots;                              // table: minimum parent index
+    uint32_t* tval = towner + kTailSlots;                              // table: node offset
+    uint32_t* pslot = tval + kTailSlots;                               // parent -> slot
+    uint32_t* plen = pslot + kTailMaxChildren;                         // parent -> words (owners) / 0
+    uint32_t* scan = plen + kTailMaxChildren;                          // 65 words
+    __shared__ uint32_t s_cursor, s_children;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lv0 = T.lv0;
+    if (tid == 0) {
+        s_cursor = d.counters[kCtrCursor + lv0];
+        s_children = lv0 == 2 ? min(d.counters[kCtrBricks], d.brick_bound)
+                              : min(d.counters[kCtrParents + lv0 - 1], T.parent_bound[lv0 - 1]);
+    }
+    for (uint32_t i = tid; i < kTailSlots; i += kTailThreads) { tkey[i] = 0; towner[i] = 0xFFFFFFFFu; }
+    __syncthreads();
+    const uint32_t local_shift = 3 * (d.log2 - d.rt_log2);
+    for (uint32_t lv = lv0; lv < d.log2; ++lv) {
+        const uint32_t C = min(s_children, kTailMaxChildren);
+        const RecordSet& ps = T.set[(lv - 2) & 1];
+        const RecordSet& cs = T.set[(lv - 3) & 1];
+        const bool box = lv + 1 <= d.rt_log2;
+        const uint32_t child_size = 1u << lv;
+        // 1. stage children
+        for (uint32_t i = tid; i < C; i += kTailThreads) {
+            if (lv == 2) {
+                skey[i] = d.bkey[i];
+                sref[i] = brick_ref(d, i);
+                scnt[i] = __popcll(d.bmask[i]);
+            } else {
+                skey[i] = cs.key[i];
+                sref[i] = lv == lv0 ? __ldcg(&T.ctable0[cs.slot[i]].w) : cs.slot[i];
+                scnt[i] = cs.cnt[i];
+            }
+        }
+        __syncthreads();
+        // 2. heads (4 consecutive children per thread) and parent indices
+        constexpr uint32_t PER = kTailMaxChildren / kTailThreads;
+        uint32_t hmask = 0, hc = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t i = tid * PER + k;
+            if (i < C && (i == 0 || (skey[i] >> 3) != (skey[i - 1] >> 3))) { hmask |= 1u << k; ++hc; }
+        }
+        uint32_t P;
+        uint32_t pbase = tail_scan(hc, scan, &P);
+        // 3. build parents (records and words in global memory)
+        uint32_t par = pbase;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            if (!((hmask >> k) & 1)) continue;
+            const uint32_t i = tid * PER + k;
+            const uint64_t pkey = skey[i] >> 3;
+            uint32_t mask = 0, count = 0, n = 0;
+            uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
+            uint32_t* pw = ps.words + uint64_t(par) * kNodeStride;
+            for (uint32_t j = i; j < C && n < 8; ++j) {
+                const uint64_t ck = skey[j];
+                if ((ck >> 3) != pkey) break;
+                const uint32_t idx = uint32_t(ck & 7);
+                mask |= 1u << idx;
+                count = sat_add(count, scnt[j]);
+                pw[2 + n] = sref[j];
+                if (box) {
+                    uint64_t clo, chi;
+                    if (lv == 2) brick_box(d.bmask[j], clo, chi);
+                    else { clo = cs.lo[j]; chi = cs.hi[j]; }
+                    const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
+                                   oz = (idx >> 2) * child_size;
+                    lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
+                    lo[1] = min(lo[1], cell_y(clo) + oy); hi[1] = max(hi[1], cell_y(chi) + oy);
+                    lo[2] = min(lo[2], cell_z(clo) + oz); hi[2] = max(hi[2], cell_z(chi) + oz);
+                }
+                ++n;
+            }
+            pw[0] = mask;
+            pw[1] = count;
+            ps.key[par] = pkey;
+            ps.cnt[par] = count;
+            ps.first[par] = lv == 2 ? d.bfirst[i] : cs.first[i];
+            if (box) {
+                ps.lo[par] = pack_cell(lo[0], lo[1], lo[2]);
+                ps.hi[par] = pack_cell(hi[0], hi[1], hi[2]);
+            }
+            plen[par] = 2 + n;
+            ++par;
+        }
+        __syncthreads();  // all words written (visible to the block)
+        // 4. dedup in the shared-memory table (owner = minimum parent index)
+        for (uint32_t q = tid; q < P; q += kTailThreads) {
+            const uint32_t* w = ps.words + uint64_t(q) * kNodeStride;
+            const uint32_t len = plen[q];
+            uint64_t h64 = len;
+            for (uint32_t k = 0; k < len; ++k) h64 = mix64(h64 ^ w[k]);
+            uint32_t h = uint32_t(h64) & (kTailSlots - 1);
+            uint32_t probes = 0;
+            for (; probes < kTailSlots; ++probes, h = (h + 1) & (kTailSlots - 1)) {
+                uint32_t cur = atomicCAS(tkey + h, 0u, q + 1);
+                if (cur == 0) break;
+                const uint32_t o = cur - 1;
+                if (plen[o] != len) continue;
+                const uint32_t* ow = ps.words + uint64_t(o) * kNodeStride;
+                bool same = true;
+                for (uint32_t k = 0; k < len && same; ++k) same = ow[k] == w[k];
+                if (same) break;
+            }
+            if (probes == kTailSlots) atomicOr(d.counters + kCtrError, kErrTable);
+            pslot[q] = h;
+            atomicMin(towner + h, q);
+        }
+        __syncthreads();
+        // 5. owners: word offsets in parent order, write words, slot value = offset
+        uint32_t wl = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t q = tid * PER + k;
+            if (q < P && towner[pslot[q]] == q) wl += plen[q];
+        }
+        uint32_t words;
+        uint32_t off = tail_scan(wl, scan, &words) + s_cursor;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t q = tid * PER + k;
+            if (q < P && towner[pslot[q]] == q) {
+                const uint32_t* w = ps.words + uint64_t(q) * kNodeStride;
+                if (uint64_t(off) + plen[q] <= d.node_bound) {
+                    for (uint32_t m = 0; m < plen[q]; ++m) d.nodes[off + m] = w[m];
+                } else {
+                    atomicOr(d.counters + kCtrError, kErrBound);
+                }
+                tval[pslot[q]] = off;
+                off += plen[q];
+            }
+        }
+        uint32_t owners = 0;
+        for (uint32_t q = tid; q < P; q += kTailThreads) owners += towner[pslot[q]] == q;
+        uint32_t utotal;
+        tail_scan(owners, scan, &utotal);  // includes a barrier: tval complete
+        // 6. references for the next level, prims, roots
+        for (uint32_t q = tid; q < P; q += kTailThreads) {
+            const uint32_t node = tval[pslot[q]];
+            ps.slot[q] = node;
+            if (lv + 1 == d.rt_log2 && q < d.prim_bound) {
+                const uint64_t full = ps.key[q];
+                const uint64_t key = full & ((1ull << local_shift) - 1);
+                const uint32_t chunk = uint32_t(full >> local_shift);
+                const uint32_t cx = compact3(key), cy = compact3(key >> 1), cz = compact3(key >> 2);
+                const uint32_t first = d.chunked ? d.chunk_first[chunk] : 0;
+                const uint32_t size = 1u << d.rt_log2;
+                uint4 rec;
+                rec.x = node;
+                rec.y = ps.first[q] - first;
+                const uint64_t pc = pack_cell(cx, cy, cz);
+                rec.z = uint32_t(pc);
+                rec.w = uint32_t(pc >> 32);
+                reinterpret_cast<uint4*>(d.prims)[q] = rec;
+                const uint64_t plo = ps.lo[q], phi = ps.hi[q];
+                const float eps = 1.0f / 256.0f;
+                float* b = d.aabbs + uint64_t(q) * 6;
+                b[0] = __fsub_rn(__fadd_rn(float(cx * size), float(cell_x(plo))), eps);
+                b[1] = __fsub_rn(__fadd_rn(float(cy * size), float(cell_y(plo))), eps);
+                b[2] = __fsub_rn(__fadd_rn(float(cz * size), float(cell_z(plo))), eps);
+                b[3] = __fadd_rn(__fadd_rn(float(cx * size), float(cell_x(phi))), eps);
+                b[4] = __fadd_rn(__fadd_rn(float(cy * size), float(cell_y(phi))), eps);
+                b[5] = __fadd_rn(__fadd_rn(float(cz * size), float(cell_z(phi))), eps);
+                if (d.chunked && (q == 0 || (ps.key[q - 1] >> local_shift) != chunk)) d.prim_start[chunk] = q;
+            }
+            if (lv + 1 == d.log2 && d.chunked) {
+                const uint32_t chunk = uint32_t(ps.key[q]);
+                if (chunk < d.seg_count) d.roots[chunk] = node;
+            }
+        }
+        // clear the table for the next level
+        for (uint32_t i = tid; i < kTailSlots; i += kTailThreads) { tkey[i] = 0; towner[i] = 0xFFFFFFFFu; }
+        if (tid == 0) {
+            d.counters[kCtrParents + lv] = P;
+            d.counters[kCtrUniqueLv + lv] = utotal;
+            s_cursor += words;
+            d.counters[kCtrCursor + lv + 1] = s_cursor;
+            s_children = P;
+            if (lv + 1 == d.rt_log2) d.counters[kCtrPrims] = P;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        // final counts and the empty geometry (gbuild.zig:607-624)
+        const uint32_t top_set = (d.log2 - 1 - 2) & 1;
+        uint32_t cursor = s_cursor;
+        uint32_t root = s_children > 0 ? T.set[top_set].slot[0] : 0;
+        if (d.counters[kCtrUnique] == 0) {
+            if (cursor + 2 <= d.node_bound) {
+                d.nodes[cursor] = 0;
+                d.nodes[cursor + 1] = 0;
+            }
+            root = cursor;
+            cursor += 2;
+            d.counters[kCtrPrims] = 0;
+        }
+        d.counters[kCtrRoot] = root;
+        d.counters[kCtrWords] = cursor;
+    }
+}
+
 // Mixed batch: chunk c of edge 2^log2[c] < 2^top_log2 sits in the low corner of its
 // cell, so above its own top level it hangs below single-child nodes (child index
 // 0). Its root is found by descending from the cell's top node.
@@ -1373,61 +1624,6 @@ __device__ __forceinline__ void finalize_top(const BuildDesc& d, const LevelDesc
 __global__ void __launch_bounds__(kBlock) k_finalize(BuildDesc d, LevelDesc top) {
     grid_dep_wait();
     finalize_top(d, top);
-}
-
-// ---------------------------------------------------------------------------
-// The small levels in one cooperative kernel. Levels whose children fit a few tiles
-// per SM spend their time in launch gaps and look-back chains, not in bandwidth: one
-// launch over all SMs runs every such level (build tiles, barrier, owner tiles,
-// barrier, prims) and the finalisation, the phases separated by grid barriers. The
-// launch is cooperative (all blocks resident), every block takes its tiles in
-// increasing order (so each look-back ends), and every barrier wait is bounded.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void grid_barrier(const BuildDesc& d) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t* bar = d.counters + kCtrBarrier;
-        const uint32_t gen = ld_acquire32(bar + 1);
-        __threadfence();
-        if (atomicAdd(bar, 1u) + 1 == gridDim.x) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            uint32_t spins = 0;
-            while (ld_acquire32(bar + 1) == gen) {
-                if (++spins > kSpinLimit) { atomicOr(d.counters + kCtrError, kErrSpin); break; }
-                if (spins > 8) __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(kBlock) k_levels_coop(BuildDesc d, LevelsDesc S) {
-    for (uint32_t k = 0; k < S.nlev; ++k) {
-        const LevelDesc& L = S.lv[k];
-        for (uint32_t t = blockIdx.x; t < L.build_tiles; t += gridDim.x) {
-            node_build_tile<1>(d, L, t);
-            __syncthreads();  // the next tile reuses the shared memory
-        }
-        grid_barrier(d);
-        for (uint32_t t = blockIdx.x; t < L.own_tiles; t += gridDim.x) {
-            node_own_tile<1>(d, L, t);
-            __syncthreads();
-        }
-        if (blockIdx.x == 0 && threadIdx.x == 0 && d.counters[kCtrParents + L.lv] == 0) {
-            // an empty level passes the word cursor on
-            d.counters[kCtrCursor + L.lv + 1] = d.counters[kCtrCursor + L.lv];
-            d.counters[kCtrUniqueLv + L.lv] = 0;
-        }
-        grid_barrier(d);
-        // prims read this level's records and table; the next level writes the other
-        // record set, and the level after it comes two barriers later
-        if (L.lv + 1 == d.rt_log2) prims_range(d, L, blockIdx.x * kBlock + threadIdx.x, gridDim.x * kBlock);
-    }
-    if (blockIdx.x == 0) finalize_top(d, S.lv[S.nlev - 1]);
 }
 
 // Diagnostics: one bounded wait that nothing ends. Tile 1 looks back at tile 0,
