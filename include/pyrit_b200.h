@@ -212,11 +212,11 @@ PYRB_API const char* pyrb_result_string(pyrb_result r);
  * chosen per build, 9 bits on 8192 entries where that takes one radix pass less than
  * 8 bits, else 8 bits on 4096; hash load factor in percent, 25..90) and of the way the
  * voxels are ordered (path: 0 automatic, the default -- for edges up to 2^10, a cell
- * grid in device memory for dense chunks with at most 4 cells per entry, brick buckets
- * (a counting sort on the brick number, then a per-brick cell grid in shared memory)
- * for sparser builds of at most 2^24 brick positions, else the radix sort; 1 always the
- * sort; 2 the grid and 3 the buckets wherever the edge allows them). The output never
- * depends on any of them. Applies to builds started afterwards on any thread. Returns
+ * grid in device memory for dense chunks with at most 4 cells per entry, else the radix
+ * sort; 1 always the sort; 2 the grid wherever the edge allows it; 3 brick buckets, a
+ * counting sort on the brick number followed by a per-brick cell grid in shared memory,
+ * for edges up to 2^10 and at most 2^24 brick positions). The output never depends on
+ * any of them. Applies to builds started afterwards on any thread. Returns
  * PYRB_ERROR_INVALID_ARGUMENT for unsupported values. */
 typedef struct pyrb_tuning {
     uint32_t radix_bits;

@@ -81,8 +81,12 @@ constexpr uint64_t kGridCellsPerEntry = 4;
 // A node level takes tiles of one item per thread below this many large tiles (2 per SM)
 constexpr uint32_t kSmallLevelTiles = 296;
 constexpr uint64_t kGridMaxCells = uint64_t(1) << 33;
-// Sparser builds take the brick buckets while their brick counters (4 B per brick
-// position) stay well inside the L2: up to 2^24 bricks (64 MB, a 1024^3 volume).
+// The brick buckets (pyrb_tuning.path = 3) need their brick counters (4 B per brick
+// position) well inside the L2: up to 2^24 bricks (64 MB, a 1024^3 volume). They are
+// not chosen automatically: on the 1024^3 Bernoulli(0.15) worst case they measured
+// 11.35 ms per build against 8.73 ms for the sort (their scatter's returning atomics
+// and the mostly empty 64-cell bricks of the compaction cost more than the sort
+// passes they replace).
 constexpr uint64_t kBucketMaxBricks = uint64_t(1) << 24;
 
 // ---------------------------------------------------------------------------
@@ -497,7 +501,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     if (!p.key64 && grid_cells <= kGridMaxCells)
         p.grid = path == kPathGrid || (path == kPathAuto && grid_cells <= kGridCellsPerEntry * nmax);
     if (!p.key64 && !p.grid && (grid_cells >> 6) <= kBucketMaxBricks)
-        p.bucket = path == kPathBucket || path == kPathAuto;
+        p.bucket = path == kPathBucket;
     if (p.grid || p.bucket) tile_keys = 4096;  // the scatter's tiles over the entries
     p.rb = (p.grid || p.bucket) ? 0 : rb;
     p.it = tile_keys / kBlock;

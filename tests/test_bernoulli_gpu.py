@@ -16,8 +16,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(params=["sort", "grid", "bucket"])
 def path(request):
-    """The sparse worst case on every path: the brick buckets (the automatic choice at
-    6.6 cells per entry), the radix sort and the cell grid forced."""
+    """The sparse worst case on every path: the radix sort (the automatic choice at 6.6
+    cells per entry), the cell grid and the brick buckets forced."""
     from pyrit_b200 import gpu_build, native
     gpu_build.set_tuning(0, 0, 50, {"sort": native.PATH_SORT, "grid": native.PATH_GRID,
                                     "bucket": native.PATH_BUCKET}[request.param])
