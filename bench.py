@@ -257,11 +257,6 @@ def kernel_roofline(stage_ms, st, n_in, n_u, leaves, key_bytes, peak, cells=0):
         if nb is None or no is None:
             continue
         add("node_dedup:%d" % lv, nb + no, node_bytes(lv))
-    # the small levels in one cooperative launch: all of its levels' node bytes
-    for k, ms in stage_ms.items():
-        if k.startswith("levels:"):
-            lv0 = int(k.split(":")[1])
-            add(k, ms, sum(node_bytes(lv) for lv in range(lv0, 24) if st.level_parents[lv]))
     return out
 
 
@@ -414,7 +409,6 @@ def run_ours(args):
              "leaf_insert": "k_leaf_insert", "leaf_own": "k_leaf_own", "bucket_count": "k_bkt_count",
              "bucket_scatter": "k_bkt_scatter", "bucket_tile_count": "k_grid_count<bucket>",
              "bucket_tile_write": "k_grid_write<bucket>"}
-    names.update({k: "k_levels_coop" for k in kernels if k.startswith("levels:")})
     dom = max((k for k in kernels if k in names), key=lambda k: kernels[k]["share"])
     dom_kernel = names[dom]
     dom_bytes, dom_ms = kernels[dom]["alg_bytes"], kernels[dom]["ms"]

@@ -1053,8 +1053,7 @@ constexpr size_t node_build_smem_bytes(bool bricks, int nb = kNBIT) {
            size_t(kBlock * nb) * 4 + 64;
 }
 
-// One tile of the node build (shared by k_node_build and the cooperative kernel of
-// the small levels, which takes its tiles in a loop).
+// One tile of the node build (k_node_build takes one per block).
 template <int NB>
 __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelDesc& L, const uint32_t tile) {
     extern __shared__ uint64_t smem64[];
@@ -1196,7 +1195,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc
 }
 
 // Owners of level lv get word offsets (scan of their lengths) and write their words.
-// One tile of the node owners (shared by k_node_own and the cooperative kernel).
+// One tile of the node owners (k_node_own takes one per block).
 template <int NIT>
 __device__ __forceinline__ void node_own_tile(const BuildDesc& d, const LevelDesc& L, const uint32_t tile) {
     __shared__ uint64_t s_scan[2 * kWarps + 2];
@@ -1250,7 +1249,7 @@ __device__ __forceinline__ void node_own_tile(const BuildDesc& d, const LevelDes
             uint32_t w[kNodeStride];
 #pragma unroll
             for (int k = 0; k < int(kNodeStride) / 2; ++k) {
-                uint2 v = __ldcg(src + k);  // in the cooperative kernel: written by its build phase
+                uint2 v = __ldcg(src + k);  // written by the build kernel just before: bypass L1
                 w[2 * k] = v.x;
                 w[2 * k + 1] = v.y;
             }
@@ -1291,7 +1290,7 @@ __global__ void k_level_cursor(BuildDesc d, uint32_t lv) {
 // offset, attribute rank relative to the chunk, cell, AABB base + lo - 1/256 and
 // base + hi + 1/256 in f32 (adds in the reference's order, no FMA possible).
 // ---------------------------------------------------------------------------
-// Prims of threads t0, t0 + stride, ... (shared by k_prims and the cooperative kernel).
+// Prims of threads t0, t0 + stride, ... (k_prims: every thread of its grid).
 __device__ __forceinline__ void prims_range(const BuildDesc& d, const LevelDesc& L, uint32_t t0, uint32_t stride) {
     const uint32_t P = min(d.counters[kCtrParents + L.lv], L.parent_bound);
     const uint32_t local_shift = 3 * (d.log2 - d.rt_log2);
