@@ -424,6 +424,7 @@ struct Plan {
     uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0, o_chunk_vstart = 0;
     uint64_t o_bcount = 0, o_brec = 0, o_bloc = 0, o_bsum = 0;
     uint64_t o_set[2][7] = {};
+    uint64_t o_cwords = 0;
     uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
     // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
     uint64_t out_size[6] = {};
@@ -655,6 +656,12 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_set[s][5] = ol.take(m * 8);                 // hi
         p.o_set[s][6] = ol.take(m * kNodeStride * 4);   // words
     }
+    // words of the small levels' parents at their first child's index (one buffer,
+    // levels run one after another)
+    uint64_t cw = 0;
+    for (uint32_t lv = 2; lv < log2; ++lv)
+        if (p.bnb[lv] == 1) cw = std::max<uint64_t>(cw, lv == 2 ? B : P[lv - 1]);
+    p.o_cwords = ol.take(std::max<uint64_t>(cw, 1) * kNodeStride * 4);
     p.scratch_bytes = align_up(ol.size, 256);
     const uint64_t prims = std::max(d.prim_bound, 1u);
     const uint64_t outs[6] = {uint64_t(d.node_bound) * 4, uint64_t(B) * 8, uint64_t(nmax) * 8, uint64_t(nmax) * 4,
@@ -762,6 +769,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
         L.plo = static_cast<uint64_t*>(at(p.o_set[ps][4]));
         L.phi = static_cast<uint64_t*>(at(p.o_set[ps][5]));
         L.pwords = static_cast<uint32_t*>(at(p.o_set[ps][6]));
+        L.cwords = static_cast<uint32_t*>(at(p.o_cwords));
         L.ptable = static_cast<uint4*>(at(p.o_table[lv]));
         L.build_status = static_cast<uint64_t*>(at(p.o_bstat[lv]));
         L.own_status = static_cast<uint64_t*>(at(p.o_ostat[lv]));

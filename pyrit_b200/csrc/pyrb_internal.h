@@ -187,7 +187,9 @@ struct LevelDesc {
     uint64_t* plo;
     uint64_t* phi;
     uint32_t* pwords;        // [parent_bound][10]
-    uint4* ptable;           // {index + 1, -, ~owner, node offset}
+    uint32_t* cwords;        // build_nb == 1: [child_bound][10], words at the first child's index
+                             // (the table key of these levels: the first child's index + 1)
+    uint4* ptable;           // {key + 1, -, ~owner, node offset}; key: parent index, or first child index
     uint64_t* build_status;
     uint64_t* own_status;
 };

@@ -986,25 +986,26 @@ __device__ __forceinline__ uint64_t node_hash(uint32_t mask, uint32_t count, con
     return h;
 }
 
-// Insert parent `par` (words already stored and fenced) into the level table.
-// refs point to shared memory. Returns the slot; the minimum index owns it.
-__device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, const uint32_t* all_words, uint32_t par,
-                                                uint32_t mask, uint32_t count, const uint32_t* refs, uint32_t n,
-                                                uint32_t* err) {
-    uint32_t h = uint32_t(node_hash(mask, count, refs, n)) & (cap - 1);
+// Insert parent `par` into the level table. Its words are at key_words[key * stride]
+// (stored before this call: the CAS releases them); colliding residents are compared
+// by their words at key_words[(resident key) * stride]. h is the home slot, refs point
+// to shared memory. Returns the slot; the minimum parent index owns it.
+__device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, const uint32_t* key_words, uint32_t key,
+                                                uint32_t par, uint32_t h, uint32_t mask, uint32_t count,
+                                                const uint32_t* refs, uint32_t n, uint32_t* err) {
     for (uint32_t probe = 0; probe < cap; ++probe) {
         uint32_t* kp = &table[h].x;
         uint32_t cur = ld_acquire32(kp);
         if (cur == 0) {
             // release: our words (stored before this call) are visible with the key
-            cur = cas_acq_rel32(kp, 0u, par + 1);
+            cur = cas_acq_rel32(kp, 0u, key + 1);
             if (cur == 0) {
                 atomicMax(&table[h].z, ~par);  // first of its words: claim without waiting
                 return h;
             }
         }
         // acquired above: the resident's words are visible
-        const uint32_t* ow = all_words + uint64_t(cur - 1) * kNodeStride;
+        const uint32_t* ow = key_words + uint64_t(cur - 1) * kNodeStride;
         uint32_t o[kNodeStride];
 #pragma unroll
         for (int k = 0; k < int(kNodeStride); k += 2) {
@@ -1026,6 +1027,8 @@ __device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, cons
     return 0;
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Leaf index of brick b: its own (it owns its mask) or its mask's owner's, found
 // through the table's owner word (only bricks that repeat a mask take this gather).
 __device__ __forceinline__ uint32_t brick_ref(const BuildDesc& d, uint32_t b) {
@@ -1033,14 +1036,74 @@ __device__ __forceinline__ uint32_t brick_ref(const BuildDesc& d, uint32_t b) {
     return r != kNoRef ? r : __ldcg(d.bref + ~__ldcg(&d.leaf_table[__ldcg(d.bslot + b)].z));
 }
 
-// Tile of the node build: kNodeBuildTile children staged in shared memory (plus
-// a halo of up to 7 children of the tile's last parent), heads found with warp
-// ballots, positions by a look-back scan, then every thread builds parents from
-// shared memory.
+// Assembles the parent whose first child is staged at i: mask, saturating count,
+// number of children, box (when needed; at level 2 from the brick masks).
+struct NodeParent {
+    uint32_t mask, count, n;
+    uint32_t lo[3], hi[3];
+};
+__device__ __forceinline__ NodeParent node_assemble(const LevelDesc& L, const uint64_t* skey, const uint64_t* slo,
+                                                    const uint64_t* shi, const uint32_t* scnt, uint32_t i, uint32_t tn) {
+    NodeParent q;
+    q.mask = 0; q.count = 0; q.n = 0;
+    q.lo[0] = q.lo[1] = q.lo[2] = 0xFFFFFFFFu;
+    q.hi[0] = q.hi[1] = q.hi[2] = 0;
+    const uint64_t pkey = skey[i] >> 3;
+    const uint32_t child_size = 1u << L.lv;
+    for (uint32_t j = i; j < tn && q.n < 8; ++j) {
+        const uint64_t ck = skey[j];
+        if ((ck >> 3) != pkey) break;
+        const uint32_t idx = uint32_t(ck & 7);
+        q.mask |= 1u << idx;
+        q.count = sat_add(q.count, scnt[j]);
+        if (L.need_box) {
+            const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
+                           oz = (idx >> 2) * child_size;
+            uint64_t clo = slo[j], chi = shi[j];
+            if (L.lv == 2) brick_box(slo[j], clo, chi);
+            q.lo[0] = min(q.lo[0], cell_x(clo) + ox); q.hi[0] = max(q.hi[0], cell_x(chi) + ox);
+            q.lo[1] = min(q.lo[1], cell_y(clo) + oy); q.hi[1] = max(q.hi[1], cell_y(chi) + oy);
+            q.lo[2] = min(q.lo[2], cell_z(clo) + oz); q.hi[2] = max(q.hi[2], cell_z(chi) + oz);
+        }
+        ++q.n;
+    }
+    return q;
+}
+
+// Records of parent `par` (key, count, first voxel, box, table slot and, when asked
+// for, its words).
+__device__ __forceinline__ void node_store(const LevelDesc& L, uint32_t par, const NodeParent& q, uint64_t pkey,
+                                           uint32_t first, const uint32_t* refs, uint32_t slot, bool words) {
+    if (words) {
+        uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
+        pw[0] = q.mask;
+        pw[1] = q.count;
+        for (uint32_t k = 0; k < q.n; ++k) pw[2 + k] = refs[k];
+    }
+    L.pkey[par] = pkey;
+    L.pcnt[par] = q.count;
+    L.pfirst[par] = first;
+    if (L.need_box) {
+        L.plo[par] = pack_cell(q.lo[0], q.lo[1], q.lo[2]);
+        L.phi[par] = pack_cell(q.hi[0], q.hi[1], q.hi[2]);
+    }
+    L.pslot[par] = slot;
+}
+
+// Tile of the node build: kBlock * NB children staged in shared memory (plus a halo
+// of up to 7 children of the tile's last parent), heads found with warp ballots,
+// positions by a look-back scan, then every thread builds parents from shared memory
+// and inserts them into the level's table.
 // Parents per thread of the node-owner kernel and children per thread of the node
 // build: large levels take 8 and 4 (tiles of 2048 parents / 1024 children), levels
 // small enough to leave most SMs idle with those take 1 (tiles of 256), so that their
 // tiles spread over the whole GPU (plan_build picks per level).
+// Small levels (NB == 1) are latency-bound: a global round trip costs about a
+// microsecond, an acquire-release atomic several. There every load of a staging step
+// is in flight together, and each parent (at most one per thread) is assembled before
+// the look-back: its words go to L.cwords at its first child's index (the table key of
+// these levels), so that the release of the insert after the look-back finds them long
+// performed, and its home slot is prefetched into the L2.
 constexpr int kNodeIT = 8;
 constexpr int kNodeTile = kBlock * kNodeIT;     // tile of the node-owner kernel (large levels)
 constexpr int kNBIT = 4;
@@ -1053,9 +1116,9 @@ constexpr size_t node_build_smem_bytes(bool bricks, int nb = kNBIT) {
            size_t(kBlock * nb) * 4 + 64;
 }
 
-// One tile of the node build (k_node_build takes one per block).
 template <int NB>
-__device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelDesc& L, const uint32_t tile) {
+__device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelDesc& L, const uint32_t tile,
+                                                const uint32_t children) {
     extern __shared__ uint64_t smem64[];
     constexpr int kTile = kBlock * NB;
     constexpr int N = kTile + kNodeHalo;
@@ -1070,43 +1133,98 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
     __shared__ uint64_t s_base;
     __shared__ uint64_t s_prev;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t C = L.lv == 2 ? min(d.counters[kCtrBricks], d.brick_bound)
-                                 : min(d.counters[kCtrParents + L.lv - 1], L.child_bound);
+    const uint32_t C = min(children, L.lv == 2 ? d.brick_bound : L.child_bound);
     const uint32_t ntiles = (C + kTile - 1) / kTile;
     if (tile >= ntiles) return;
     const uint32_t t0 = tile * kTile;
     const uint32_t own_n = min(uint32_t(kTile), C - t0);
     const uint32_t tn = min(uint32_t(N), C - t0);
-    // stage the children: coalesced loads; references of bricks from the dense
-    // leaf-reference array, of nodes by one gather per child from the level's table
-    // (every slot index loaded before the gathers, so that they are all in flight)
     constexpr int SPT = (N + kBlock - 1) / kBlock;
-    if (L.lv == 2) {
-        for (uint32_t i = threadIdx.x; i < tn; i += kBlock) sref[i] = brick_ref(d, t0 + i);
-    } else {
-        uint32_t cs[SPT];
+    if constexpr (NB == 1) {
+        // stage the children, every load of a step in flight together: the records,
+        // then (level 2) the owners of repeated masks and their leaf indices, or the
+        // children's node offsets from the level below's table
+        uint64_t key[SPT], lo[SPT], hi[SPT];
+        uint32_t first[SPT], cnt[SPT], ref[SPT], slot[SPT];
 #pragma unroll
         for (int r = 0; r < SPT; ++r) {
             const uint32_t i = threadIdx.x + r * kBlock;
-            cs[r] = i < tn ? L.cslot[t0 + i] : 0u;
+            const bool v = i < tn;
+            const uint32_t c = t0 + i;
+            key[r] = v ? L.ckey[c] : 0;
+            first[r] = v ? L.cfirst[c] : 0;
+            lo[r] = 0;
+            hi[r] = 0;
+            if (L.lv == 2) {
+                lo[r] = v ? L.cmask[c] : 0;
+                ref[r] = v ? __ldcg(d.bref + c) : 0;
+                slot[r] = v ? __ldcg(d.bslot + c) : 0;
+                cnt[r] = __popcll(lo[r]);
+            } else {
+                cnt[r] = v ? L.ccnt[c] : 0;
+                slot[r] = v ? L.cslot[c] : 0;
+                ref[r] = 0;
+                if (L.need_box && v) { lo[r] = L.clo[c]; hi[r] = L.chi[c]; }
+            }
         }
-#pragma unroll
-        for (int r = 0; r < SPT; ++r) {
-            const uint32_t i = threadIdx.x + r * kBlock;
-            if (i < tn) sref[i] = __ldcg(&L.ctable[cs[r]].w);
-        }
-    }
-    for (uint32_t i = threadIdx.x; i < tn; i += kBlock) {
-        const uint32_t c = t0 + i;
-        skey[i] = L.ckey[c];
-        sfirst[i] = L.cfirst[c];
         if (L.lv == 2) {
-            const uint64_t m = L.cmask[c];
-            scnt[i] = __popcll(m);
-            if (L.need_box) slo[i] = m;
+            uint32_t own[SPT];
+#pragma unroll
+            for (int r = 0; r < SPT; ++r)
+                own[r] = threadIdx.x + r * kBlock < tn && ref[r] == kNoRef ? ~__ldcg(&d.leaf_table[slot[r]].z) : 0;
+#pragma unroll
+            for (int r = 0; r < SPT; ++r)
+                if (threadIdx.x + r * kBlock < tn && ref[r] == kNoRef) ref[r] = __ldcg(d.bref + own[r]);
         } else {
-            scnt[i] = L.ccnt[c];
-            if (L.need_box) { slo[i] = L.clo[c]; shi[i] = L.chi[c]; }
+#pragma unroll
+            for (int r = 0; r < SPT; ++r)
+                if (threadIdx.x + r * kBlock < tn) ref[r] = __ldcg(&L.ctable[slot[r]].w);
+        }
+#pragma unroll
+        for (int r = 0; r < SPT; ++r) {
+            const uint32_t i = threadIdx.x + r * kBlock;
+            if (i < tn) {
+                skey[i] = key[r];
+                sfirst[i] = first[r];
+                sref[i] = ref[r];
+                scnt[i] = cnt[r];
+                if (L.need_box) {
+                    slo[i] = lo[r];
+                    if (L.lv != 2) shi[i] = hi[r];
+                }
+            }
+        }
+    } else {
+        // stage the children: coalesced loads; references of bricks from the dense
+        // leaf-reference array, of nodes by one gather per child from the level's table
+        // (every slot index loaded before the gathers, so that they are all in flight)
+        if (L.lv == 2) {
+            for (uint32_t i = threadIdx.x; i < tn; i += kBlock) sref[i] = brick_ref(d, t0 + i);
+        } else {
+            uint32_t cs[SPT];
+#pragma unroll
+            for (int r = 0; r < SPT; ++r) {
+                const uint32_t i = threadIdx.x + r * kBlock;
+                cs[r] = i < tn ? L.cslot[t0 + i] : 0u;
+            }
+#pragma unroll
+            for (int r = 0; r < SPT; ++r) {
+                const uint32_t i = threadIdx.x + r * kBlock;
+                if (i < tn) sref[i] = __ldcg(&L.ctable[cs[r]].w);
+            }
+        }
+        for (uint32_t i = threadIdx.x; i < tn; i += kBlock) {
+            const uint32_t c = t0 + i;
+            skey[i] = L.ckey[c];
+            sfirst[i] = L.cfirst[c];
+            if (L.lv == 2) {
+                const uint64_t m = L.cmask[c];
+                scnt[i] = __popcll(m);
+                if (L.need_box) slo[i] = m;
+            } else {
+                scnt[i] = L.ccnt[c];
+                if (L.need_box) { slo[i] = L.clo[c]; shi[i] = L.chi[c]; }
+            }
         }
     }
     if (threadIdx.x == 0) s_prev = t0 > 0 ? L.ckey[t0 - 1] : ~0ull;
@@ -1128,11 +1246,7 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
     uint32_t total;
     uint32_t wexcl = block_excl_scan(lane == 0 ? wc : 0, s_scan, &total);
     wexcl = __shfl_sync(kFull, wexcl, 0);
-    if (warp == 0) {
-        if (lane == 0 && tile != 0) st_relaxed(L.build_status + tile, kFlagAgg | total);
-        uint64_t ex = lookback_warp(L.build_status, tile, 0, total, d.counters + kCtrError);
-        if (lane == 0) s_base = ex;
-    }
+    if (threadIdx.x == 0 && tile != 0) st_relaxed(L.build_status + tile, kFlagAgg | total);
     uint32_t run = wexcl;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
@@ -1141,87 +1255,145 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
         run += __popc(hb[j]);
     }
     __syncthreads();
-    if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrParents + L.lv] = uint32_t(s_base + total);
-    const uint32_t base = uint32_t(s_base);
-    const uint32_t child_size = 1u << L.lv;
-    for (uint32_t h = threadIdx.x; h < total; h += kBlock) {
-        const uint32_t i = shead[h];
-        const uint32_t par = base + h;
-        const uint64_t pkey = skey[i] >> 3;
-        uint32_t mask = 0, count = 0, n = 0;
-        uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
-        for (uint32_t j = i; j < tn && n < 8; ++j) {
-            const uint64_t ck = skey[j];
-            if ((ck >> 3) != pkey) break;
-            const uint32_t idx = uint32_t(ck & 7);
-            mask |= 1u << idx;
-            count = sat_add(count, scnt[j]);
-            if (L.need_box) {
-                const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
-                               oz = (idx >> 2) * child_size;
-                uint64_t clo = slo[j], chi = shi[j];
-                if (L.lv == 2) brick_box(slo[j], clo, chi);
-                lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
-                lo[1] = min(lo[1], cell_y(clo) + oy); hi[1] = max(hi[1], cell_y(chi) + oy);
-                lo[2] = min(lo[2], cell_z(clo) + oz); hi[2] = max(hi[2], cell_z(chi) + oz);
+    if constexpr (NB == 1) {
+        // the tile's parents, one per thread: assembled, words published at the first
+        // child's index, home slot prefetched, all before the look-back
+        const bool mine = threadIdx.x < total;
+        NodeParent q;
+        uint32_t i = 0, h = 0;
+        if (mine) {
+            i = shead[threadIdx.x];
+            q = node_assemble(L, skey, slo, shi, scnt, i, tn);
+            uint32_t* cw = L.cwords + uint64_t(t0 + i) * kNodeStride;
+            cw[0] = q.mask;
+            cw[1] = q.count;
+            for (uint32_t k = 0; k < q.n; ++k) cw[2 + k] = sref[i + k];
+            h = uint32_t(node_hash(q.mask, q.count, sref + i, q.n)) & (L.pcap - 1);
+            prefetch_l2(&L.ptable[h]);
+        }
+        if (warp == 0) {
+            uint64_t ex = lookback_warp(L.build_status, tile, 0, total, d.counters + kCtrError);
+            if (lane == 0) s_base = ex;
+        }
+        __syncthreads();
+        if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrParents + L.lv] = uint32_t(s_base + total);
+        if (mine) {
+            const uint32_t par = uint32_t(s_base) + threadIdx.x;
+            if (par >= L.parent_bound) {
+                atomicOr(d.counters + kCtrError, kErrBound);
+            } else {
+                // the insert first: its release then covers only the words stored above
+                const uint32_t slot = node_insert(L.ptable, L.pcap, L.cwords, t0 + i, par, h, q.mask, q.count,
+                                                  sref + i, q.n, d.counters + kCtrError);
+                node_store(L, par, q, skey[i] >> 3, sfirst[i], sref + i, slot, true);
             }
-            ++n;
         }
-        if (par >= L.parent_bound) {
-            atomicOr(d.counters + kCtrError, kErrBound);
-            continue;
+    } else {
+        if (warp == 0) {
+            uint64_t ex = lookback_warp(L.build_status, tile, 0, total, d.counters + kCtrError);
+            if (lane == 0) s_base = ex;
         }
-        uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
-        pw[0] = mask;
-        pw[1] = count;
-        for (uint32_t k = 0; k < n; ++k) pw[2 + k] = sref[i + k];
-        L.pkey[par] = pkey;
-        L.pcnt[par] = count;
-        L.pfirst[par] = sfirst[i];
-        if (L.need_box) {
-            L.plo[par] = pack_cell(lo[0], lo[1], lo[2]);
-            L.phi[par] = pack_cell(hi[0], hi[1], hi[2]);
+        __syncthreads();
+        if (tile == ntiles - 1 && threadIdx.x == 0) d.counters[kCtrParents + L.lv] = uint32_t(s_base + total);
+        const uint32_t base = uint32_t(s_base);
+        for (uint32_t hh = threadIdx.x; hh < total; hh += kBlock) {
+            const uint32_t i = shead[hh];
+            const uint32_t par = base + hh;
+            const NodeParent q = node_assemble(L, skey, slo, shi, scnt, i, tn);
+            if (par >= L.parent_bound) {
+                atomicOr(d.counters + kCtrError, kErrBound);
+                continue;
+            }
+            // words first (the insert's release publishes them with the key)
+            uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
+            pw[0] = q.mask;
+            pw[1] = q.count;
+            for (uint32_t k = 0; k < q.n; ++k) pw[2 + k] = sref[i + k];
+            const uint32_t h = uint32_t(node_hash(q.mask, q.count, sref + i, q.n)) & (L.pcap - 1);
+            const uint32_t slot = node_insert(L.ptable, L.pcap, L.pwords, par, par, h, q.mask, q.count, sref + i,
+                                              q.n, d.counters + kCtrError);
+            node_store(L, par, q, skey[i] >> 3, sfirst[i], sref + i, slot, false);
         }
-        L.pslot[par] = node_insert(L.ptable, L.pcap, L.pwords, par, mask, count, sref + i, n, d.counters + kCtrError);
     }
+}
+
+// The tile id and one counter word in one round trip: the load is issued before the
+// atomic's result is waited for.
+__device__ __forceinline__ uint32_t dyn_tile_and(uint32_t* counters, uint32_t ctr, uint32_t idx, uint32_t idx2,
+                                                 uint32_t* s_slot, uint32_t* val, uint32_t* val2) {
+    if (threadIdx.x == 0) {
+        const uint32_t v = counters[idx], v2 = counters[idx2];
+        s_slot[0] = atomicAdd(counters + kCtrTiles + ctr, 1u);
+        s_slot[1] = v;
+        s_slot[2] = v2;
+    }
+    __syncthreads();
+    const uint32_t t = s_slot[0];
+    *val = s_slot[1];
+    *val2 = s_slot[2];
+    __syncthreads();
+    return t;
 }
 
 template <int NB>
 __global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc L) {
     grid_dep_wait();
-    __shared__ uint32_t s_tile;
-    const uint32_t tile = dyn_tile(d.counters, L.tile_ctr_build, &s_tile);
-    node_build_tile<NB>(d, L, tile);
+    __shared__ uint32_t s_tile[3];
+    uint32_t children, unused;
+    const uint32_t ci = L.lv == 2 ? kCtrBricks : kCtrParents + L.lv - 1;
+    const uint32_t tile = dyn_tile_and(d.counters, L.tile_ctr_build, ci, ci, s_tile, &children, &unused);
+    node_build_tile<NB>(d, L, tile, children);
 }
 
 // Owners of level lv get word offsets (scan of their lengths) and write their words.
-// One tile of the node owners (k_node_own takes one per block).
+// One tile of the node owners (k_node_own takes one per block). With one parent per
+// thread (small levels) the parent's words are loaded with its slot, before the
+// owner test, so that the tile takes two dependent round trips before its look-back.
 template <int NIT>
-__device__ __forceinline__ void node_own_tile(const BuildDesc& d, const LevelDesc& L, const uint32_t tile) {
+__device__ __forceinline__ void node_own_tile(const BuildDesc& d, const LevelDesc& L, const uint32_t tile,
+                                              const uint32_t parents, const uint32_t cursor) {
     __shared__ uint64_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t P = min(d.counters[kCtrParents + L.lv], L.parent_bound);
+    const uint32_t P = min(parents, L.parent_bound);
     constexpr uint32_t kTile = kBlock * NIT;
     const uint32_t ntiles = (P + kTile - 1) / kTile;
     if (tile >= ntiles) return;
-    const uint32_t cursor = d.counters[kCtrCursor + L.lv];
     const uint32_t wstart = tile * kTile + warp * 32 * NIT;
     uint32_t len[NIT], slot[NIT];
+    uint32_t w1[NIT == 1 ? kNodeStride : 1];  // NIT == 1: the parent's words
     uint64_t wsum = 0;  // words | count << 31
+    if constexpr (NIT == 1) {
+        const uint32_t i = wstart + lane;
+        const bool v = i < P;
+        slot[0] = v ? L.pslot[i] : 0;
+        const uint2* src = reinterpret_cast<const uint2*>(L.pwords + uint64_t(v ? i : 0) * kNodeStride);
 #pragma unroll
-    for (int j = 0; j < NIT; ++j) {
-        uint32_t i = wstart + j * 32 + lane;
-        len[j] = 0;
-        slot[j] = 0;
-        if (i < P) {
-            slot[j] = L.pslot[i];
-            if (~ld_relaxed32(&L.ptable[slot[j]].z) == i) len[j] = 2 + __popc(L.pwords[uint64_t(i) * kNodeStride] & 0xFF);
+        for (int k = 0; k < int(kNodeStride) / 2; ++k) {
+            const uint2 x = v ? __ldcg(src + k) : make_uint2(0, 0);
+            w1[2 * k] = x.x;
+            w1[2 * k + 1] = x.y;
         }
-        uint64_t v = len[j] | (uint64_t(len[j] ? 1 : 0) << 31);
+        len[0] = v && ~ld_relaxed32(&L.ptable[slot[0]].z) == i ? 2 + __popc(w1[0] & 0xFF) : 0;
+        uint64_t x = len[0] | (uint64_t(len[0] ? 1 : 0) << 31);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-        wsum += v;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+        wsum = x;
+    } else {
+#pragma unroll
+        for (int j = 0; j < NIT; ++j) {
+            uint32_t i = wstart + j * 32 + lane;
+            len[j] = 0;
+            slot[j] = 0;
+            if (i < P) {
+                slot[j] = L.pslot[i];
+                if (~ld_relaxed32(&L.ptable[slot[j]].z) == i) len[j] = 2 + __popc(L.pwords[uint64_t(i) * kNodeStride] & 0xFF);
+            }
+            uint64_t v = len[j] | (uint64_t(len[j] ? 1 : 0) << 31);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+            wsum += v;
+        }
     }
     uint64_t total;
     uint64_t wexcl = block_excl_scan64(lane == 0 ? wsum : 0, s_scan, &total);
@@ -1245,13 +1417,18 @@ __device__ __forceinline__ void node_own_tile(const BuildDesc& d, const LevelDes
         uint32_t off = run + x - len[j];
         if (len[j]) {
             uint32_t dst = cursor + off;
-            const uint2* src = reinterpret_cast<const uint2*>(L.pwords + uint64_t(i) * kNodeStride);
             uint32_t w[kNodeStride];
+            if constexpr (NIT == 1) {
 #pragma unroll
-            for (int k = 0; k < int(kNodeStride) / 2; ++k) {
-                uint2 v = __ldcg(src + k);  // written by the build kernel just before: bypass L1
-                w[2 * k] = v.x;
-                w[2 * k + 1] = v.y;
+                for (int k = 0; k < int(kNodeStride); ++k) w[k] = w1[k];
+            } else {
+                const uint2* src = reinterpret_cast<const uint2*>(L.pwords + uint64_t(i) * kNodeStride);
+#pragma unroll
+                for (int k = 0; k < int(kNodeStride) / 2; ++k) {
+                    uint2 v = __ldcg(src + k);  // written by the build kernel just before: bypass L1
+                    w[2 * k] = v.x;
+                    w[2 * k + 1] = v.y;
+                }
             }
             if (uint64_t(dst) + len[j] <= d.node_bound) {
 #pragma unroll
@@ -1274,9 +1451,11 @@ __device__ __forceinline__ void node_own_tile(const BuildDesc& d, const LevelDes
 template <int NIT>
 __global__ void __launch_bounds__(kBlock) k_node_own(BuildDesc d, LevelDesc L) {
     grid_dep_wait();
-    __shared__ uint32_t s_tile;
-    const uint32_t tile = dyn_tile(d.counters, L.tile_ctr_own, &s_tile);
-    node_own_tile<NIT>(d, L, tile);
+    __shared__ uint32_t s_tile[3];
+    uint32_t parents, cursor;
+    const uint32_t tile = dyn_tile_and(d.counters, L.tile_ctr_own, kCtrParents + L.lv, kCtrCursor + L.lv, s_tile,
+                                       &parents, &cursor);
+    node_own_tile<NIT>(d, L, tile, parents, cursor);
 }
 
 // Empty levels still have to pass the cursor on.
@@ -1331,16 +1510,23 @@ __global__ void __launch_bounds__(kBlock) k_prims(BuildDesc d, LevelDesc L) {
 
 // ---------------------------------------------------------------------------
 // Upper levels in one CTA. Each level: stage the children in shared memory, find
-// heads (block scan), build the parents' words into global memory, dedup them in a
-// shared-memory table (owner = minimum parent index), give the owners word offsets
-// (block scan of their lengths), write their words, and turn every parent's slot
-// into its node offset, which the next level uses as the child reference. Prims
-// (level rt_log2 - 1), roots and the final counts are written here as well.
-// Same output as k_node_build/k_node_own/k_prims/k_finalize per level.
+// heads (block scan), build the parents' words into global memory (their hashes into
+// shared memory), dedup them in a shared-memory table (owner = minimum parent index),
+// give the owners word offsets (block scan of their lengths), write their words, and
+// turn every parent's slot into its node offset, which the next level uses as the
+// child reference. Prims (level rt_log2 - 1), roots and the final counts are written
+// here as well. Same output as k_node_build/k_node_own/k_prims/k_finalize per level.
+// A global round trip costs about a microsecond here and a level has only a few
+// thousand parents, so the kernel is latency-bound: every load of a step is issued
+// before the first is used (loops unrolled over the thread's fixed share), children
+// and their boxes are staged in shared memory, and words are read back from global
+// memory only to compare two parents with equal hashes and to copy the owners out.
 // ---------------------------------------------------------------------------
+constexpr uint32_t kTailPer = kTailMaxChildren / kTailThreads;  // children (and parents) per thread
+constexpr uint32_t kTailScanWords = 72;
 constexpr size_t tail_smem_bytes() {
-    return size_t(kTailMaxChildren) * (8 + 4 + 4) + size_t(kTailSlots) * (4 + 4 + 4) + size_t(kTailMaxChildren) * (4 + 4) +
-           64 * 8;
+    return size_t(kTailMaxChildren) * (8 + 8 + 8 + 4 + 4 + 4 + 2 + 1) + size_t(kTailSlots) * (4 + 4) +
+           kTailScanWords * 4;
 }
 
 __device__ __forceinline__ uint32_t tail_scan(uint32_t v, uint32_t* sm, uint32_t* total) {
@@ -1371,18 +1557,32 @@ __device__ __forceinline__ uint32_t tail_scan(uint32_t v, uint32_t* sm, uint32_t
     return r;
 }
 
+// The kNodeStride words of parent q, written earlier in this kernel (L2, not L1).
+__device__ __forceinline__ void tail_words(const uint32_t* words, uint32_t q, uint32_t (&w)[kNodeStride]) {
+    const uint2* src = reinterpret_cast<const uint2*>(words + uint64_t(q) * kNodeStride);
+#pragma unroll
+    for (int k = 0; k < int(kNodeStride) / 2; ++k) {
+        const uint2 v = __ldcg(src + k);
+        w[2 * k] = v.x;
+        w[2 * k + 1] = v.y;
+    }
+}
+
 __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) {
     grid_dep_wait();
     extern __shared__ uint64_t tsm64[];
     uint64_t* skey = tsm64;                                            // children keys
-    uint32_t* sref = reinterpret_cast<uint32_t*>(skey + kTailMaxChildren);
+    uint64_t* slo = skey + kTailMaxChildren;                           // children boxes (level 2: masks)
+    uint64_t* shi = slo + kTailMaxChildren;
+    uint32_t* sref = reinterpret_cast<uint32_t*>(shi + kTailMaxChildren);
     uint32_t* scnt = sref + kTailMaxChildren;
-    uint32_t* tkey = scnt + kTailMaxChildren;                          // table: parent index + 1
+    uint32_t* pval = scnt + kTailMaxChildren;                          // parent: hash, then (owners) node offset
+    uint32_t* tkey = pval + kTailMaxChildren;                          // table: parent index + 1
     uint32_t* towner = tkey + kTailSlots;                              // table: minimum parent index
-    uint32_t* tval = towner + kTailSlots;                              // table: node offset
-    uint32_t* pslot = tval + kTailSlots;                               // parent -> slot
-    uint32_t* plen = pslot + kTailMaxChildren;                         // parent -> words (owners) / 0
-    uint32_t* scan = plen + kTailMaxChildren;                          // 65 words
+    uint32_t* scan = towner + kTailSlots;
+    uint16_t* pslot = reinterpret_cast<uint16_t*>(scan + kTailScanWords);  // parent -> slot
+    uint8_t* plen = reinterpret_cast<uint8_t*>(pslot + kTailMaxChildren);  // parent -> words
+    static_assert(kTailSlots <= 65536 && kNodeStride < 256, "slot and length fit their arrays");
     __shared__ uint32_t s_cursor, s_children;
     const uint32_t tid = threadIdx.x;
     const uint32_t lv0 = T.lv0;
@@ -1400,50 +1600,106 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
         const RecordSet& cs = T.set[(lv - 3) & 1];
         const bool box = lv + 1 <= d.rt_log2;
         const uint32_t child_size = 1u << lv;
-        // 1. stage children
-        for (uint32_t i = tid; i < C; i += kTailThreads) {
-            if (lv == 2) {
-                skey[i] = d.bkey[i];
-                sref[i] = brick_ref(d, i);
-                scnt[i] = __popcll(d.bmask[i]);
-            } else {
-                skey[i] = cs.key[i];
-                sref[i] = lv == lv0 ? __ldcg(&T.ctable0[cs.slot[i]].w) : cs.slot[i];
-                scnt[i] = cs.cnt[i];
+        // 1. stage children (coalesced: child tid + k * kTailThreads)
+        if (lv == 2) {
+            uint64_t key[kTailPer], mask[kTailPer];
+            uint32_t ref[kTailPer], slot[kTailPer], own[kTailPer];
+#pragma unroll
+            for (uint32_t k = 0; k < kTailPer; ++k) {
+                const uint32_t i = tid + k * kTailThreads;
+                const bool v = i < C;
+                key[k] = v ? d.bkey[i] : 0;
+                mask[k] = v ? d.bmask[i] : 0;
+                ref[k] = v ? __ldcg(d.bref + i) : 0;
+                slot[k] = v ? __ldcg(d.bslot + i) : 0;
+            }
+            // a brick that repeats a mask takes the leaf index of the mask's owner
+#pragma unroll
+            for (uint32_t k = 0; k < kTailPer; ++k)
+                own[k] = ref[k] == kNoRef ? ~__ldcg(&d.leaf_table[slot[k]].z) : 0;
+#pragma unroll
+            for (uint32_t k = 0; k < kTailPer; ++k)
+                if (ref[k] == kNoRef) ref[k] = __ldcg(d.bref + own[k]);
+#pragma unroll
+            for (uint32_t k = 0; k < kTailPer; ++k) {
+                const uint32_t i = tid + k * kTailThreads;
+                if (i < C) {
+                    skey[i] = key[k];
+                    slo[i] = mask[k];
+                    sref[i] = ref[k];
+                    scnt[i] = __popcll(mask[k]);
+                }
+            }
+        } else {
+            uint64_t key[kTailPer], lo[kTailPer], hi[kTailPer];
+            uint32_t ref[kTailPer], cnt[kTailPer];
+#pragma unroll
+            for (uint32_t k = 0; k < kTailPer; ++k) {
+                const uint32_t i = tid + k * kTailThreads;
+                const bool v = i < C;
+                key[k] = v ? __ldcg(cs.key + i) : 0;
+                ref[k] = v ? __ldcg(cs.slot + i) : 0;
+                cnt[k] = v ? __ldcg(cs.cnt + i) : 0;
+                lo[k] = v && box ? __ldcg(cs.lo + i) : 0;
+                hi[k] = v && box ? __ldcg(cs.hi + i) : 0;
+            }
+            if (lv == lv0) {
+                // references from the last kernel-built level's table (slot -> node offset)
+#pragma unroll
+                for (uint32_t k = 0; k < kTailPer; ++k)
+                    if (tid + k * kTailThreads < C) ref[k] = __ldcg(&T.ctable0[ref[k]].w);
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kTailPer; ++k) {
+                const uint32_t i = tid + k * kTailThreads;
+                if (i < C) {
+                    skey[i] = key[k];
+                    sref[i] = ref[k];
+                    scnt[i] = cnt[k];
+                    slo[i] = lo[k];
+                    shi[i] = hi[k];
+                }
             }
         }
         __syncthreads();
-        // 2. heads (4 consecutive children per thread) and parent indices
-        constexpr uint32_t PER = kTailMaxChildren / kTailThreads;
+        // 2. heads (kTailPer consecutive children per thread) and parent indices
         uint32_t hmask = 0, hc = 0;
 #pragma unroll
-        for (uint32_t k = 0; k < PER; ++k) {
-            const uint32_t i = tid * PER + k;
+        for (uint32_t k = 0; k < kTailPer; ++k) {
+            const uint32_t i = tid * kTailPer + k;
             if (i < C && (i == 0 || (skey[i] >> 3) != (skey[i - 1] >> 3))) { hmask |= 1u << k; ++hc; }
         }
         uint32_t P;
         uint32_t pbase = tail_scan(hc, scan, &P);
-        // 3. build parents (records and words in global memory)
+        // 3. build parents: records and words into global memory, hashes into pval
+        uint32_t fst[kTailPer];
+#pragma unroll
+        for (uint32_t k = 0; k < kTailPer; ++k) {
+            const uint32_t i = tid * kTailPer + k;
+            fst[k] = (hmask >> k) & 1 ? (lv == 2 ? d.bfirst[i] : __ldcg(cs.first + i)) : 0;
+        }
         uint32_t par = pbase;
 #pragma unroll
-        for (uint32_t k = 0; k < PER; ++k) {
+        for (uint32_t k = 0; k < kTailPer; ++k) {
             if (!((hmask >> k) & 1)) continue;
-            const uint32_t i = tid * PER + k;
+            const uint32_t i = tid * kTailPer + k;
             const uint64_t pkey = skey[i] >> 3;
             uint32_t mask = 0, count = 0, n = 0;
             uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
             uint32_t* pw = ps.words + uint64_t(par) * kNodeStride;
+            uint64_t hr = 0;  // hash of the references, in order
             for (uint32_t j = i; j < C && n < 8; ++j) {
                 const uint64_t ck = skey[j];
                 if ((ck >> 3) != pkey) break;
                 const uint32_t idx = uint32_t(ck & 7);
                 mask |= 1u << idx;
                 count = sat_add(count, scnt[j]);
-                pw[2 + n] = sref[j];
+                const uint32_t r = sref[j];
+                pw[2 + n] = r;
+                hr = mix64(hr ^ r);
                 if (box) {
-                    uint64_t clo, chi;
-                    if (lv == 2) brick_box(d.bmask[j], clo, chi);
-                    else { clo = cs.lo[j]; chi = cs.hi[j]; }
+                    uint64_t clo = slo[j], chi = shi[j];
+                    if (lv == 2) brick_box(slo[j], clo, chi);
                     const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
                                    oz = (idx >> 2) * child_size;
                     lo[0] = min(lo[0], cell_x(clo) + ox); hi[0] = max(hi[0], cell_x(chi) + ox);
@@ -1456,84 +1712,96 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
             pw[1] = count;
             ps.key[par] = pkey;
             ps.cnt[par] = count;
-            ps.first[par] = lv == 2 ? d.bfirst[i] : cs.first[i];
+            ps.first[par] = fst[k];
             if (box) {
                 ps.lo[par] = pack_cell(lo[0], lo[1], lo[2]);
                 ps.hi[par] = pack_cell(hi[0], hi[1], hi[2]);
             }
-            plen[par] = 2 + n;
+            pval[par] = uint32_t(mix64(mix64(hr ^ (uint64_t(n) << 32 | mask)) ^ count));
+            plen[par] = uint8_t(2 + n);
             ++par;
         }
         __syncthreads();  // all words written (visible to the block)
-        // 4. dedup in the shared-memory table (owner = minimum parent index)
+        // 4. dedup in the shared-memory table (owner = minimum parent index); words are
+        //    compared only for equal lengths in one probe sequence
         for (uint32_t q = tid; q < P; q += kTailThreads) {
-            const uint32_t* w = ps.words + uint64_t(q) * kNodeStride;
             const uint32_t len = plen[q];
-            uint64_t h64 = len;
-            for (uint32_t k = 0; k < len; ++k) h64 = mix64(h64 ^ w[k]);
-            uint32_t h = uint32_t(h64) & (kTailSlots - 1);
+            uint32_t h = pval[q] & (kTailSlots - 1);
+            uint32_t w[kNodeStride];
+            bool have = false;
             uint32_t probes = 0;
             for (; probes < kTailSlots; ++probes, h = (h + 1) & (kTailSlots - 1)) {
-                uint32_t cur = atomicCAS(tkey + h, 0u, q + 1);
+                const uint32_t cur = atomicCAS(tkey + h, 0u, q + 1);
                 if (cur == 0) break;
                 const uint32_t o = cur - 1;
-                if (plen[o] != len) continue;
-                const uint32_t* ow = ps.words + uint64_t(o) * kNodeStride;
+                if (plen[o] != len || pval[o] != pval[q]) continue;
+                if (!have) { tail_words(ps.words, q, w); have = true; }
+                uint32_t ow[kNodeStride];
+                tail_words(ps.words, o, ow);
                 bool same = true;
-                for (uint32_t k = 0; k < len && same; ++k) same = ow[k] == w[k];
+#pragma unroll
+                for (uint32_t k = 0; k < kNodeStride; ++k) same = same && (k >= len || ow[k] == w[k]);
                 if (same) break;
             }
             if (probes == kTailSlots) atomicOr(d.counters + kCtrError, kErrTable);
-            pslot[q] = h;
+            pslot[q] = uint16_t(h);
             atomicMin(towner + h, q);
         }
         __syncthreads();
-        // 5. owners: word offsets in parent order, write words, slot value = offset
-        uint32_t wl = 0;
+        // 5. owners: word offsets in parent order (pval = offset), then words out, one
+        //    parent per thread
+        uint32_t wl = 0, owners = 0;
 #pragma unroll
-        for (uint32_t k = 0; k < PER; ++k) {
-            const uint32_t q = tid * PER + k;
-            if (q < P && towner[pslot[q]] == q) wl += plen[q];
+        for (uint32_t k = 0; k < kTailPer; ++k) {
+            const uint32_t q = tid * kTailPer + k;
+            if (q < P && towner[pslot[q]] == q) { wl += plen[q]; ++owners; }
         }
         uint32_t words;
         uint32_t off = tail_scan(wl, scan, &words) + s_cursor;
 #pragma unroll
-        for (uint32_t k = 0; k < PER; ++k) {
-            const uint32_t q = tid * PER + k;
+        for (uint32_t k = 0; k < kTailPer; ++k) {
+            const uint32_t q = tid * kTailPer + k;
             if (q < P && towner[pslot[q]] == q) {
-                const uint32_t* w = ps.words + uint64_t(q) * kNodeStride;
-                if (uint64_t(off) + plen[q] <= d.node_bound) {
-                    for (uint32_t m = 0; m < plen[q]; ++m) d.nodes[off + m] = w[m];
-                } else {
-                    atomicOr(d.counters + kCtrError, kErrBound);
-                }
-                tval[pslot[q]] = off;
+                pval[q] = off;
                 off += plen[q];
             }
         }
-        uint32_t owners = 0;
-        for (uint32_t q = tid; q < P; q += kTailThreads) owners += towner[pslot[q]] == q;
         uint32_t utotal;
-        tail_scan(owners, scan, &utotal);  // includes a barrier: tval complete
-        // 6. references for the next level, prims, roots
+        tail_scan(owners, scan, &utotal);  // includes a barrier: pval of every owner set
         for (uint32_t q = tid; q < P; q += kTailThreads) {
-            const uint32_t node = tval[pslot[q]];
+            if (towner[pslot[q]] != q) continue;
+            uint32_t w[kNodeStride];
+            tail_words(ps.words, q, w);
+            const uint32_t dst = pval[q], len = plen[q];
+            if (uint64_t(dst) + len <= d.node_bound) {
+#pragma unroll
+                for (uint32_t m = 0; m < kNodeStride; ++m)
+                    if (m < len) d.nodes[dst + m] = w[m];
+            } else {
+                atomicOr(d.counters + kCtrError, kErrBound);
+            }
+        }
+        // 6. references for the next level, prims, roots
+        const bool prims = lv + 1 == d.rt_log2;
+        for (uint32_t q = tid; q < P; q += kTailThreads) {
+            const uint32_t node = pval[towner[pslot[q]]];
             ps.slot[q] = node;
-            if (lv + 1 == d.rt_log2 && q < d.prim_bound) {
-                const uint64_t full = ps.key[q];
+            if (prims && q < d.prim_bound) {
+                const uint64_t full = __ldcg(ps.key + q), plo = __ldcg(ps.lo + q), phi = __ldcg(ps.hi + q);
+                const uint32_t pfirst = __ldcg(ps.first + q);
+                const uint64_t prev = q > 0 ? __ldcg(ps.key + q - 1) : 0;
                 const uint64_t key = full & ((1ull << local_shift) - 1);
                 const uint32_t chunk = uint32_t(full >> local_shift);
-                const uint32_t cx = compact3(key), cy = compact3(key >> 1), cz = compact3(key >> 2);
                 const uint32_t first = d.chunked ? d.chunk_first[chunk] : 0;
+                const uint32_t cx = compact3(key), cy = compact3(key >> 1), cz = compact3(key >> 2);
                 const uint32_t size = 1u << d.rt_log2;
                 uint4 rec;
                 rec.x = node;
-                rec.y = ps.first[q] - first;
+                rec.y = pfirst - first;
                 const uint64_t pc = pack_cell(cx, cy, cz);
                 rec.z = uint32_t(pc);
                 rec.w = uint32_t(pc >> 32);
                 reinterpret_cast<uint4*>(d.prims)[q] = rec;
-                const uint64_t plo = ps.lo[q], phi = ps.hi[q];
                 const float eps = 1.0f / 256.0f;
                 float* b = d.aabbs + uint64_t(q) * 6;
                 b[0] = __fsub_rn(__fadd_rn(float(cx * size), float(cell_x(plo))), eps);
@@ -1542,13 +1810,14 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
                 b[3] = __fadd_rn(__fadd_rn(float(cx * size), float(cell_x(phi))), eps);
                 b[4] = __fadd_rn(__fadd_rn(float(cy * size), float(cell_y(phi))), eps);
                 b[5] = __fadd_rn(__fadd_rn(float(cz * size), float(cell_z(phi))), eps);
-                if (d.chunked && (q == 0 || (ps.key[q - 1] >> local_shift) != chunk)) d.prim_start[chunk] = q;
+                if (d.chunked && (q == 0 || (prev >> local_shift) != chunk)) d.prim_start[chunk] = q;
             }
             if (lv + 1 == d.log2 && d.chunked) {
-                const uint32_t chunk = uint32_t(ps.key[q]);
+                const uint32_t chunk = uint32_t(__ldcg(ps.key + q));
                 if (chunk < d.seg_count) d.roots[chunk] = node;
             }
         }
+        __syncthreads();  // every thread is done with the table
         // clear the table for the next level
         for (uint32_t i = tid; i < kTailSlots; i += kTailThreads) { tkey[i] = 0; towner[i] = 0xFFFFFFFFu; }
         if (tid == 0) {
@@ -1565,7 +1834,7 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
         // final counts and the empty geometry (gbuild.zig:607-624)
         const uint32_t top_set = (d.log2 - 1 - 2) & 1;
         uint32_t cursor = s_cursor;
-        uint32_t root = s_children > 0 ? T.set[top_set].slot[0] : 0;
+        uint32_t root = s_children > 0 ? __ldcg(T.set[top_set].slot) : 0;
         if (d.counters[kCtrUnique] == 0) {
             if (cursor + 2 <= d.node_bound) {
                 d.nodes[cursor] = 0;
