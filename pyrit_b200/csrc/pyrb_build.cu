@@ -424,7 +424,7 @@ struct Plan {
     uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0, o_chunk_vstart = 0;
     uint64_t o_bcount = 0, o_brec = 0, o_bloc = 0, o_bsum = 0;
     uint64_t o_set[2][7] = {};
-    uint64_t o_cwords = 0;
+    uint64_t o_cwords = 0, o_bdisp = 0;
     uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
     // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
     uint64_t out_size[6] = {};
@@ -564,6 +564,8 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     d.brick_bound = B;
     d.brick_tiles = d.sort_tiles * std::max(1u, tile_keys / 4096u);  // the unique tiles
     d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
+    if ((uint64_t(B) * 100 + lf - 1) / lf > (uint64_t(1) << 31))
+        return fail(PYRB_ERROR_INVALID_ARGUMENT, "brick bound exceeds the leaf table's 2^31 slots");
     d.leaf_cap = next_pow2((uint64_t(B) * 100 + lf - 1) / lf, 1024);
     // region by region only for a single volume: chunk batches (terrain-like chunks)
     // repeat their masks so much that their inserts stay in a small, cached set of
@@ -595,6 +597,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
     }
     p.o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
+    p.o_bdisp = zl.take(uint64_t(B));
     // a table filled region by region is cleared by its insert kernel, not by the memset
     p.o_leaf_table = d.leaf_regions > 1 ? 0 : zl.take(uint64_t(d.leaf_cap) * 16);
     p.o_regions = zl.take(3 * kMaxLeafRegions * 4);
@@ -738,6 +741,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     d.bmask = static_cast<uint64_t*>(at(p.o_bmask));
     d.bfirst = static_cast<uint32_t*>(at(p.o_bfirst));
     d.bslot = static_cast<uint32_t*>(at(p.o_bslot));
+    d.bdisp = static_cast<uint8_t*>(at(p.o_bdisp));
     d.bref = static_cast<uint32_t*>(at(p.o_bref));
     d.nodes = reinterpret_cast<uint32_t*>(outs[0]);
     d.leaves = reinterpret_cast<uint64_t*>(outs[1]);

@@ -701,8 +701,8 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
 }
 
 // ---------------------------------------------------------------------------
-// Dedup tables. Leaf table slot: {mask lo, mask hi, ~owner, leaf index};
-// node table slot: {parent index + 1, 0, ~owner, node offset}. ~owner with
+// Dedup tables. Leaf table slot: {mask lo, mask hi, ~owner, -};
+// node table slot: {key + 1, 0, ~owner, node offset}. ~owner with
 // atomicMax makes the minimum index the owner on zero-initialised tables.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void claim_owner(uint4* slot, uint32_t idx) {
@@ -715,50 +715,97 @@ __device__ __forceinline__ void claim_owner(uint4* slot, uint32_t idx) {
 // unless the table is filled region by region).
 __device__ __forceinline__ uint32_t probe_next(uint32_t h, uint32_t smask) { return (h & ~smask) | ((h + 1) & smask); }
 
-__device__ __forceinline__ uint32_t leaf_insert_at(uint4* table, uint32_t smask, uint64_t mask, uint32_t idx, uint32_t* err,
-                                                   uint32_t h, uint32_t probe0) {
+// 16-byte compare-and-swap: installs {lo, hi} if the slot holds {clo, chi}; returns the
+// slot's value before (an atomic snapshot of all 16 bytes).
+__device__ __forceinline__ void cas128(void* p, uint64_t clo, uint64_t chi, uint64_t lo, uint64_t hi, uint64_t& olo,
+                                       uint64_t& ohi) {
+    asm volatile(
+        "{\n\t.reg .b128 d, b, c;\n\tmov.b128 b, {%2, %3};\n\tmov.b128 c, {%4, %5};\n\t"
+        "atom.relaxed.gpu.global.cas.b128 d, [%6], b, c;\n\tmov.b128 {%0, %1}, d;\n\t}"
+        : "=l"(olo), "=l"(ohi)
+        : "l"(clo), "l"(chi), "l"(lo), "l"(hi), "l"(p)
+        : "memory");
+}
+
+// Leaf owners without a second look at the table. A brick becomes the owner of its
+// mask's slot when it installs itself (the 16-byte claim of an empty slot writes mask
+// and ~index at once; a later brick with a smaller index raises ~owner with a returning
+// atomicMax); whoever replaces an owner learns which one from the atomic's result and
+// marks it displaced. The minimum index is the only brick that installed itself and was
+// never displaced: bslot carries kInstalled, bdisp the displaced marks, and the owner
+// pass reads just those two streams.
+constexpr uint32_t kInstalled = 0x80000000u;
+constexpr uint32_t kSlotMask = 0x7FFFFFFFu;
+
+// A brick whose mask is in slot s (its ~owner last seen as z): tries to become the
+// owner. Returns kInstalled if it did.
+__device__ __forceinline__ uint32_t leaf_claim(const BuildDesc& d, uint4* slot, uint32_t idx, uint32_t z) {
+    const uint32_t inv = ~idx;
+    if (z >= inv) return 0;  // ~owner only grows: an owner at or below idx exists already
+    const uint32_t old = atomicMax(&slot->z, inv);
+    if (old >= inv) return 0;
+    if (old != 0) d.bdisp[~old] = 1;  // the owner replaced
+    return kInstalled;
+}
+
+// Insert of mask m (brick idx) from slot h on, probe0 probes already taken; returns the
+// slot | kInstalled when the brick became its owner.
+__device__ __forceinline__ uint32_t leaf_insert_at(const BuildDesc& d, uint4* table, uint32_t smask, uint64_t mask,
+                                                   uint32_t idx, uint32_t h, uint32_t probe0) {
     for (uint32_t probe = probe0; probe <= smask; ++probe) {
-        unsigned long long* kp = reinterpret_cast<unsigned long long*>(table + h);
-        unsigned long long cur = ld_relaxed(reinterpret_cast<const uint64_t*>(kp));
+        uint4* slot = table + h;
+        uint64_t cur = ld_relaxed(reinterpret_cast<const uint64_t*>(slot));
+        uint32_t z = 0;
         if (cur == 0) {
-            cur = atomicCAS(kp, 0ull, (unsigned long long)mask);
-            if (cur == 0) {
-                // first of its mask: claim without waiting (the result is not needed)
-                atomicMax(&table[h].z, ~idx);
-                return h;
-            }
+            uint64_t ohi;
+            cas128(slot, 0, 0, mask, uint64_t(~idx), cur, ohi);
+            if (cur == 0 && ohi == 0) return h | kInstalled;
+            z = uint32_t(ohi);
+        } else {
+            z = ld_relaxed32(&slot->z);
         }
-        if (cur == mask) {
-            claim_owner(table + h, idx);
-            return h;
-        }
+        if (cur == mask) return h | leaf_claim(d, slot, idx, z);
         h = probe_next(h, smask);
     }
-    atomicOr(err, kErrTable);
+    atomicOr(d.counters + kCtrError, kErrTable);
     return 0;
 }
 
-// The first probe of two inserts, their loads and compare-and-swaps in flight together
-// (each thread takes two bricks per round: the inserts are latency-bound on random
-// table slots; measured 11 % faster than one at a time).
-__device__ __forceinline__ void leaf_insert2(uint4* table, uint32_t cap, uint32_t smask, bool w0, uint64_t m0, uint32_t i0,
-                                             bool w1, uint64_t m1, uint32_t i1, uint32_t* s0, uint32_t* s1, uint32_t* err) {
+// The first probe of two inserts, their loads and claims in flight together (each
+// thread takes two bricks per round: the inserts are latency-bound on random table
+// slots; measured 11 % faster than one at a time). *s0 / *s1: slot | kInstalled.
+__device__ __forceinline__ void leaf_insert2(const BuildDesc& d, uint4* table, uint32_t cap, uint32_t smask, bool w0,
+                                             uint64_t m0, uint32_t i0, bool w1, uint64_t m1, uint32_t i1, uint32_t* s0,
+                                             uint32_t* s1) {
     const uint32_t h0 = uint32_t(mix64(m0)) & (cap - 1), h1 = uint32_t(mix64(m1)) & (cap - 1);
-    unsigned long long* p0 = reinterpret_cast<unsigned long long*>(table + h0);
-    unsigned long long* p1 = reinterpret_cast<unsigned long long*>(table + h1);
-    unsigned long long c0 = w0 ? __ldcg(p0) : 0ull, c1 = w1 ? __ldcg(p1) : 0ull;
-    unsigned long long r0 = c0, r1 = c1;
-    if (w0 && c0 == 0) r0 = atomicCAS(p0, 0ull, (unsigned long long)m0);
-    if (w1 && c1 == 0) r1 = atomicCAS(p1, 0ull, (unsigned long long)m1);
+    uint4* p0 = table + h0;
+    uint4* p1 = table + h1;
+    // the slot's first 16 bytes as one load: mask and (possibly older) ~owner
+    uint4 c0 = w0 ? __ldcg(p0) : make_uint4(0, 0, 0, 0), c1 = w1 ? __ldcg(p1) : make_uint4(0, 0, 0, 0);
+    uint64_t r0 = uint64_t(c0.y) << 32 | c0.x, r1 = uint64_t(c1.y) << 32 | c1.x;
+    uint32_t z0 = c0.z, z1 = c1.z;
+    bool f0 = false, f1 = false;
+    if (w0 && r0 == 0) {
+        uint64_t hi;
+        cas128(p0, 0, 0, m0, uint64_t(~i0), r0, hi);
+        f0 = r0 == 0 && hi == 0;
+        z0 = uint32_t(hi);
+    }
+    if (w1 && r1 == 0) {
+        uint64_t hi;
+        cas128(p1, 0, 0, m1, uint64_t(~i1), r1, hi);
+        f1 = r1 == 0 && hi == 0;
+        z1 = uint32_t(hi);
+    }
     if (w0) {
-        if (r0 == 0) { atomicMax(&table[h0].z, ~i0); *s0 = h0; }
-        else if (r0 == m0) { claim_owner(table + h0, i0); *s0 = h0; }
-        else *s0 = leaf_insert_at(table, smask, m0, i0, err, probe_next(h0, smask), 1);
+        if (f0) *s0 = h0 | kInstalled;
+        else if (r0 == m0) *s0 = h0 | leaf_claim(d, p0, i0, z0);
+        else *s0 = leaf_insert_at(d, table, smask, m0, i0, probe_next(h0, smask), 1);
     }
     if (w1) {
-        if (r1 == 0) { atomicMax(&table[h1].z, ~i1); *s1 = h1; }
-        else if (r1 == m1) { claim_owner(table + h1, i1); *s1 = h1; }
-        else *s1 = leaf_insert_at(table, smask, m1, i1, err, probe_next(h1, smask), 1);
+        if (f1) *s1 = h1 | kInstalled;
+        else if (r1 == m1) *s1 = h1 | leaf_claim(d, p1, i1, z1);
+        else *s1 = leaf_insert_at(d, table, smask, m1, i1, probe_next(h1, smask), 1);
     }
 }
 
@@ -830,10 +877,20 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
         const unsigned g0 = __match_any_sync(kFull, m0), g1 = __match_any_sync(kFull, m1);
         const unsigned l0 = __ffs(g0) - 1, l1 = __ffs(g1) - 1;
         uint32_t s0 = 0, s1 = 0;
-        leaf_insert2(d.leaf_table, d.leaf_cap, d.leaf_cap - 1, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1,
-                     &s0, &s1, d.counters + kCtrError);
+        leaf_insert2(d, d.leaf_table, d.leaf_cap, d.leaf_cap - 1, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1,
+                     &s0, &s1);
         s0 = __shfl_sync(kFull, s0, l0);
         s1 = __shfl_sync(kFull, s1, l1);
+        // the other bricks of a group: the lowest lane holds the lowest brick here (brick
+        // order), but they claim all the same, so that the rule stays the same everywhere
+        if (v0 && lane != l0) {
+            uint4* sl = d.leaf_table + (s0 & kSlotMask);
+            s0 = (s0 & kSlotMask) | leaf_claim(d, sl, b0, ld_relaxed32(&sl->z));
+        }
+        if (v1 && lane != l1) {
+            uint4* sl = d.leaf_table + (s1 & kSlotMask);
+            s1 = (s1 & kSlotMask) | leaf_claim(d, sl, b1, ld_relaxed32(&sl->z));
+        }
         if (v0) d.bslot[b0] = s0;
         if (v1) d.bslot[b1] = s1;
     }
@@ -900,13 +957,18 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert_regions(BuildDesc d) {
     const unsigned g0 = __match_any_sync(kFull, m0), g1 = __match_any_sync(kFull, m1);
     const unsigned l0 = __ffs(g0) - 1, l1 = __ffs(g1) - 1;
     uint32_t s0 = 0, s1 = 0;
-    leaf_insert2(d.leaf_table, d.leaf_cap, smask, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1, &s0, &s1,
-                 d.counters + kCtrError);
+    leaf_insert2(d, d.leaf_table, d.leaf_cap, smask, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1, &s0, &s1);
     s0 = __shfl_sync(kFull, s0, l0);
     s1 = __shfl_sync(kFull, s1, l1);
     // the lowest lane of a group need not hold its lowest brick: the others claim too
-    if (v0 && lane != l0) claim_owner(d.leaf_table + s0, b0);
-    if (v1 && lane != l1) claim_owner(d.leaf_table + s1, b1);
+    if (v0 && lane != l0) {
+        uint4* sl = d.leaf_table + (s0 & kSlotMask);
+        s0 = (s0 & kSlotMask) | leaf_claim(d, sl, b0, ld_relaxed32(&sl->z));
+    }
+    if (v1 && lane != l1) {
+        uint4* sl = d.leaf_table + (s1 & kSlotMask);
+        s1 = (s1 & kSlotMask) | leaf_claim(d, sl, b1, ld_relaxed32(&sl->z));
+    }
     if (v0) d.bslot[b0] = s0;
     if (v1) d.bslot[b1] = s1;
 }
@@ -927,23 +989,20 @@ __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
     if (tile >= ntiles) return;
     const uint32_t wstart = tile * kBrickTile + warp * 32 * kBrickIT;
     unsigned ob[kBrickIT];
-    uint32_t slot[kBrickIT], inv_owner[kBrickIT];
+    uint32_t slot[kBrickIT];
+    uint8_t disp[kBrickIT];
     uint32_t wc = 0;
-    // slots, then all owner words, then the ballots (loads in flight together)
+    // owners: installed and never displaced (two coalesced streams, no table reads)
 #pragma unroll
     for (int j = 0; j < kBrickIT; ++j) {
         uint32_t b = wstart + j * 32 + lane;
-        slot[j] = b < B ? d.bslot[b] : 0u;
+        slot[j] = b < B ? __ldcg(d.bslot + b) : 0u;
+        disp[j] = b < B ? __ldcg(d.bdisp + b) : uint8_t(1);
     }
 #pragma unroll
     for (int j = 0; j < kBrickIT; ++j) {
         uint32_t b = wstart + j * 32 + lane;
-        inv_owner[j] = b < B ? ld_relaxed32(&d.leaf_table[slot[j]].z) : 0u;
-    }
-#pragma unroll
-    for (int j = 0; j < kBrickIT; ++j) {
-        uint32_t b = wstart + j * 32 + lane;
-        const bool own = b < B && ~inv_owner[j] == b;
+        const bool own = b < B && (slot[j] & kInstalled) && !disp[j];
         ob[j] = __ballot_sync(kFull, own);
         wc += __popc(ob[j]);
     }
@@ -1033,7 +1092,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 // through the table's owner word (only bricks that repeat a mask take this gather).
 __device__ __forceinline__ uint32_t brick_ref(const BuildDesc& d, uint32_t b) {
     const uint32_t r = __ldcg(d.bref + b);
-    return r != kNoRef ? r : __ldcg(d.bref + ~__ldcg(&d.leaf_table[__ldcg(d.bslot + b)].z));
+    return r != kNoRef ? r : __ldcg(d.bref + ~__ldcg(&d.leaf_table[__ldcg(d.bslot + b) & kSlotMask].z));
 }
 
 // Assembles the parent whose first child is staged at i: mask, saturating count,
@@ -1158,7 +1217,7 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
             if (L.lv == 2) {
                 lo[r] = v ? L.cmask[c] : 0;
                 ref[r] = v ? __ldcg(d.bref + c) : 0;
-                slot[r] = v ? __ldcg(d.bslot + c) : 0;
+                slot[r] = v ? __ldcg(d.bslot + c) & kSlotMask : 0;
                 cnt[r] = __popcll(lo[r]);
             } else {
                 cnt[r] = v ? L.ccnt[c] : 0;
@@ -1611,7 +1670,7 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
                 key[k] = v ? d.bkey[i] : 0;
                 mask[k] = v ? d.bmask[i] : 0;
                 ref[k] = v ? __ldcg(d.bref + i) : 0;
-                slot[k] = v ? __ldcg(d.bslot + i) : 0;
+                slot[k] = v ? __ldcg(d.bslot + i) & kSlotMask : 0;
             }
             // a brick that repeats a mask takes the leaf index of the mask's owner
 #pragma unroll
