@@ -420,11 +420,11 @@ struct Plan {
              o_leafown_status = 0, o_leaf_table = 0, o_regions = 0;
     uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
     uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
-    uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bslot = 0, o_bref = 0;
+    uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bref = 0;
     uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0, o_chunk_vstart = 0;
     uint64_t o_bcount = 0, o_brec = 0, o_bloc = 0, o_bsum = 0;
     uint64_t o_set[2][7] = {};
-    uint64_t o_cwords = 0, o_bdisp = 0;
+    uint64_t o_cwords = 0, o_binst = 0, o_bdisp = 0;
     uint64_t zero_bytes = 0, ff_bytes = 0, scratch_bytes = 0;
     // output buffers (bytes): nodes, leaves, keys, attrs, prims, aabbs
     uint64_t out_size[6] = {};
@@ -597,6 +597,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
     }
     p.o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
+    p.o_binst = zl.take(uint64_t(B));
     p.o_bdisp = zl.take(uint64_t(B));
     // a table filled region by region is cleared by its insert kernel, not by the memset
     p.o_leaf_table = d.leaf_regions > 1 ? 0 : zl.take(uint64_t(d.leaf_cap) * 16);
@@ -645,7 +646,6 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     p.o_bkey = ol.take(uint64_t(B) * 8);
     p.o_bmask = ol.take(uint64_t(B) * 8);
     p.o_bfirst = ol.take(uint64_t(B) * 4);
-    p.o_bslot = ol.take(uint64_t(B) * 4);
     p.o_bref = ol.take(uint64_t(B) * 4);
     // parent record sets: A for even offsets from level 2, B for odd
     const uint32_t setn[2] = {P[2], log2 > 3 ? P[3] : 1u};
@@ -740,7 +740,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     d.bkey = static_cast<uint64_t*>(at(p.o_bkey));
     d.bmask = static_cast<uint64_t*>(at(p.o_bmask));
     d.bfirst = static_cast<uint32_t*>(at(p.o_bfirst));
-    d.bslot = static_cast<uint32_t*>(at(p.o_bslot));
+    d.binst = static_cast<uint8_t*>(at(p.o_binst));
     d.bdisp = static_cast<uint8_t*>(at(p.o_bdisp));
     d.bref = static_cast<uint32_t*>(at(p.o_bref));
     d.nodes = reinterpret_cast<uint32_t*>(outs[0]);
@@ -781,7 +781,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
             L.ckey = d.bkey;
             L.cmask = d.bmask;
             L.cfirst = d.bfirst;
-            L.cslot = d.bslot;
+            L.cslot = nullptr;  // brick references come from bref (and the leaf table)
             L.ctable = d.leaf_table;
         } else {
             const LevelDesc& C = levels.back();

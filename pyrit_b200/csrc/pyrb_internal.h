@@ -104,9 +104,9 @@ struct BuildDesc {
     uint64_t* bkey;
     uint64_t* bmask;
     uint32_t* bfirst;
-    uint32_t* bslot;
     uint32_t* bref;          // [B] leaf index of an owner brick, kNoRef for the others
-    uint8_t* bdisp;          // [B] 1: the brick was its mask's owner once and was replaced (zeroed)
+    uint8_t* binst;          // [B] 1: the brick made itself its mask's owner (zeroed)
+    uint8_t* bdisp;          // [B] 1: ... and was replaced by a smaller brick index (zeroed)
     uint4* leaf_table;       // {mask lo, mask hi, ~owner, leaf index}
     uint32_t leaf_cap;
     // Tables larger than L2 are filled region by region: leaf_regions > 1 groups the

@@ -732,8 +732,9 @@ __device__ __forceinline__ void cas128(void* p, uint64_t clo, uint64_t chi, uint
 // and ~index at once; a later brick with a smaller index raises ~owner with a returning
 // atomicMax); whoever replaces an owner learns which one from the atomic's result and
 // marks it displaced. The minimum index is the only brick that installed itself and was
-// never displaced: bslot carries kInstalled, bdisp the displaced marks, and the owner
-// pass reads just those two streams.
+// never displaced: binst holds the installed marks, bdisp the displaced ones, and the
+// owner pass reads just those two streams. A brick that is not the owner finds its
+// mask's slot again by probing (leaf_find), as the insert did.
 constexpr uint32_t kInstalled = 0x80000000u;
 constexpr uint32_t kSlotMask = 0x7FFFFFFFu;
 
@@ -807,6 +808,20 @@ __device__ __forceinline__ void leaf_insert2(const BuildDesc& d, uint4* table, u
         else if (r1 == m1) *s1 = h1 | leaf_claim(d, p1, i1, z1);
         else *s1 = leaf_insert_at(d, table, smask, m1, i1, probe_next(h1, smask), 1);
     }
+}
+
+// The slot holding `mask` (it was inserted): the same probe sequence as the insert,
+// each probe one 16-byte load that also returns the slot's ~owner.
+__device__ __forceinline__ uint4 leaf_find(const BuildDesc& d, uint64_t mask) {
+    const uint32_t smask = d.leaf_regions > 1 ? d.leaf_cap / d.leaf_regions - 1 : d.leaf_cap - 1;
+    uint32_t h = uint32_t(mix64(mask)) & (d.leaf_cap - 1);
+    for (uint32_t probe = 0; probe <= smask; ++probe) {
+        const uint4 v = __ldcg(d.leaf_table + h);
+        if ((uint64_t(v.y) << 32 | v.x) == mask) return v;
+        h = probe_next(h, smask);
+    }
+    atomicOr(d.counters + kCtrError, kErrTable);
+    return make_uint4(0, 0, 0, 0);
 }
 
 // Brick-indexed kernels (leaf owners) take tiles of kBrickTile bricks.
@@ -891,8 +906,8 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
             uint4* sl = d.leaf_table + (s1 & kSlotMask);
             s1 = (s1 & kSlotMask) | leaf_claim(d, sl, b1, ld_relaxed32(&sl->z));
         }
-        if (v0) d.bslot[b0] = s0;
-        if (v1) d.bslot[b1] = s1;
+        if (v0 && (s0 & kInstalled)) d.binst[b0] = 1;
+        if (v1 && (s1 & kInstalled)) d.binst[b1] = 1;
     }
 }
 
@@ -969,8 +984,9 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert_regions(BuildDesc d) {
         uint4* sl = d.leaf_table + (s1 & kSlotMask);
         s1 = (s1 & kSlotMask) | leaf_claim(d, sl, b1, ld_relaxed32(&sl->z));
     }
-    if (v0) d.bslot[b0] = s0;
-    if (v1) d.bslot[b1] = s1;
+    // one byte per brick that became an owner: scattered, but the array stays in L2
+    if (v0 && (s0 & kInstalled)) d.binst[b0] = 1;
+    if (v1 && (s1 & kInstalled)) d.binst[b1] = 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -989,20 +1005,19 @@ __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
     if (tile >= ntiles) return;
     const uint32_t wstart = tile * kBrickTile + warp * 32 * kBrickIT;
     unsigned ob[kBrickIT];
-    uint32_t slot[kBrickIT];
-    uint8_t disp[kBrickIT];
+    uint8_t inst[kBrickIT], disp[kBrickIT];
     uint32_t wc = 0;
     // owners: installed and never displaced (two coalesced streams, no table reads)
 #pragma unroll
     for (int j = 0; j < kBrickIT; ++j) {
         uint32_t b = wstart + j * 32 + lane;
-        slot[j] = b < B ? __ldcg(d.bslot + b) : 0u;
+        inst[j] = b < B ? __ldcg(d.binst + b) : uint8_t(0);
         disp[j] = b < B ? __ldcg(d.bdisp + b) : uint8_t(1);
     }
 #pragma unroll
     for (int j = 0; j < kBrickIT; ++j) {
         uint32_t b = wstart + j * 32 + lane;
-        const bool own = b < B && (slot[j] & kInstalled) && !disp[j];
+        const bool own = b < B && inst[j] && !disp[j];
         ob[j] = __ballot_sync(kFull, own);
         wc += __popc(ob[j]);
     }
@@ -1092,7 +1107,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 // through the table's owner word (only bricks that repeat a mask take this gather).
 __device__ __forceinline__ uint32_t brick_ref(const BuildDesc& d, uint32_t b) {
     const uint32_t r = __ldcg(d.bref + b);
-    return r != kNoRef ? r : __ldcg(d.bref + ~__ldcg(&d.leaf_table[__ldcg(d.bslot + b) & kSlotMask].z));
+    return r != kNoRef ? r : __ldcg(d.bref + ~leaf_find(d, __ldcg(d.bmask + b)).z);
 }
 
 // Assembles the parent whose first child is staged at i: mask, saturating count,
@@ -1217,7 +1232,7 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
             if (L.lv == 2) {
                 lo[r] = v ? L.cmask[c] : 0;
                 ref[r] = v ? __ldcg(d.bref + c) : 0;
-                slot[r] = v ? __ldcg(d.bslot + c) & kSlotMask : 0;
+                slot[r] = 0;
                 cnt[r] = __popcll(lo[r]);
             } else {
                 cnt[r] = v ? L.ccnt[c] : 0;
@@ -1227,10 +1242,11 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
             }
         }
         if (L.lv == 2) {
+            // a brick that repeats a mask: its mask's slot (found by probing) names the owner
             uint32_t own[SPT];
 #pragma unroll
             for (int r = 0; r < SPT; ++r)
-                own[r] = threadIdx.x + r * kBlock < tn && ref[r] == kNoRef ? ~__ldcg(&d.leaf_table[slot[r]].z) : 0;
+                own[r] = threadIdx.x + r * kBlock < tn && ref[r] == kNoRef ? ~leaf_find(d, lo[r]).z : 0;
 #pragma unroll
             for (int r = 0; r < SPT; ++r)
                 if (threadIdx.x + r * kBlock < tn && ref[r] == kNoRef) ref[r] = __ldcg(d.bref + own[r]);
@@ -1662,7 +1678,7 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
         // 1. stage children (coalesced: child tid + k * kTailThreads)
         if (lv == 2) {
             uint64_t key[kTailPer], mask[kTailPer];
-            uint32_t ref[kTailPer], slot[kTailPer], own[kTailPer];
+            uint32_t ref[kTailPer], own[kTailPer];
 #pragma unroll
             for (uint32_t k = 0; k < kTailPer; ++k) {
                 const uint32_t i = tid + k * kTailThreads;
@@ -1670,12 +1686,11 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BuildDesc d, TailDesc T) 
                 key[k] = v ? d.bkey[i] : 0;
                 mask[k] = v ? d.bmask[i] : 0;
                 ref[k] = v ? __ldcg(d.bref + i) : 0;
-                slot[k] = v ? __ldcg(d.bslot + i) & kSlotMask : 0;
             }
             // a brick that repeats a mask takes the leaf index of the mask's owner
 #pragma unroll
             for (uint32_t k = 0; k < kTailPer; ++k)
-                own[k] = ref[k] == kNoRef ? ~__ldcg(&d.leaf_table[slot[k]].z) : 0;
+                own[k] = ref[k] == kNoRef ? ~leaf_find(d, mask[k]).z : 0;
 #pragma unroll
             for (uint32_t k = 0; k < kTailPer; ++k)
                 if (ref[k] == kNoRef) ref[k] = __ldcg(d.bref + own[k]);
