@@ -763,8 +763,8 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
         L.own_it = p.oit[lv];
         L.need_box = lv + 1 <= d.rt_log2 ? 1u : 0u;
         L.pcap = p.cap[lv];
-        L.tile_ctr_build = 12 + 2 * (lv - 2);
-        L.tile_ctr_own = 13 + 2 * (lv - 2);
+        L.tile_ctr_build = kTileLevel0 + 2 * (lv - 2);
+        L.tile_ctr_own = kTileLevel0 + 1 + 2 * (lv - 2);
         const int ps = (lv - 2) & 1;
         L.pkey = static_cast<uint64_t*>(at(p.o_set[ps][0]));
         L.pcnt = static_cast<uint32_t*>(at(p.o_set[ps][1]));

@@ -286,7 +286,9 @@ __global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
 // Pass 3: every tile again, now with its first voxel and brick from the scan: sorted
 // unique keys and attributes, brick records, first voxel of every chunk.
 // 5 tiles per SM (48 registers): the tiles write as soon as their loads arrive, so
-// more of them in flight keep more loads outstanding
+// more of them in flight keep more loads outstanding. (One pass with a decoupled
+// look-back instead of count, scan and write measured slower on large grids, 9.8
+// against 8.6 ms on the 1024-chunk mix, and no faster at 2^24 cells.)
 template <bool kBucket>
 __global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     grid_dep_wait();

@@ -23,8 +23,14 @@ constexpr int kCtrNeed = 7;        // largest generator count above the chunk ca
 constexpr int kCtrCursor = 8;      // + lv: first node word of level lv (lv = 2..25)
 constexpr int kCtrParents = 36;    // + lv: P_lv
 constexpr int kCtrUniqueLv = 64;   // + lv: U_lv
-constexpr int kCtrTiles = 96;      // dynamic tile counters, one per launch
+constexpr int kCtrTiles = 96;      // dynamic tile counters, one per launch:
 constexpr int kCtrCount = 160;
+// ... disjoint ranges, so that no kernel of a build finds a counter another one advanced
+constexpr uint32_t kTileUnique = 0, kTileLeafOwn = 1, kTileLeafInsert = 2;
+constexpr uint32_t kTileLevel0 = 4;   // level lv: build 4 + 2 (lv - 2), owners 5 + 2 (lv - 2)
+constexpr uint32_t kTileSort0 = 44;   // sort pass p: 44 + p (8 passes at most: 64-bit keys take 8-bit digits)
+static_assert(kTileLevel0 + 2 * (20 - 2) + 1 < kTileSort0, "level counters below the sort's");
+static_assert(kTileSort0 + 16 <= kCtrCount - kCtrTiles, "sort counters fit");
 constexpr uint32_t kMaxLeafRegions = 64;
 #ifndef PYRB_LEAF_REGION_LOG
 #define PYRB_LEAF_REGION_LOG 22

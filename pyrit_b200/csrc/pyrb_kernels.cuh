@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(NT, PYRB_SORT_MIN_BLOCKS * kBlock / NT) k_sort
     uint32_t* vland = s_tile + 4;         // [TILE] values in tile order, copied asynchronously
 
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = dyn_tile(d.counters, pass, s_tile);
+    const uint32_t tile = dyn_tile(d.counters, kTileSort0 + pass, s_tile);
     if (tile >= d.seg_tile[d.seg_count]) return;
     const TileSpan sp = tile_span(d, tile);
     const uint32_t shift = d.pass_shift[pass], dmask = (1u << d.pass_bits[pass]) - 1;
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // a sort tile larger than kBlock * IT entries is taken in parts, each a unique tile
     const uint32_t parts = d.tile_keys / (kBlock * IT);
-    const uint32_t tile = dyn_tile(d.counters, 8, &s_tile);
+    const uint32_t tile = dyn_tile(d.counters, kTileUnique, &s_tile);
     const uint32_t ntiles = d.seg_tile[d.seg_count] * parts;
     if (tile >= ntiles) return;
     TileSpan sp = tile_span(d, tile / parts);
@@ -938,7 +938,7 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert_regions(BuildDesc d) {
         s_tbase[R] = t;
         s_ibase[R] = b;
     }
-    const uint32_t tile = dyn_tile(d.counters, 11, &s_tile);  // its barrier publishes s_tbase
+    const uint32_t tile = dyn_tile(d.counters, kTileLeafInsert, &s_tile);  // its barrier publishes s_tbase
     if (tile >= s_tbase[R]) return;
     uint32_t r = 0;
     while (s_tbase[r + 1] <= tile) ++r;
@@ -999,7 +999,7 @@ __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = dyn_tile(d.counters, 10, &s_tile);
+    const uint32_t tile = dyn_tile(d.counters, kTileLeafOwn, &s_tile);
     const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
     const uint32_t ntiles = (B + kBrickTile - 1) / kBrickTile;
     if (tile >= ntiles) return;

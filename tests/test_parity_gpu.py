@@ -284,6 +284,29 @@ def test_large_edges_64bit_keys_match_oracle(gb, log2, rt, n):
     assert_same_build(g, o, label=f"log2={log2}")
 
 
+@pytest.mark.parametrize("log2,rt,n", [(10, 7, 30000), (20, 3, 3000)])
+def test_eight_sort_passes_match_oracle(gb, log2, rt, n):
+    """The most sort passes a build takes: 8, for 4-bit digits on 31-bit keys (edge
+    2^10) and for 64-bit keys (edge 2^20, 61 bits), which always take 8-bit digits;
+    each pass has its own dynamic tile counter, none shared with the unique, leaf or
+    level kernels."""
+    rng = np.random.default_rng(100 + log2)
+    side = 1 << log2
+    centers = rng.integers(0, side, (4, 3))
+    pts = (centers[rng.integers(0, 4, n)] + rng.integers(-12, 13, (n, 3))) % side
+    v = np.concatenate([pts, rng.integers(0, 4, (n, 1))], 1).astype(np.uint32)
+    v = np.concatenate([v, v[:40]])
+    from pyrit_b200 import native
+    old = gb.get_tuning()
+    try:
+        gb.set_tuning(4, 1024, 50, native.PATH_SORT)
+        g = gb.build(log2, rt, dev(v)).download()
+        assert gb.last_stats().sort_passes == 8
+    finally:
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
+    assert_same_build(g, orc.gb_build(log2, rt, v), label=f"4-bit digits, log2={log2}")
+
+
 @pytest.mark.parametrize("seed", [0, 1])
 def test_world_edit_overlay_matches_worldedit_then_build_chunks(gb, seed):
     """World path: generated chunk voxels with each chunk's overlay edits merged by the
