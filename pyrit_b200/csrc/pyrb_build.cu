@@ -81,6 +81,9 @@ constexpr uint64_t kGridCellsPerEntry = 4;
 // A node level takes tiles of one item per thread below this many large tiles (2 per SM)
 constexpr uint32_t kSmallLevelTiles = 296;
 constexpr uint64_t kGridMaxCells = uint64_t(1) << 33;
+// Up to this many compaction tiles the count pass's last block scans the tile counts
+// (a few rounds of one 256-thread block); larger grids take the 1024-thread scan kernel
+constexpr uint32_t kGridFoldTiles = 16384;
 // The brick buckets (pyrb_tuning.path = 3) need their brick counters (4 B per brick
 // position) well inside the L2: up to 2^24 bricks (64 MB, a 1024^3 volume). They are
 // not chosen automatically: on the 1024^3 Bernoulli(0.15) worst case they measured
@@ -583,6 +586,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         d.use_bucket = p.bucket ? 1u : 0u;
         d.grid_cells = grid_cells;
         d.grid_tiles = uint32_t(std::max<uint64_t>((grid_cells + 64 * kGridTileBricks - 1) / (64 * kGridTileBricks), 1));
+        d.grid_fold = d.grid_tiles <= kGridFoldTiles ? 1u : 0u;
         d.bucket_scan_tiles = uint32_t(std::max<uint64_t>(((grid_cells >> 6) + kBucketScanTile - 1) / kBucketScanTile, 1));
     }
 
@@ -823,11 +827,13 @@ uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaSt
         prof.mark("bucket_scatter");
         launch(k_grid_count<true>, d.grid_tiles, kBlock, 0, st, d);
         prof.mark("bucket_tile_count");
-        launch(k_grid_scan, 1, kGridScanThreads, 0, st, d);
-        prof.mark("grid_scan");
+        if (!d.grid_fold) {
+            launch(k_grid_scan, 1, kGridScanThreads, 0, st, d);
+            prof.mark("grid_scan");
+        }
         launch(k_grid_write<true>, d.grid_tiles, kBlock, 0, st, d);
         prof.mark("bucket_tile_write");
-        launches += 8;
+        launches += d.grid_fold ? 7 : 8;
         if (d.chunked) {
             launch(k_grid_chunks, std::max(std::min((p.K + kBlock - 1) / kBlock, 1024u), 1u), kBlock, 0, st, d);
             prof.mark("grid_chunks");
@@ -838,11 +844,13 @@ uint32_t launch_plan(const Plan& p, const std::vector<LevelDesc>& levels, cudaSt
         prof.mark("grid_scatter");
         launch(k_grid_count<false>, d.grid_tiles, kBlock, 0, st, d);
         prof.mark("grid_count");
-        launch(k_grid_scan, 1, kGridScanThreads, 0, st, d);
-        prof.mark("grid_scan");
+        if (!d.grid_fold) {
+            launch(k_grid_scan, 1, kGridScanThreads, 0, st, d);
+            prof.mark("grid_scan");
+        }
         launch(k_grid_write<false>, d.grid_tiles, kBlock, 0, st, d);
         prof.mark("grid_write");
-        launches += 4;
+        launches += d.grid_fold ? 3 : 4;
         if (d.chunked) {
             launch(k_grid_chunks, std::max(std::min((p.K + kBlock - 1) / kBlock, 1024u), 1u), kBlock, 0, st, d);
             prof.mark("grid_chunks");

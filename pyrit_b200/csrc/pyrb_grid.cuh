@@ -187,59 +187,25 @@ __device__ __forceinline__ void bucket_load_attrs(const BuildDesc& d, uint64_t w
     }
 }
 
-// Pass 1 of the compaction: voxels and non-empty bricks of every tile, packed
-// (voxels | bricks << 32) into grid_count[tile]. No dependency between tiles.
-// kBucket: the cells come from the brick buckets (sparse builds), else from the grid.
-template <bool kBucket>
-__global__ void __launch_bounds__(kBlock) k_grid_count(BuildDesc d) {
-    grid_dep_wait();
-    __shared__ uint64_t s_sum[kWarps];
-    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = blockIdx.x;
-    const uint64_t nbricks = d.grid_cells >> 6;
-    const uint64_t wb0 = uint64_t(tile) * kGridTileBricks + uint64_t(warp) * kGridWarpBricks;
-    uint32_t a0[kGridWarpBricks], a1[kGridWarpBricks];
-    if constexpr (kBucket) {
-        __shared__ uint64_t s_cells[kGridTileBricks * 64];
-        bucket_load_attrs(d, wb0, nbricks, s_cells + warp * kGridWarpBricks * 64, a0, a1);
-    } else {
-        grid_load_attrs(d, wb0, nbricks, a0, a1);
-    }
-    uint32_t vox = 0, bricks = 0;
-#pragma unroll
-    for (int k = 0; k < kGridWarpBricks; ++k) {
-        const uint32_t n = __popc(__ballot_sync(kFull, a0[k] != 0)) + __popc(__ballot_sync(kFull, a1[k] != 0));
-        vox += n;
-        bricks += n ? 1u : 0u;
-    }
-    if (lane == 0) s_sum[warp] = uint64_t(vox) | (uint64_t(bricks) << 32);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint64_t t = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) t += s_sum[w];
-        d.grid_count[tile] = t;
-    }
-}
-
 // Pass 2: exclusive scan of the tile counts in place (one block, chunks of 16 per
 // thread); the totals are the build's voxel and brick counts.
 constexpr int kGridScanThreads = 1024, kGridScanPer = 16;
-// Exclusive scan of a[0, T) in place by one block of kGridScanThreads; returns the
-// total (valid in every thread).
+// Exclusive scan of a[0, T) in place by one block of NT threads; returns the total
+// (valid in every thread). The values may come from other blocks: read from L2.
+template <int NT = kGridScanThreads, int PER = kGridScanPer>
 __device__ __forceinline__ uint64_t block_scan_inplace(uint64_t* a, uint32_t T) {
-    __shared__ uint64_t s_w[kGridScanThreads / 32];
+    __shared__ uint64_t s_w[NT / 32];
     __shared__ uint64_t s_carry;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = kGridScanThreads / 32;
+    constexpr int NW = NT / 32;
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
-    for (uint32_t base = 0; base < T; base += kGridScanThreads * kGridScanPer) {
-        const uint32_t i0 = base + threadIdx.x * kGridScanPer;
-        uint64_t v[kGridScanPer], sum = 0;
+    for (uint32_t base = 0; base < T; base += NT * PER) {
+        const uint32_t i0 = base + threadIdx.x * PER;
+        uint64_t v[PER], sum = 0;
 #pragma unroll
-        for (int j = 0; j < kGridScanPer; ++j) {
-            v[j] = i0 + j < T ? a[i0 + j] : 0;
+        for (int j = 0; j < PER; ++j) {
+            v[j] = i0 + j < T ? __ldcg(a + i0 + j) : 0;
             sum += v[j];
         }
         uint64_t x = sum;
@@ -263,17 +229,70 @@ __device__ __forceinline__ uint64_t block_scan_inplace(uint64_t* a, uint32_t T) 
         __syncthreads();
         uint64_t run = s_carry + s_w[warp] + x - sum;
 #pragma unroll
-        for (int j = 0; j < kGridScanPer; ++j) {
+        for (int j = 0; j < PER; ++j) {
             if (i0 + j < T) a[i0 + j] = run;
             run += v[j];
         }
         __syncthreads();
-        if (threadIdx.x == kGridScanThreads - 1) s_carry = run;
+        if (threadIdx.x == NT - 1) s_carry = run;
         __syncthreads();
     }
     return s_carry;
 }
 
+// Pass 1 of the compaction: voxels and non-empty bricks of every tile, packed
+// (voxels | bricks << 32) into grid_count[tile]. No dependency between tiles. On grids
+// of at most kGridFoldTiles tiles the last block to finish also does pass 2 (the
+// scan), which saves a launch and its wait.
+// kBucket: the cells come from the brick buckets (sparse builds), else from the grid.
+template <bool kBucket>
+__global__ void __launch_bounds__(kBlock, 8) k_grid_count(BuildDesc d) {
+    grid_dep_wait();
+    __shared__ uint64_t s_sum[kWarps];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint64_t nbricks = d.grid_cells >> 6;
+    const uint64_t wb0 = uint64_t(tile) * kGridTileBricks + uint64_t(warp) * kGridWarpBricks;
+    uint32_t a0[kGridWarpBricks], a1[kGridWarpBricks];
+    if constexpr (kBucket) {
+        __shared__ uint64_t s_cells[kGridTileBricks * 64];
+        bucket_load_attrs(d, wb0, nbricks, s_cells + warp * kGridWarpBricks * 64, a0, a1);
+    } else {
+        grid_load_attrs(d, wb0, nbricks, a0, a1);
+    }
+    uint32_t vox = 0, bricks = 0;
+#pragma unroll
+    for (int k = 0; k < kGridWarpBricks; ++k) {
+        const uint32_t n = __popc(__ballot_sync(kFull, a0[k] != 0)) + __popc(__ballot_sync(kFull, a1[k] != 0));
+        vox += n;
+        bricks += n ? 1u : 0u;
+    }
+    if (lane == 0) s_sum[warp] = uint64_t(vox) | (uint64_t(bricks) << 32);
+    __syncthreads();
+    __shared__ uint32_t s_last;
+    if (threadIdx.x == 0) {
+        uint64_t t = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) t += s_sum[w];
+        d.grid_count[tile] = t;
+        if (d.grid_fold) {
+            // the last block to finish scans every tile's count (no scan launch)
+            __threadfence();
+            s_last = atomicAdd(d.counters + kCtrTiles + kTileGridDone, 1u) == gridDim.x - 1;
+        }
+    }
+    if (!d.grid_fold) return;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const uint64_t total = block_scan_inplace<kBlock, 4>(d.grid_count, d.grid_tiles);
+    if (threadIdx.x == 0) {
+        d.counters[kCtrUnique] = uint32_t(total);
+        d.counters[kCtrBricks] = uint32_t(total >> 32);
+    }
+}
+
+// Pass 2 on its own (larger grids): one block of kGridScanThreads.
 __global__ void __launch_bounds__(kGridScanThreads) k_grid_scan(BuildDesc d) {
     grid_dep_wait();
     const uint64_t total = block_scan_inplace(d.grid_count, d.grid_tiles);

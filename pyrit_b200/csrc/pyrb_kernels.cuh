@@ -52,6 +52,27 @@ __global__ void __launch_bounds__(1024) k_plan(BuildDesc d) {
     __shared__ uint64_t s_cells[1024];
     __shared__ uint64_t s_cell_carry;
     const uint32_t K = d.seg_count;
+    if (K == 1 && d.mode != kModeChunksEdits) {
+        // one segment (a single volume): no scans
+        if (threadIdx.x == 0) {
+            uint32_t size = d.n_total;
+            if (d.mode == kModeChunks) size = __ldg(d.offsets + 1) - __ldg(d.offsets);
+            if (d.mode == kModeBatch) {
+                size = __ldg(d.voxel_offsets + 1) - __ldg(d.voxel_offsets);
+                if (d.edit_offsets2) size += __ldg(d.edit_offsets2 + 1) - __ldg(d.edit_offsets2);
+            }
+            d.seg_entry[0] = 0;
+            d.seg_entry[1] = size;
+            d.seg_tile[0] = 0;
+            d.seg_tile[1] = (size + d.tile_keys - 1) / d.tile_keys;
+            if (d.use_grid | d.use_bucket) {
+                const uint32_t l = d.mode == kModeBatch ? __ldg(d.chunk_log2) : d.log2;
+                d.grid_off[0] = 0;
+                d.grid_off[1] = uint64_t(1) << (3 * l);
+            }
+        }
+        return;
+    }
     if (threadIdx.x == 0) { s_carry[0] = 0; s_carry[1] = 0; s_cell_carry = 0; }
     __syncthreads();
     for (uint32_t base = 0; base < K; base += 1024) {
