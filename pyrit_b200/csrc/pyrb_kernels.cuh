@@ -793,41 +793,40 @@ __device__ __forceinline__ uint32_t leaf_insert_at(const BuildDesc& d, uint4* ta
     return 0;
 }
 
-// The first probe of two inserts, their loads and claims in flight together (each
-// thread takes two bricks per round: the inserts are latency-bound on random table
-// slots; measured 11 % faster than one at a time). *s0 / *s1: slot | kInstalled.
-__device__ __forceinline__ void leaf_insert2(const BuildDesc& d, uint4* table, uint32_t cap, uint32_t smask, bool w0,
-                                             uint64_t m0, uint32_t i0, bool w1, uint64_t m1, uint32_t i1, uint32_t* s0,
-                                             uint32_t* s1) {
-    const uint32_t h0 = uint32_t(mix64(m0)) & (cap - 1), h1 = uint32_t(mix64(m1)) & (cap - 1);
-    uint4* p0 = table + h0;
-    uint4* p1 = table + h1;
-    // the slot's first 16 bytes as one load: mask and (possibly older) ~owner
-    uint4 c0 = w0 ? __ldcg(p0) : make_uint4(0, 0, 0, 0), c1 = w1 ? __ldcg(p1) : make_uint4(0, 0, 0, 0);
-    uint64_t r0 = uint64_t(c0.y) << 32 | c0.x, r1 = uint64_t(c1.y) << 32 | c1.x;
-    uint32_t z0 = c0.z, z1 = c1.z;
-    bool f0 = false, f1 = false;
-    if (w0 && r0 == 0) {
-        uint64_t hi;
-        cas128(p0, 0, 0, m0, uint64_t(~i0), r0, hi);
-        f0 = r0 == 0 && hi == 0;
-        z0 = uint32_t(hi);
+// The first probe of N inserts, their loads and claims in flight together (each thread
+// takes N bricks per round: the inserts are latency-bound on random table slots).
+// out[k]: slot | kInstalled.
+template <int N>
+__device__ __forceinline__ void leaf_insert_n(const BuildDesc& d, uint4* table, uint32_t cap, uint32_t smask,
+                                              const bool (&w)[N], const uint64_t (&m)[N], const uint32_t (&idx)[N],
+                                              uint32_t (&out)[N]) {
+    uint32_t h[N], z[N];
+    uint64_t r[N];
+    bool f[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        h[k] = uint32_t(mix64(m[k])) & (cap - 1);
+        // the slot's first 16 bytes as one load: mask and (possibly older) ~owner
+        const uint4 c = w[k] ? __ldcg(table + h[k]) : make_uint4(0, 0, 0, 0);
+        r[k] = uint64_t(c.y) << 32 | c.x;
+        z[k] = c.z;
+        f[k] = false;
     }
-    if (w1 && r1 == 0) {
-        uint64_t hi;
-        cas128(p1, 0, 0, m1, uint64_t(~i1), r1, hi);
-        f1 = r1 == 0 && hi == 0;
-        z1 = uint32_t(hi);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        if (w[k] && r[k] == 0) {
+            uint64_t hi;
+            cas128(table + h[k], 0, 0, m[k], uint64_t(~idx[k]), r[k], hi);
+            f[k] = r[k] == 0 && hi == 0;
+            z[k] = uint32_t(hi);
+        }
     }
-    if (w0) {
-        if (f0) *s0 = h0 | kInstalled;
-        else if (r0 == m0) *s0 = h0 | leaf_claim(d, p0, i0, z0);
-        else *s0 = leaf_insert_at(d, table, smask, m0, i0, probe_next(h0, smask), 1);
-    }
-    if (w1) {
-        if (f1) *s1 = h1 | kInstalled;
-        else if (r1 == m1) *s1 = h1 | leaf_claim(d, p1, i1, z1);
-        else *s1 = leaf_insert_at(d, table, smask, m1, i1, probe_next(h1, smask), 1);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        if (!w[k]) continue;
+        if (f[k]) out[k] = h[k] | kInstalled;
+        else if (r[k] == m[k]) out[k] = h[k] | leaf_claim(d, table + h[k], idx[k], z[k]);
+        else out[k] = leaf_insert_at(d, table, smask, m[k], idx[k], probe_next(h[k], smask), 1);
     }
 }
 
@@ -849,19 +848,43 @@ __device__ __forceinline__ uint4 leaf_find(const BuildDesc& d, uint64_t mask) {
 constexpr int kBrickIT = 8;
 constexpr int kBrickTile = kBlock * kBrickIT;
 
+// Per-region starts of tiles (clearing tiles, then insert tiles) and of the region's
+// bricks in the grouped list, for every region at once by warp 0 (one round trip).
+__device__ __forceinline__ void region_bases(const BuildDesc& d, uint32_t nz, uint32_t per_tile, uint32_t* tbase,
+                                             uint32_t* ibase) {
+    static_assert(kMaxLeafRegions == 64, "two regions per lane");
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t R = d.leaf_regions;
+    const uint32_t ra = lane, rb = lane + 32;
+    const uint32_t ca = ra < R ? __ldcg(d.region_count + ra) : 0, cb = rb < R ? __ldcg(d.region_count + rb) : 0;
+    const uint32_t ta = ra < R ? nz + (ca + per_tile - 1) / per_tile : 0;
+    const uint32_t tb = rb < R ? nz + (cb + per_tile - 1) / per_tile : 0;
+    uint32_t xa = ta, xb = tb, ya = ca, yb = cb;  // inclusive scans
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t p0 = __shfl_up_sync(kFull, xa, o), p1 = __shfl_up_sync(kFull, xb, o);
+        const uint32_t p2 = __shfl_up_sync(kFull, ya, o), p3 = __shfl_up_sync(kFull, yb, o);
+        if (lane >= unsigned(o)) { xa += p0; xb += p1; ya += p2; yb += p3; }
+    }
+    xb += __shfl_sync(kFull, xa, 31);
+    yb += __shfl_sync(kFull, ya, 31);
+    if (ra < R) { tbase[ra] = xa - ta; ibase[ra] = ya - ca; }
+    if (rb < R) { tbase[rb] = xb - tb; ibase[rb] = yb - cb; }
+    const uint32_t tt = __shfl_sync(kFull, xb, 31), tbs = __shfl_sync(kFull, yb, 31);
+    if (lane == 0) { tbase[R] = tt; ibase[R] = tbs; }
+}
+
 // Bricks grouped by the leaf-table region of their mask (BuildDesc::leaf_regions):
 // per tile, ranks within each region by shared-memory counters, one global cursor
 // reservation per region; the order inside a region does not matter (the owner is
 // the minimum brick index whatever the insert order).
 __global__ void __launch_bounds__(kBlock) k_leaf_part(BuildDesc d) {
     grid_dep_wait();
-    __shared__ uint32_t s_base[kMaxLeafRegions], s_cnt[kMaxLeafRegions], s_res[kMaxLeafRegions];
+    __shared__ uint32_t s_base[kMaxLeafRegions + 1], s_cnt[kMaxLeafRegions], s_res[kMaxLeafRegions];
+    __shared__ uint32_t s_tb[kMaxLeafRegions + 1];
     const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
     const uint32_t R = d.leaf_regions;
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (uint32_t r = 0; r < R; ++r) { s_base[r] = run; run += d.region_count[r]; }
-    }
+    if (threadIdx.x < 32) region_bases(d, 0, 1, s_tb, s_base);  // s_base: each region's first brick
     for (uint32_t t0 = blockIdx.x * kBrickTile; t0 < B; t0 += gridDim.x * kBrickTile) {
         if (threadIdx.x < R) s_cnt[threadIdx.x] = 0;
         __syncthreads();
@@ -903,32 +926,38 @@ __global__ void __launch_bounds__(kBlock) k_leaf_part(BuildDesc d) {
 // touches the table.
 __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
     grid_dep_wait();
+    constexpr int N = 2;
     const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
     const unsigned lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * kBlock;
-    for (uint32_t base = blockIdx.x * kBlock; base < B; base += 2 * stride) {
-        const uint32_t b0 = base + threadIdx.x, b1 = b0 + stride;
-        const bool v0 = b0 < B, v1 = b1 < B;
-        const uint64_t m0 = v0 ? d.bmask[b0] : 0, m1 = v1 ? d.bmask[b1] : 0;  // masks are never 0
-        const unsigned g0 = __match_any_sync(kFull, m0), g1 = __match_any_sync(kFull, m1);
-        const unsigned l0 = __ffs(g0) - 1, l1 = __ffs(g1) - 1;
-        uint32_t s0 = 0, s1 = 0;
-        leaf_insert2(d, d.leaf_table, d.leaf_cap, d.leaf_cap - 1, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1,
-                     &s0, &s1);
-        s0 = __shfl_sync(kFull, s0, l0);
-        s1 = __shfl_sync(kFull, s1, l1);
-        // the other bricks of a group: the lowest lane holds the lowest brick here (brick
-        // order), but they claim all the same, so that the rule stays the same everywhere
-        if (v0 && lane != l0) {
-            uint4* sl = d.leaf_table + (s0 & kSlotMask);
-            s0 = (s0 & kSlotMask) | leaf_claim(d, sl, b0, ld_relaxed32(&sl->z));
+    for (uint32_t base = blockIdx.x * kBlock; base < B; base += N * stride) {
+        bool v[N], w[N];
+        uint64_t m[N];
+        uint32_t b[N], s[N], l[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            b[k] = base + threadIdx.x + k * stride;
+            v[k] = b[k] < B;
+            m[k] = v[k] ? d.bmask[b[k]] : 0;  // masks are never 0
         }
-        if (v1 && lane != l1) {
-            uint4* sl = d.leaf_table + (s1 & kSlotMask);
-            s1 = (s1 & kSlotMask) | leaf_claim(d, sl, b1, ld_relaxed32(&sl->z));
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            l[k] = __ffs(__match_any_sync(kFull, m[k])) - 1;
+            w[k] = v[k] && lane == l[k];
+            s[k] = 0;
         }
-        if (v0 && (s0 & kInstalled)) d.binst[b0] = 1;
-        if (v1 && (s1 & kInstalled)) d.binst[b1] = 1;
+        leaf_insert_n<N>(d, d.leaf_table, d.leaf_cap, d.leaf_cap - 1, w, m, b, s);
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            s[k] = __shfl_sync(kFull, s[k], l[k]);
+            // the other bricks of a group: the lowest lane holds the lowest brick here (brick
+            // order), but they claim all the same, so that the rule stays the same everywhere
+            if (v[k] && lane != l[k]) {
+                uint4* sl = d.leaf_table + (s[k] & kSlotMask);
+                s[k] = (s[k] & kSlotMask) | leaf_claim(d, sl, b[k], ld_relaxed32(&sl->z));
+            }
+            if (v[k] && (s[k] & kInstalled)) d.binst[b[k]] = 1;
+        }
     }
 }
 
@@ -939,26 +968,26 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert(BuildDesc d) {
 // written while they sit in L2 and the inserts find them there. Probing wraps inside
 // the region. A tile waits only for tiles with smaller numbers, which are running or
 // done; the wait is bounded.
-constexpr uint32_t kZeroSlots = 2048;        // slots a clearing tile clears (32 KB)
-constexpr uint32_t kInsTile = 2 * kBlock;    // bricks an insert tile takes
+#ifndef PYRB_ZERO_SLOTS
+#define PYRB_ZERO_SLOTS 2048
+#endif
+constexpr uint32_t kZeroSlots = PYRB_ZERO_SLOTS;  // slots a clearing tile clears (32 KB)
+// Bricks per thread of an insert tile: one (tiles of 256 bricks) measured fastest at
+// 1024^3 (leaf inserts 0.67 ms against 0.70 with two and 0.87 with four in flight per
+// thread: smaller tiles keep more of them resident and waiting less)
+#ifndef PYRB_INS_PER_THREAD
+#define PYRB_INS_PER_THREAD 1
+#endif
+constexpr int kInsPerThread = PYRB_INS_PER_THREAD;
+constexpr uint32_t kInsTile = kInsPerThread * kBlock;  // bricks an insert tile takes
+
 __global__ void __launch_bounds__(kBlock) k_leaf_insert_regions(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_tbase[kMaxLeafRegions + 1], s_ibase[kMaxLeafRegions + 1];
     const uint32_t R = d.leaf_regions, S = d.leaf_cap / R, smask = S - 1;
     const uint32_t nz = (S + kZeroSlots - 1) / kZeroSlots;
-    if (threadIdx.x == 0) {
-        uint32_t t = 0, b = 0;
-        for (uint32_t r = 0; r < R; ++r) {
-            s_tbase[r] = t;
-            s_ibase[r] = b;
-            const uint32_t c = d.region_count[r];
-            t += nz + (c + kInsTile - 1) / kInsTile;
-            b += c;
-        }
-        s_tbase[R] = t;
-        s_ibase[R] = b;
-    }
+    if (threadIdx.x < 32) region_bases(d, nz, kInsTile, s_tbase, s_ibase);
     const uint32_t tile = dyn_tile(d.counters, kTileLeafInsert, &s_tile);  // its barrier publishes s_tbase
     if (tile >= s_tbase[R]) return;
     uint32_t r = 0;
@@ -985,29 +1014,38 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert_regions(BuildDesc d) {
     __syncthreads();
     const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
     const unsigned lane = threadIdx.x & 31;
-    const uint32_t i0 = s_ibase[r] + (k - nz) * kInsTile + threadIdx.x, i1 = i0 + kBlock, iend = s_ibase[r + 1];
-    const uint32_t b0 = i0 < iend ? d.pidx[i0] : 0u, b1 = i1 < iend ? d.pidx[i1] : 0u;
-    const bool v0 = i0 < iend && b0 < B, v1 = i1 < iend && b1 < B;  // b >= B: never, unless counts disagree
-    if ((i0 < iend && !v0) || (i1 < iend && !v1)) atomicOr(d.counters + kCtrError, kErrBound);
-    const uint64_t m0 = v0 ? d.pmask[i0] : 0, m1 = v1 ? d.pmask[i1] : 0;  // masks are never 0
-    const unsigned g0 = __match_any_sync(kFull, m0), g1 = __match_any_sync(kFull, m1);
-    const unsigned l0 = __ffs(g0) - 1, l1 = __ffs(g1) - 1;
-    uint32_t s0 = 0, s1 = 0;
-    leaf_insert2(d, d.leaf_table, d.leaf_cap, smask, v0 && lane == l0, m0, b0, v1 && lane == l1, m1, b1, &s0, &s1);
-    s0 = __shfl_sync(kFull, s0, l0);
-    s1 = __shfl_sync(kFull, s1, l1);
-    // the lowest lane of a group need not hold its lowest brick: the others claim too
-    if (v0 && lane != l0) {
-        uint4* sl = d.leaf_table + (s0 & kSlotMask);
-        s0 = (s0 & kSlotMask) | leaf_claim(d, sl, b0, ld_relaxed32(&sl->z));
+    constexpr int N = kInsPerThread;
+    const uint32_t iend = s_ibase[r + 1];
+    uint32_t ii[N], b[N], s[N], l[N];
+    bool v[N], w[N];
+    uint64_t m[N];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        ii[q] = s_ibase[r] + (k - nz) * kInsTile + q * kBlock + threadIdx.x;
+        b[q] = ii[q] < iend ? d.pidx[ii[q]] : 0u;
+        m[q] = ii[q] < iend ? d.pmask[ii[q]] : 0;
     }
-    if (v1 && lane != l1) {
-        uint4* sl = d.leaf_table + (s1 & kSlotMask);
-        s1 = (s1 & kSlotMask) | leaf_claim(d, sl, b1, ld_relaxed32(&sl->z));
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        v[q] = ii[q] < iend && b[q] < B;  // b >= B: never, unless counts disagree
+        if (ii[q] < iend && !v[q]) atomicOr(d.counters + kCtrError, kErrBound);
+        if (!v[q]) m[q] = 0;              // masks are never 0
+        l[q] = __ffs(__match_any_sync(kFull, m[q])) - 1;
+        w[q] = v[q] && lane == l[q];
+        s[q] = 0;
     }
-    // one byte per brick that became an owner: scattered, but the array stays in L2
-    if (v0 && (s0 & kInstalled)) d.binst[b0] = 1;
-    if (v1 && (s1 & kInstalled)) d.binst[b1] = 1;
+    leaf_insert_n<N>(d, d.leaf_table, d.leaf_cap, smask, w, m, b, s);
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        s[q] = __shfl_sync(kFull, s[q], l[q]);
+        // the lowest lane of a group need not hold its lowest brick: the others claim too
+        if (v[q] && lane != l[q]) {
+            uint4* sl = d.leaf_table + (s[q] & kSlotMask);
+            s[q] = (s[q] & kSlotMask) | leaf_claim(d, sl, b[q], ld_relaxed32(&sl->z));
+        }
+        // one byte per brick that became an owner: scattered, but the array stays in L2
+        if (v[q] && (s[q] & kInstalled)) d.binst[b[q]] = 1;
+    }
 }
 
 // ---------------------------------------------------------------------------
