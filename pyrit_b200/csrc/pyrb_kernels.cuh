@@ -1514,15 +1514,18 @@ __device__ __forceinline__ void node_own_tile(const BuildDesc& d, const LevelDes
         for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
         wsum = x;
     } else {
+        // slots and masks of all the thread's parents in flight, then their owner words
+        uint32_t mw[NIT];
 #pragma unroll
         for (int j = 0; j < NIT; ++j) {
-            uint32_t i = wstart + j * 32 + lane;
-            len[j] = 0;
-            slot[j] = 0;
-            if (i < P) {
-                slot[j] = L.pslot[i];
-                if (~ld_relaxed32(&L.ptable[slot[j]].z) == i) len[j] = 2 + __popc(L.pwords[uint64_t(i) * kNodeStride] & 0xFF);
-            }
+            const uint32_t i = wstart + j * 32 + lane;
+            slot[j] = i < P ? __ldcg(L.pslot + i) : 0u;
+            mw[j] = i < P ? __ldcg(L.pwords + uint64_t(i) * kNodeStride) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < NIT; ++j) {
+            const uint32_t i = wstart + j * 32 + lane;
+            len[j] = i < P && ~ld_relaxed32(&L.ptable[slot[j]].z) == i ? 2 + __popc(mw[j] & 0xFF) : 0u;
             uint64_t v = len[j] | (uint64_t(len[j] ? 1 : 0) << 31);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
