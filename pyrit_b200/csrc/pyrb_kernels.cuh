@@ -1113,19 +1113,21 @@ __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
 // ---------------------------------------------------------------------------
 // Node words are [mask, count, ref_0 .. ref_{n-1}]; the hash only places table
 // slots (equality is decided by comparing all words).
-__device__ __forceinline__ uint64_t node_hash(uint32_t mask, uint32_t count, const uint32_t* refs, uint32_t n) {
+__device__ __forceinline__ uint64_t node_hash(uint32_t mask, uint32_t count, const uint32_t (&refs)[8], uint32_t n) {
     uint64_t h = mix64(mix64(uint64_t(n + 2) ^ mask) ^ count);
-    for (uint32_t k = 0; k < n; ++k) h = mix64(h ^ refs[k]);
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k)
+        if (k < n) h = mix64(h ^ refs[k]);
     return h;
 }
 
 // Insert parent `par` into the level table. Its words are at key_words[key * stride]
 // (stored before this call: the CAS releases them); colliding residents are compared
-// by their words at key_words[(resident key) * stride]. h is the home slot, refs point
-// to shared memory. Returns the slot; the minimum parent index owns it.
+// by their words at key_words[(resident key) * stride]. h is the home slot, refs the
+// parent's child references. Returns the slot; the minimum parent index owns it.
 __device__ __forceinline__ uint32_t node_insert(uint4* table, uint32_t cap, const uint32_t* key_words, uint32_t key,
                                                 uint32_t par, uint32_t h, uint32_t mask, uint32_t count,
-                                                const uint32_t* refs, uint32_t n, uint32_t* err) {
+                                                const uint32_t (&refs)[8], uint32_t n, uint32_t* err) {
     for (uint32_t probe = 0; probe < cap; ++probe) {
         uint32_t* kp = &table[h].x;
         uint32_t cur = ld_acquire32(kp);
@@ -1169,36 +1171,55 @@ __device__ __forceinline__ uint32_t brick_ref(const BuildDesc& d, uint32_t b) {
     return r != kNoRef ? r : __ldcg(d.bref + ~leaf_find(d, __ldcg(d.bmask + b)).z);
 }
 
+// Per-child shared arrays of the node build are padded by one slot every 8 children:
+// a thread walks its parent's children, so the lanes of a warp read children ~8 apart
+// (one parent each), which without padding hit the same banks (16-way for 8-byte
+// words).
+__device__ __forceinline__ uint32_t cpad(uint32_t i) { return i + (i >> 3); }
+
 // Assembles the parent whose first child is staged at i: mask, saturating count,
-// number of children, box (when needed; at level 2 from the brick masks).
+// number of children, their references, box (when needed; at level 2 from the brick
+// masks).
 struct NodeParent {
     uint32_t mask, count, n;
     uint32_t lo[3], hi[3];
+    uint32_t refs[8];
 };
 __device__ __forceinline__ NodeParent node_assemble(const LevelDesc& L, const uint64_t* skey, const uint64_t* slo,
-                                                    const uint64_t* shi, const uint32_t* scnt, uint32_t i, uint32_t tn) {
+                                                    const uint64_t* shi, const uint32_t* scnt, const uint32_t* sref,
+                                                    uint32_t i, uint32_t tn) {
     NodeParent q;
     q.mask = 0; q.count = 0; q.n = 0;
     q.lo[0] = q.lo[1] = q.lo[2] = 0xFFFFFFFFu;
     q.hi[0] = q.hi[1] = q.hi[2] = 0;
-    const uint64_t pkey = skey[i] >> 3;
+    const uint64_t pkey = skey[cpad(i)] >> 3;
     const uint32_t child_size = 1u << L.lv;
-    for (uint32_t j = i; j < tn && q.n < 8; ++j) {
-        const uint64_t ck = skey[j];
-        if ((ck >> 3) != pkey) break;
+    bool in = true;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t j = i + k;
+        uint64_t ck = 0;
+        in = in && j < tn;
+        if (in) {
+            ck = skey[cpad(j)];
+            in = (ck >> 3) == pkey;
+        }
+        q.refs[k] = 0;
+        if (!in) continue;
         const uint32_t idx = uint32_t(ck & 7);
         q.mask |= 1u << idx;
-        q.count = sat_add(q.count, scnt[j]);
+        q.count = sat_add(q.count, scnt[cpad(j)]);
+        q.refs[k] = sref[cpad(j)];
         if (L.need_box) {
             const uint32_t ox = (idx & 1) * child_size, oy = ((idx >> 1) & 1) * child_size,
                            oz = (idx >> 2) * child_size;
-            uint64_t clo = slo[j], chi = shi[j];
-            if (L.lv == 2) brick_box(slo[j], clo, chi);
+            uint64_t clo = slo[cpad(j)], chi = shi[cpad(j)];
+            if (L.lv == 2) brick_box(clo, clo, chi);
             q.lo[0] = min(q.lo[0], cell_x(clo) + ox); q.hi[0] = max(q.hi[0], cell_x(chi) + ox);
             q.lo[1] = min(q.lo[1], cell_y(clo) + oy); q.hi[1] = max(q.hi[1], cell_y(chi) + oy);
             q.lo[2] = min(q.lo[2], cell_z(clo) + oz); q.hi[2] = max(q.hi[2], cell_z(chi) + oz);
         }
-        ++q.n;
+        q.n = k + 1;
     }
     return q;
 }
@@ -1206,12 +1227,14 @@ __device__ __forceinline__ NodeParent node_assemble(const LevelDesc& L, const ui
 // Records of parent `par` (key, count, first voxel, box, table slot and, when asked
 // for, its words).
 __device__ __forceinline__ void node_store(const LevelDesc& L, uint32_t par, const NodeParent& q, uint64_t pkey,
-                                           uint32_t first, const uint32_t* refs, uint32_t slot, bool words) {
+                                           uint32_t first, uint32_t slot, bool words) {
     if (words) {
         uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
         pw[0] = q.mask;
         pw[1] = q.count;
-        for (uint32_t k = 0; k < q.n; ++k) pw[2 + k] = refs[k];
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k)
+            if (k < q.n) pw[2 + k] = q.refs[k];
     }
     L.pkey[par] = pkey;
     L.pcnt[par] = q.count;
@@ -1245,7 +1268,8 @@ constexpr int kNodeHalo = 8;
 // Level 2 stages the children's brick masks (its parents' boxes come from them) rather
 // than their boxes: 28 instead of 36 bytes per child, 6 tiles per SM instead of 5.
 constexpr size_t node_build_smem_bytes(bool bricks, int nb = kNBIT) {
-    return size_t(kBlock * nb + kNodeHalo) * (bricks ? 8 + 8 + 4 + 4 + 4 : 8 + 8 + 8 + 4 + 4 + 4) +
+    return size_t(kBlock * nb + kNodeHalo + (kBlock * nb + kNodeHalo) / 8 + 1) *
+               (bricks ? 8 + 8 + 4 + 4 + 4 : 8 + 8 + 8 + 4 + 4 + 4) +
            size_t(kBlock * nb) * 4 + 64;
 }
 
@@ -1255,13 +1279,14 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
     extern __shared__ uint64_t smem64[];
     constexpr int kTile = kBlock * NB;
     constexpr int N = kTile + kNodeHalo;
+    constexpr int NP = N + N / 8 + 1;                // padded (cpad) per-child arrays
     uint64_t* skey = smem64;
-    uint64_t* slo = skey + N;                        // level 2: the brick masks
-    uint64_t* shi = L.lv == 2 ? slo : slo + N;
-    uint32_t* sref = reinterpret_cast<uint32_t*>(shi + N);
-    uint32_t* scnt = sref + N;
-    uint32_t* sfirst = scnt + N;
-    uint32_t* shead = sfirst + N;
+    uint64_t* slo = skey + NP;                       // level 2: the brick masks
+    uint64_t* shi = L.lv == 2 ? slo : slo + NP;
+    uint32_t* sref = reinterpret_cast<uint32_t*>(shi + NP);
+    uint32_t* scnt = sref + NP;
+    uint32_t* sfirst = scnt + NP;
+    uint32_t* shead = sfirst + NP;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
     __shared__ uint64_t s_prev;
@@ -1318,13 +1343,14 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
         for (int r = 0; r < SPT; ++r) {
             const uint32_t i = threadIdx.x + r * kBlock;
             if (i < tn) {
-                skey[i] = key[r];
-                sfirst[i] = first[r];
-                sref[i] = ref[r];
-                scnt[i] = cnt[r];
+                const uint32_t pi = cpad(i);
+                skey[pi] = key[r];
+                sfirst[pi] = first[r];
+                sref[pi] = ref[r];
+                scnt[pi] = cnt[r];
                 if (L.need_box) {
-                    slo[i] = lo[r];
-                    if (L.lv != 2) shi[i] = hi[r];
+                    slo[pi] = lo[r];
+                    if (L.lv != 2) shi[pi] = hi[r];
                 }
             }
         }
@@ -1333,7 +1359,7 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
         // leaf-reference array, of nodes by one gather per child from the level's table
         // (every slot index loaded before the gathers, so that they are all in flight)
         if (L.lv == 2) {
-            for (uint32_t i = threadIdx.x; i < tn; i += kBlock) sref[i] = brick_ref(d, t0 + i);
+            for (uint32_t i = threadIdx.x; i < tn; i += kBlock) sref[cpad(i)] = brick_ref(d, t0 + i);
         } else {
             uint32_t cs[SPT];
 #pragma unroll
@@ -1344,20 +1370,20 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
 #pragma unroll
             for (int r = 0; r < SPT; ++r) {
                 const uint32_t i = threadIdx.x + r * kBlock;
-                if (i < tn) sref[i] = __ldcg(&L.ctable[cs[r]].w);
+                if (i < tn) sref[cpad(i)] = __ldcg(&L.ctable[cs[r]].w);
             }
         }
         for (uint32_t i = threadIdx.x; i < tn; i += kBlock) {
-            const uint32_t c = t0 + i;
-            skey[i] = L.ckey[c];
-            sfirst[i] = L.cfirst[c];
+            const uint32_t c = t0 + i, pi = cpad(i);
+            skey[pi] = L.ckey[c];
+            sfirst[pi] = L.cfirst[c];
             if (L.lv == 2) {
                 const uint64_t m = L.cmask[c];
-                scnt[i] = __popcll(m);
-                if (L.need_box) slo[i] = m;
+                scnt[pi] = __popcll(m);
+                if (L.need_box) slo[pi] = m;
             } else {
-                scnt[i] = L.ccnt[c];
-                if (L.need_box) { slo[i] = L.clo[c]; shi[i] = L.chi[c]; }
+                scnt[pi] = L.ccnt[c];
+                if (L.need_box) { slo[pi] = L.clo[c]; shi[pi] = L.chi[c]; }
             }
         }
     }
@@ -1371,8 +1397,8 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
         const uint32_t i = warp * 32 * NB + j * 32 + lane;
         bool head = false;
         if (i < own_n) {
-            const uint64_t pk = i == 0 ? s_prev : skey[i - 1];
-            head = (t0 + i == 0) || (skey[i] >> 3) != (pk >> 3);
+            const uint64_t pk = i == 0 ? s_prev : skey[cpad(i - 1)];
+            head = (t0 + i == 0) || (skey[cpad(i)] >> 3) != (pk >> 3);
         }
         hb[j] = __ballot_sync(kFull, head);
         wc += __popc(hb[j]);
@@ -1397,12 +1423,14 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
         uint32_t i = 0, h = 0;
         if (mine) {
             i = shead[threadIdx.x];
-            q = node_assemble(L, skey, slo, shi, scnt, i, tn);
+            q = node_assemble(L, skey, slo, shi, scnt, sref, i, tn);
             uint32_t* cw = L.cwords + uint64_t(t0 + i) * kNodeStride;
             cw[0] = q.mask;
             cw[1] = q.count;
-            for (uint32_t k = 0; k < q.n; ++k) cw[2 + k] = sref[i + k];
-            h = uint32_t(node_hash(q.mask, q.count, sref + i, q.n)) & (L.pcap - 1);
+#pragma unroll
+            for (uint32_t k = 0; k < 8; ++k)
+                if (k < q.n) cw[2 + k] = q.refs[k];
+            h = uint32_t(node_hash(q.mask, q.count, q.refs, q.n)) & (L.pcap - 1);
             prefetch_l2(&L.ptable[h]);
         }
         if (warp == 0) {
@@ -1418,8 +1446,8 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
             } else {
                 // the insert first: its release then covers only the words stored above
                 const uint32_t slot = node_insert(L.ptable, L.pcap, L.cwords, t0 + i, par, h, q.mask, q.count,
-                                                  sref + i, q.n, d.counters + kCtrError);
-                node_store(L, par, q, skey[i] >> 3, sfirst[i], sref + i, slot, true);
+                                                  q.refs, q.n, d.counters + kCtrError);
+                node_store(L, par, q, skey[cpad(i)] >> 3, sfirst[cpad(i)], slot, true);
             }
         }
     } else {
@@ -1433,7 +1461,7 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
         for (uint32_t hh = threadIdx.x; hh < total; hh += kBlock) {
             const uint32_t i = shead[hh];
             const uint32_t par = base + hh;
-            const NodeParent q = node_assemble(L, skey, slo, shi, scnt, i, tn);
+            const NodeParent q = node_assemble(L, skey, slo, shi, scnt, sref, i, tn);
             if (par >= L.parent_bound) {
                 atomicOr(d.counters + kCtrError, kErrBound);
                 continue;
@@ -1442,11 +1470,13 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
             uint32_t* pw = L.pwords + uint64_t(par) * kNodeStride;
             pw[0] = q.mask;
             pw[1] = q.count;
-            for (uint32_t k = 0; k < q.n; ++k) pw[2 + k] = sref[i + k];
-            const uint32_t h = uint32_t(node_hash(q.mask, q.count, sref + i, q.n)) & (L.pcap - 1);
-            const uint32_t slot = node_insert(L.ptable, L.pcap, L.pwords, par, par, h, q.mask, q.count, sref + i,
+#pragma unroll
+            for (uint32_t k = 0; k < 8; ++k)
+                if (k < q.n) pw[2 + k] = q.refs[k];
+            const uint32_t h = uint32_t(node_hash(q.mask, q.count, q.refs, q.n)) & (L.pcap - 1);
+            const uint32_t slot = node_insert(L.ptable, L.pcap, L.pwords, par, par, h, q.mask, q.count, q.refs,
                                               q.n, d.counters + kCtrError);
-            node_store(L, par, q, skey[i] >> 3, sfirst[i], sref + i, slot, false);
+            node_store(L, par, q, skey[cpad(i)] >> 3, sfirst[cpad(i)], slot, false);
         }
     }
 }
@@ -1469,8 +1499,10 @@ __device__ __forceinline__ uint32_t dyn_tile_and(uint32_t* counters, uint32_t ct
     return t;
 }
 
+// 6 tiles per SM for the small levels; large tiles keep their parent's references in
+// registers and take 5 (51 registers, no spills)
 template <int NB>
-__global__ void __launch_bounds__(kBlock, 6) k_node_build(BuildDesc d, LevelDesc L) {
+__global__ void __launch_bounds__(kBlock, NB == 1 ? 6 : 5) k_node_build(BuildDesc d, LevelDesc L) {
     grid_dep_wait();
     __shared__ uint32_t s_tile[3];
     uint32_t children, unused;
