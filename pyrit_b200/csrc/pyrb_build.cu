@@ -81,8 +81,8 @@ constexpr uint64_t kGridCellsPerEntry = 4;
 // A node level takes tiles of one item per thread below this many large tiles (2 per SM)
 constexpr uint32_t kSmallLevelTiles = 296;
 constexpr uint64_t kGridMaxCells = uint64_t(1) << 33;
-// Up to this many compaction tiles the count pass's last block scans the tile counts
-// (a few rounds of one 256-thread block); larger grids take the 1024-thread scan kernel
+// Up to this many compaction tiles the write pass adds up its own prefix (at most 256
+// group sums and 63 tile counts); larger grids take the 1024-thread scan kernel
 constexpr uint32_t kGridFoldTiles = 16384;
 // The brick buckets (pyrb_tuning.path = 3) need their brick counters (4 B per brick
 // position) well inside the L2: up to 2^24 bricks (64 MB, a 1024^3 volume). They are
@@ -424,7 +424,7 @@ struct Plan {
     uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
     uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
     uint64_t o_k0 = 0, o_v0 = 0, o_k1 = 0, o_v1 = 0, o_bkey = 0, o_bmask = 0, o_bfirst = 0, o_bref = 0;
-    uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0, o_chunk_vstart = 0;
+    uint64_t o_grid = 0, o_grid_off = 0, o_grid_count = 0, o_chunk_vstart = 0, o_grid_super = 0;
     uint64_t o_bcount = 0, o_brec = 0, o_bloc = 0, o_bsum = 0;
     uint64_t o_set[2][7] = {};
     uint64_t o_cwords = 0, o_binst = 0, o_bdisp = 0;
@@ -619,6 +619,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_ostat[lv] = zl.take(uint64_t(p.otiles[lv]) * 8);
     }
     if (p.grid) p.o_grid = zl.take(grid_cells * 8);
+    if (d.grid_fold) p.o_grid_super = zl.take((uint64_t(d.grid_tiles) / 64 + 1) * 8);
     p.zero_bytes = align_up(zl.size, 256);
     Layout fl;  // 0xFF region follows
     fl.size = p.zero_bytes;
@@ -711,6 +712,7 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     if (p.grid || p.bucket) {
         d.grid_off = static_cast<uint64_t*>(at(p.o_grid_off));
         d.grid_count = static_cast<uint64_t*>(at(p.o_grid_count));
+        d.grid_super = static_cast<uint64_t*>(at(p.o_grid_super));
         d.chunk_vstart = static_cast<uint32_t*>(at(p.o_chunk_vstart));
     }
     if (p.grid) {

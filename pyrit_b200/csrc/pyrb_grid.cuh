@@ -33,6 +33,7 @@
 namespace pyrb {
 
 constexpr int kGridWarpBricks = 8;                          // bricks per warp and tile
+constexpr uint32_t kGridSuper = 64;                         // tiles per group sum (small grids)
 constexpr int kGridTileBricks = kWarps * kGridWarpBricks;   // 64 bricks = 4096 cells per tile
 
 __device__ __forceinline__ void red_max_u64(uint64_t* p, uint64_t v) {
@@ -242,8 +243,9 @@ __device__ __forceinline__ uint64_t block_scan_inplace(uint64_t* a, uint32_t T) 
 
 // Pass 1 of the compaction: voxels and non-empty bricks of every tile, packed
 // (voxels | bricks << 32) into grid_count[tile]. No dependency between tiles. On grids
-// of at most kGridFoldTiles tiles the last block to finish also does pass 2 (the
-// scan), which saves a launch and its wait.
+// of at most kGridFoldTiles tiles there is no pass 2: every tile's first voxel and
+// brick come from the sums of the kGridSuper-tile groups before it and the counts of
+// the tiles before it in its group, which the write pass adds up itself.
 // kBucket: the cells come from the brick buckets (sparse builds), else from the grid.
 template <bool kBucket>
 __global__ void __launch_bounds__(kBlock, 8) k_grid_count(BuildDesc d) {
@@ -269,26 +271,15 @@ __global__ void __launch_bounds__(kBlock, 8) k_grid_count(BuildDesc d) {
     }
     if (lane == 0) s_sum[warp] = uint64_t(vox) | (uint64_t(bricks) << 32);
     __syncthreads();
-    __shared__ uint32_t s_last;
     if (threadIdx.x == 0) {
         uint64_t t = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) t += s_sum[w];
         d.grid_count[tile] = t;
-        if (d.grid_fold) {
-            // the last block to finish scans every tile's count (no scan launch)
-            __threadfence();
-            s_last = atomicAdd(d.counters + kCtrTiles + kTileGridDone, 1u) == gridDim.x - 1;
-        }
-    }
-    if (!d.grid_fold) return;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const uint64_t total = block_scan_inplace<kBlock, 4>(d.grid_count, d.grid_tiles);
-    if (threadIdx.x == 0) {
-        d.counters[kCtrUnique] = uint32_t(total);
-        d.counters[kCtrBricks] = uint32_t(total >> 32);
+        // small grids: the sum of every kGridSuper tiles as well (the write pass adds
+        // those before its own and the counts in its own group: no scan)
+        if (d.grid_fold) atomicAdd(reinterpret_cast<unsigned long long*>(d.grid_super + tile / kGridSuper),
+                                   (unsigned long long)t);
     }
 }
 
@@ -312,6 +303,7 @@ template <bool kBucket>
 __global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     grid_dep_wait();
     __shared__ uint64_t s_sum[kWarps];
+    __shared__ uint64_t s_prefix;
     __shared__ uint32_t s_rcount[kMaxLeafRegions];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x;
@@ -335,7 +327,31 @@ __global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     }
     if (lane == 0) s_sum[warp] = uint64_t(vox) | (uint64_t(bricks) << 32);
     __syncthreads();
-    uint64_t wofs = d.grid_count[tile];  // the tile's first voxel | first brick << 32
+    uint64_t wofs;  // the tile's first voxel | first brick << 32
+    if (d.grid_fold) {
+        if (warp == 0) {
+            const uint32_t g = tile / kGridSuper, t0 = g * kGridSuper;
+            uint64_t x = 0;
+            for (uint32_t i = lane; i < g; i += 32) x += __ldcg(d.grid_super + i);
+            for (uint32_t i = t0 + lane; i < tile; i += 32) x += __ldcg(d.grid_count + i);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+            if (lane == 0) {
+                s_prefix = x;
+                if (tile == d.grid_tiles - 1) {  // the build's voxel and brick counts
+                    uint64_t t = x;
+#pragma unroll
+                    for (int w = 0; w < kWarps; ++w) t += s_sum[w];
+                    d.counters[kCtrUnique] = uint32_t(t);
+                    d.counters[kCtrBricks] = uint32_t(t >> 32);
+                }
+            }
+        }
+        __syncthreads();
+        wofs = s_prefix;
+    } else {
+        wofs = d.grid_count[tile];
+    }
 #pragma unroll
     for (int w = 0; w < kWarps; ++w)
         if (w < int(warp)) wofs += s_sum[w];

@@ -26,7 +26,7 @@ constexpr int kCtrUniqueLv = 64;   // + lv: U_lv
 constexpr int kCtrTiles = 96;      // dynamic tile counters, one per launch:
 constexpr int kCtrCount = 160;
 // ... disjoint ranges, so that no kernel of a build finds a counter another one advanced
-constexpr uint32_t kTileUnique = 0, kTileLeafOwn = 1, kTileLeafInsert = 2, kTileGridDone = 3;
+constexpr uint32_t kTileUnique = 0, kTileLeafOwn = 1, kTileLeafInsert = 2;
 constexpr uint32_t kTileLevel0 = 4;   // level lv: build 4 + 2 (lv - 2), owners 5 + 2 (lv - 2)
 constexpr uint32_t kTileSort0 = 44;   // sort pass p: 44 + p (8 passes at most: 64-bit keys take 8-bit digits)
 static_assert(kTileLevel0 + 2 * (20 - 2) + 1 < kTileSort0, "level counters below the sort's");
@@ -151,7 +151,8 @@ struct BuildDesc {
     uint64_t* grid;          // [grid_cells], zeroed before the build
     uint64_t* grid_off;      // [K + 1] first cell of every chunk (k_plan)
     uint64_t* grid_count;    // [grid_tiles] voxels | bricks << 32 per tile, then their exclusive scan
-    uint32_t grid_fold;      // the count pass's last block scans the counts (grid_tiles <= kGridFoldTiles)
+    uint32_t grid_fold;      // no scan pass (grid_tiles <= kGridFoldTiles): group sums, added up by the write pass
+    uint64_t* grid_super;    // grid_fold: [grid_tiles / 64 + 1] voxels | bricks << 32 of every 64 tiles (zeroed)
     uint32_t* chunk_vstart;  // [K] voxels before the first cell of every chunk (chunk builds)
 
     // Brick buckets of a sparse build (use_bucket): the entries of every brick position
