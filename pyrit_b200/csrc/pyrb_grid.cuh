@@ -318,6 +318,14 @@ __global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     } else {
         grid_load_attrs(d, wb0, nbricks, a0, a1);
     }
+    // small grids: warp 0 loads the group sums and counts before this tile now, while
+    // the cells are in flight (added up below)
+    uint64_t pre = 0;
+    if (d.grid_fold && warp == 0) {
+        const uint32_t g = tile / kGridSuper, t0 = g * kGridSuper;
+        for (uint32_t i = lane; i < g; i += 32) pre += __ldcg(d.grid_super + i);
+        for (uint32_t i = t0 + lane; i < tile; i += 32) pre += __ldcg(d.grid_count + i);
+    }
     uint32_t vox = 0, bricks = 0;
 #pragma unroll
     for (int k = 0; k < kGridWarpBricks; ++k) {
@@ -330,10 +338,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_grid_write(BuildDesc d) {
     uint64_t wofs;  // the tile's first voxel | first brick << 32
     if (d.grid_fold) {
         if (warp == 0) {
-            const uint32_t g = tile / kGridSuper, t0 = g * kGridSuper;
-            uint64_t x = 0;
-            for (uint32_t i = lane; i < g; i += 32) x += __ldcg(d.grid_super + i);
-            for (uint32_t i = t0 + lane; i < tile; i += 32) x += __ldcg(d.grid_count + i);
+            uint64_t x = pre;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
             if (lane == 0) {
