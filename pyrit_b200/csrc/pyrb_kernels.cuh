@@ -42,6 +42,26 @@ __device__ __forceinline__ uint32_t dyn_tile(uint32_t* counters, uint32_t ctr, u
     return t;
 }
 
+// The tile id and one counter word in one round trip: the load is issued before the
+// atomic's result is waited for.
+__device__ __forceinline__ uint32_t dyn_tile_and(uint32_t* counters, uint32_t ctr, uint32_t idx, uint32_t idx2,
+                                                 uint32_t* s_slot, uint32_t* val, uint32_t* val2) {
+    if (threadIdx.x == 0) {
+        const uint32_t v = counters[idx], v2 = counters[idx2];
+        s_slot[0] = atomicAdd(counters + kCtrTiles + ctr, 1u);
+        s_slot[1] = v;
+        s_slot[2] = v2;
+    }
+    __syncthreads();
+    const uint32_t t = s_slot[0];
+    *val = s_slot[1];
+    *val2 = s_slot[2];
+    __syncthreads();
+    return t;
+}
+
+// 6 tiles per SM for the small levels; large tiles keep their parent's references in
+// registers and take 5 (51 registers, no spills)
 // ---------------------------------------------------------------------------
 // Segment plan: first entry and first sort tile of every segment.
 // ---------------------------------------------------------------------------
@@ -1054,12 +1074,13 @@ __global__ void __launch_bounds__(kBlock) k_leaf_insert_regions(BuildDesc d) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_leaf_own(BuildDesc d) {
     grid_dep_wait();
-    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_tile[3];
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_base;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = dyn_tile(d.counters, kTileLeafOwn, &s_tile);
-    const uint32_t B = min(d.counters[kCtrBricks], d.brick_bound);
+    uint32_t bcount, unused;
+    const uint32_t tile = dyn_tile_and(d.counters, kTileLeafOwn, kCtrBricks, kCtrBricks, s_tile, &bcount, &unused);
+    const uint32_t B = min(bcount, d.brick_bound);
     const uint32_t ntiles = (B + kBrickTile - 1) / kBrickTile;
     if (tile >= ntiles) return;
     const uint32_t wstart = tile * kBrickTile + warp * 32 * kBrickIT;
@@ -1481,26 +1502,6 @@ __device__ __forceinline__ void node_build_tile(const BuildDesc& d, const LevelD
     }
 }
 
-// The tile id and one counter word in one round trip: the load is issued before the
-// atomic's result is waited for.
-__device__ __forceinline__ uint32_t dyn_tile_and(uint32_t* counters, uint32_t ctr, uint32_t idx, uint32_t idx2,
-                                                 uint32_t* s_slot, uint32_t* val, uint32_t* val2) {
-    if (threadIdx.x == 0) {
-        const uint32_t v = counters[idx], v2 = counters[idx2];
-        s_slot[0] = atomicAdd(counters + kCtrTiles + ctr, 1u);
-        s_slot[1] = v;
-        s_slot[2] = v2;
-    }
-    __syncthreads();
-    const uint32_t t = s_slot[0];
-    *val = s_slot[1];
-    *val2 = s_slot[2];
-    __syncthreads();
-    return t;
-}
-
-// 6 tiles per SM for the small levels; large tiles keep their parent's references in
-// registers and take 5 (51 registers, no spills)
 template <int NB>
 __global__ void __launch_bounds__(kBlock, NB == 1 ? 6 : 5) k_node_build(BuildDesc d, LevelDesc L) {
     grid_dep_wait();
