@@ -398,10 +398,10 @@ cudaError_t launch_sort_any(uint32_t rb, uint32_t it, const BuildDesc& d, cudaSt
 }
 
 // The default digit width and tile: 9-bit digits on 8192-entry tiles where they take
-// one pass less than 8-bit digits (25-27-bit sort keys: edge 256), else 8-bit digits
-// on 4096-entry tiles. Measured at 256^3 (value noise, 5.1 M entries): 3 passes of
-// 9 bits on 8192 entries 0.49-0.50 ms per build, 4 passes of 8 bits 0.52; 9 bits on
-// 4096 entries no faster than 8 bits.
+// one pass less than 8-bit digits (9 and 18 brick bits: edges 2^5 and 2^8), else 8-bit
+// digits on 4096-entry tiles. Measured on 25-bit keys (value noise, 5.1 M entries): 3
+// passes of 9 bits on 8192 entries 0.49-0.50 ms per build, 4 passes of 8 bits 0.52;
+// 9 bits on 4096 entries no faster than 8 bits.
 void auto_tuning(uint32_t sort_bits, uint32_t* rb, uint32_t* tile_keys) {
     const bool nine = (sort_bits + 8) / 9 < (sort_bits + 7) / 8;
     *rb = nine ? 9u : 8u;
@@ -495,7 +495,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     } else {
         rb = p.key64 ? 8u : g_radix_bits.load();
         tile_keys = p.key64 ? 2048u : g_tile_keys.load();
-        if (rb == 0) auto_tuning(lb + 1, &rb, &tile_keys);
+        if (rb == 0) auto_tuning(lb - 6, &rb, &tile_keys);
         lf = g_load_pct.load();
         path = g_path.load();
     }
@@ -526,13 +526,14 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     d.top = log2 - 1;
     d.chunked = p.chunked ? 1u : 0u;
 
-    // digit plan over lb + 1 bits (the invalid bit on top); none for the grid
-    const uint32_t sort_bits = lb + 1;
+    // digit plan over the brick bits 6 .. lb - 1 (k_unique resolves the cell bits and
+    // the invalid bit); none for the grid
+    const uint32_t sort_bits = lb - 6;
     const uint32_t passes = p.passes = (p.grid || p.bucket) ? 0 : (sort_bits + rb - 1) / rb;
     d.passes = passes;
     d.radix = passes ? 1u << rb : 0;
     if (passes) {
-        uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 0;
+        uint32_t base = sort_bits / passes, extra = sort_bits % passes, sh = 6;
         for (uint32_t q = 0; q < passes; ++q) {
             uint32_t b = base + (q < extra ? 1 : 0);
             d.pass_shift[q] = sh;

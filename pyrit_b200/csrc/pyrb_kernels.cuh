@@ -513,20 +513,22 @@ __global__ void __launch_bounds__(NT, PYRB_SORT_MIN_BLOCKS * kBlock / NT) k_sort
 }
 
 // ---------------------------------------------------------------------------
-// Unique voxels and bricks, one pass over the sorted entries.
-// Unique: the last entry of a run of equal keys decides; it is kept if it is valid
-// and its attribute is non-zero (gbuild.zig:366-388). Positions by a look-back over
-// the tiles in global (segment-major) order; keys get the segment (chunk) number
-// above bit lb, like packChunks; chunkFirst (:237-242).
-// Bricks (brickHeads/brickBuild, :394-428): runs of the kept keys with equal
-// key >> 6 -> (brick key, 64-bit mask, first voxel). A brick belongs to the tile
-// holding the first ENTRY (kept or not) of its run of equal key >> 6, a test on the
-// tile's own entries and the one before it; that tile reads ahead past its end while
-// the run goes on (a brick has at most 64 distinct keys). The tile's kept entries,
-// and those read ahead, are compacted in shared memory, its bricks counted there and
-// published for a second look-back, and each brick assembled by one thread.
+// Unique voxels and bricks, one pass over the entries ordered by brick.
+// The sort orders the entries by brick (key >> 6 with the invalid bit left out) and,
+// being stable, by entry index inside a brick; the 6 cell bits stay unsorted, which
+// saves a sort pass. Unique: the last entry of each key decides; it is kept if it is
+// valid and its attribute is non-zero (gbuild.zig:366-388). Bricks (brickHeads/
+// brickBuild, :394-428): the kept voxels of a brick give its 64-bit mask, and the
+// voxels are written in cell order at the brick's first voxel + the rank of their cell
+// in the mask, so the unique keys come out sorted as the reference's do. Positions by
+// look-backs over the tiles in global (segment-major) order; keys get the segment
+// (chunk) number above bit lb, like packChunks; chunkFirst (:237-242).
+// A brick's run of entries belongs to the tile holding its first entry. The tile
+// stages its entries in shared memory and finds the runs that start in it; one warp
+// reads past the tile's end while its last run goes on, keeping per cell the last
+// entry seen there. Each run is then taken by one thread, from its last entry back:
+// the first sighting of a cell is its last entry, the cell's winner.
 // ---------------------------------------------------------------------------
-constexpr int kUniqAhead = 64;  // kept keys read ahead: the distinct keys of one brick
 
 // Table region of a mask's home slot (see BuildDesc::leaf_regions).
 __device__ __forceinline__ uint32_t leaf_region(const BuildDesc& d, uint64_t mask) {
@@ -535,8 +537,7 @@ __device__ __forceinline__ uint32_t leaf_region(const BuildDesc& d, uint64_t mas
 
 template <int IT, typename KeyT>
 constexpr size_t unique_smem_bytes() {
-    constexpr size_t CAP = size_t(kBlock) * IT + kUniqAhead;
-    return CAP * (sizeof(KeyT) + 4 + 2);  // keys, values, brick heads
+    return size_t(kBlock) * IT * (sizeof(KeyT) + 2 + 2);  // keys, run starts, destinations
 }
 
 template <int IT, typename KeyT>
@@ -544,189 +545,244 @@ template <int IT, typename KeyT>
 // so more tiles in flight per SM measured 17 % faster than 4 at 64 registers
 __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin) {
     grid_dep_wait();
-    constexpr int TILE = kBlock * IT, CAP = TILE + kUniqAhead;
+    constexpr int TILE = kBlock * IT;
+    constexpr unsigned RA = kWarps - 1;  // the warp that reads past the tile's end
+    constexpr uint16_t kNoDst = 0xFFFF;
     extern __shared__ __align__(16) unsigned char usmem[];
-    KeyT* s_key = reinterpret_cast<KeyT*>(usmem);                 // [CAP] kept keys, tile order
-    uint32_t* s_val = reinterpret_cast<uint32_t*>(s_key + CAP);   // [CAP] their attributes
-    uint16_t* s_head = reinterpret_cast<uint16_t*>(s_val + CAP);  // [CAP] compacted index of each brick head
-    __shared__ uint32_t s_tile, s_extra;
+    KeyT* s_key = reinterpret_cast<KeyT*>(usmem);                  // [TILE] the tile's keys (+ zero flag)
+    uint16_t* s_head = reinterpret_cast<uint16_t*>(s_key + TILE);  // [TILE] first entry of each run
+    uint16_t* s_dst = s_head + TILE;                               // [TILE] a kept winner's place in the tile's voxels
+    __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
-    __shared__ uint64_t s_ubase, s_bbase;
+    __shared__ uint64_t s_ubase, s_bbase, s_tcells, s_tkeep;
     __shared__ KeyT s_lead;
+    __shared__ uint32_t s_tpos[64], s_tval[64];     // past the end: last entry (+1) and attribute per cell
     __shared__ uint32_t s_rcount[kMaxLeafRegions];  // the tile's bricks per leaf-table region
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // a sort tile larger than kBlock * IT entries is taken in parts, each a unique tile
-    const uint32_t parts = d.tile_keys / (kBlock * IT);
+    // a sort tile larger than TILE entries is taken in parts, each a unique tile
+    const uint32_t parts = d.tile_keys / TILE;
     const uint32_t tile = dyn_tile(d.counters, kTileUnique, &s_tile);
     const uint32_t ntiles = d.seg_tile[d.seg_count] * parts;
     if (tile >= ntiles) return;
     TileSpan sp = tile_span(d, tile / parts);
     {
-        const uint32_t skip = (tile % parts) * (kBlock * IT);
+        const uint32_t skip = (tile % parts) * TILE;
         sp.start += skip;
-        sp.count = sp.count > skip ? min(sp.count - skip, uint32_t(kBlock * IT)) : 0u;
+        sp.count = sp.count > skip ? min(sp.count - skip, uint32_t(TILE)) : 0u;
     }
     const uint32_t seg_begin = __ldg(d.seg_entry + sp.seg), seg_end = __ldg(d.seg_entry + sp.seg + 1);
+    const uint32_t e_end = sp.start + sp.count;
     const KeyT* keys = static_cast<const KeyT*>(d.kbuf[fin]);
     const uint32_t* vals = d.vbuf[fin];
     const KeyT inv = KeyT(1) << d.lb;
-    const KeyT NONE = ~KeyT(0);  // never the brick of a key: key >> 6 has its top 6 bits clear
+    const KeyT zero = KeyT(1) << (d.lb + 1);  // staged keys: the entry's attribute is 0 (a free bit)
+    const KeyT bbits = (KeyT(1) << (d.lb - 6)) - 1;
+    const KeyT NONE = ~KeyT(0);  // never a brick: bricks have at most lb - 6 bits
+    auto brick = [&](KeyT k) -> KeyT { return (k >> 6) & bbits; };
     const uint32_t wbase = warp * 32 * IT;
     const bool regions = d.leaf_regions > 1;
     if (threadIdx.x < kMaxLeafRegions) s_rcount[threadIdx.x] = 0;
 
-    uint32_t total;
+    // the read-ahead warp's first loads go out with the tile's: the entry before the
+    // tile and the 32 after it (a tile short of TILE entries ends its segment)
+    KeyT lead = NONE, ra_k = NONE;
+    uint32_t ra_v = 0;
+    if (warp == RA) {
+        s_tpos[lane] = 0;
+        s_tpos[lane + 32] = 0;
+        if (sp.count > 0 && sp.start > seg_begin) lead = brick(keys[sp.start - 1]);
+        if (sp.count > 0 && e_end + lane < seg_end) {
+            ra_k = keys[e_end + lane];
+            ra_v = vals[e_end + lane];
+        }
+    }
+    uint32_t v[IT];  // the attributes stay in registers until the voxels are written
     {
         KeyT k[IT];
-        uint32_t v[IT];
-        unsigned keepb[IT];
-        uint32_t wcount = 0;
-        // all loads first (no shuffle between them), then the run-end tests
 #pragma unroll
         for (int j = 0; j < IT; ++j) {
-            uint32_t idx = wbase + j * 32 + lane;
-            bool in = idx < sp.count;
-            uint32_t e = sp.start + idx;
-            k[j] = in ? keys[e] : inv;
-            v[j] = in ? vals[e] : 0;
+            const uint32_t idx = wbase + j * 32 + lane;
+            const bool in = idx < sp.count;
+            k[j] = in ? keys[sp.start + idx] : KeyT(0);
+            v[j] = in ? vals[sp.start + idx] : 0u;
         }
 #pragma unroll
         for (int j = 0; j < IT; ++j) {
-            uint32_t idx = wbase + j * 32 + lane;
-            bool in = idx < sp.count;
-            uint32_t e = sp.start + idx;
-            // successor key: lane + 1 of this row, lane 0 of the next row (every lane shuffles)
-            const KeyT down = __shfl_down_sync(kFull, k[j], 1);
-            const KeyT row_next = __shfl_sync(kFull, k[j + 1 < IT ? j + 1 : j], 0);
-            KeyT nk = lane < 31 ? down : row_next;
-            if ((lane == 31 && j + 1 == IT) || idx + 1 >= sp.count) nk = (in && e + 1 < seg_end) ? keys[e + 1] : ~KeyT(0);
-            bool last = !in ? false : (e + 1 == seg_end || nk != k[j]);
-            bool keep = in && last && !(k[j] & inv) && v[j] != 0;
-            keepb[j] = __ballot_sync(kFull, keep);
-            wcount += __popc(keepb[j]);
-        }
-        uint32_t wexcl = block_excl_scan(lane == 0 ? wcount : 0, s_scan, &total);
-        wexcl = __shfl_sync(kFull, wexcl, 0);
-        // kept entries compacted in tile order
-        uint32_t run = 0;
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            if ((keepb[j] >> lane) & 1) {
-                const uint32_t p = wexcl + run + __popc(keepb[j] & lanemask_lt());
-                s_key[p] = k[j];
-                s_val[p] = v[j];
+            const uint32_t idx = wbase + j * 32 + lane;
+            if (idx < sp.count) {
+                s_key[idx] = k[j] | (v[j] == 0 ? zero : KeyT(0));
+                s_dst[idx] = kNoDst;
             }
-            run += __popc(keepb[j]);
         }
-    }
-    if (threadIdx.x == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | total);
-    if (warp == kWarps - 1) {
-        // the brick run of the entry before the tile (bricks of that run belong to an
-        // earlier tile); the tile's last run, if it started here, read on past the end
-        const KeyT lead = (sp.count > 0 && sp.start > seg_begin) ? KeyT(keys[sp.start - 1] >> 6) : NONE;
-        uint32_t extra = 0;
-        if (sp.count > 0) {
-            const uint32_t e_last = sp.start + sp.count - 1;
-            const KeyT klast = keys[e_last];
-            const KeyT rb = klast >> 6;
-            if (!(klast & inv) && rb != lead && e_last + 1 < seg_end) {
-                bool more = true;
-                for (uint32_t base = e_last + 1; more && base < seg_end; base += 32) {
+        if (warp == RA) {
+            // the tile's last run, if it started here, may go on past the end (only a
+            // full tile can have entries after it: its last entry is this lane 31's)
+            const KeyT klast = __shfl_sync(kFull, k[IT - 1], 31);
+            __syncwarp();  // the cleared s_tpos before any lane's atomicMax
+            if (sp.count > 0 && e_end < seg_end && brick(klast) != lead) {
+                const KeyT rb = brick(klast);
+                uint32_t base = e_end;
+                KeyT kk = ra_k;
+                uint32_t vv = ra_v;
+                while (true) {
                     const uint32_t e = base + lane;
-                    const KeyT ke = e < seg_end ? keys[e] : NONE;
-                    const bool in_run = e < seg_end && KeyT(ke >> 6) == rb;
-                    bool keep = false;
-                    uint32_t ve = 0;
-                    if (in_run) {
-                        const KeyT kn = e + 1 < seg_end ? keys[e + 1] : NONE;
-                        ve = vals[e];
-                        keep = (e + 1 == seg_end || kn != ke) && ve != 0;
-                    }
-                    const unsigned kb = __ballot_sync(kFull, keep);
-                    if (keep) {
-                        const uint32_t p = extra + __popc(kb & lanemask_lt());
-                        if (p < uint32_t(kUniqAhead)) {
-                            s_key[total + p] = ke;
-                            s_val[total + p] = ve;
-                        } else {
-                            atomicOr(d.counters + kCtrError, kErrBound);
-                        }
-                    }
-                    extra = min(extra + __popc(kb), uint32_t(kUniqAhead));
-                    more = __all_sync(kFull, in_run);
+                    const bool in_run = e < seg_end && brick(kk) == rb;
+                    const bool use = in_run && !(kk & inv);
+                    const uint32_t p = e - e_end + 1, c = uint32_t(kk) & 63;
+                    if (use) atomicMax(s_tpos + c, p);
+                    __syncwarp();
+                    if (use && s_tpos[c] == p) s_tval[c] = vv;  // the cell's last entry so far
+                    __syncwarp();
+                    if (!__all_sync(kFull, in_run)) break;
+                    base += 32;
+                    const uint32_t e2 = base + lane;
+                    kk = e2 < seg_end ? keys[e2] : NONE;
+                    vv = e2 < seg_end ? vals[e2] : 0u;
                 }
             }
+            const uint32_t pa = s_tpos[lane], pb = s_tpos[lane + 32];
+            const unsigned ca = __ballot_sync(kFull, pa != 0), cb = __ballot_sync(kFull, pb != 0);
+            const unsigned ka = __ballot_sync(kFull, pa != 0 && s_tval[lane] != 0);
+            const unsigned kb = __ballot_sync(kFull, pb != 0 && s_tval[lane + 32] != 0);
+            if (lane == 0) {
+                s_tcells = uint64_t(cb) << 32 | ca;
+                s_tkeep = uint64_t(kb) << 32 | ka;
+                s_lead = lead;
+            }
         }
-        if (lane == 0) { s_extra = extra; s_lead = lead; }
     }
     __syncthreads();
-    // brick heads over the compacted entries: a key whose brick differs from the
-    // previous kept key's (the first one: from the brick of the entry before the tile)
-    const uint32_t M = total + s_extra;
-    const KeyT lead = s_lead;
-    const uint32_t ch = ((M + kWarps - 1) / kWarps + 31) & ~31u;  // entries per warp, whole rows
-    const uint32_t w_lo = min(warp * ch, M), w_hi = min(w_lo + ch, M);
-    uint32_t wheads = 0;
-    for (uint32_t i0 = w_lo; i0 < w_hi; i0 += 32) {
-        const uint32_t i = i0 + lane;
-        const bool head = i < w_hi && KeyT(s_key[i] >> 6) != (i == 0 ? lead : KeyT(s_key[i - 1] >> 6));
-        wheads += __popc(__ballot_sync(kFull, head));
-    }
-    uint32_t btotal;
-    uint32_t hexcl = block_excl_scan(lane == 0 ? wheads : 0, s_scan, &btotal);
-    hexcl = __shfl_sync(kFull, hexcl, 0);
-    if (threadIdx.x == 0 && tile != 0) st_relaxed(d.brick_status + tile, kFlagAgg | btotal);
-    for (uint32_t i0 = w_lo; i0 < w_hi; i0 += 32) {
-        const uint32_t i = i0 + lane;
-        const bool head = i < w_hi && KeyT(s_key[i] >> 6) != (i == 0 ? lead : KeyT(s_key[i - 1] >> 6));
-        const unsigned hb = __ballot_sync(kFull, head);
-        if (head) s_head[hexcl + __popc(hb & lanemask_lt())] = uint16_t(i);
-        hexcl += __popc(hb);
+    // runs that start in the tile: an entry whose brick differs from the one before it
+    uint32_t R;
+    {
+        const KeyT lead_b = s_lead;
+        unsigned hb[IT];
+        uint32_t wheads = 0;
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            const uint32_t idx = wbase + j * 32 + lane;
+            bool head = false;
+            if (idx < sp.count) head = brick(s_key[idx]) != (idx == 0 ? lead_b : brick(s_key[idx - 1]));
+            hb[j] = __ballot_sync(kFull, head);
+            wheads += __popc(hb[j]);
+        }
+        uint32_t hexcl = block_excl_scan(lane == 0 ? wheads : 0u, s_scan, &R);
+        hexcl = __shfl_sync(kFull, hexcl, 0);
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            if ((hb[j] >> lane) & 1) s_head[hexcl + __popc(hb[j] & lanemask_lt())] = uint16_t(wbase + j * 32 + lane);
+            hexcl += __popc(hb[j]);
+        }
     }
     __syncthreads();
-    // positions are global over all segments: warps 0 and 1 look back to tile 0 for
-    // the voxel and the brick offsets while the others assemble the first two rounds
-    // of brick masks
-    auto brick_mask = [&](uint32_t b, uint32_t& lo) -> uint64_t {
-        lo = s_head[b];
-        const uint32_t hi = b + 1 < btotal ? s_head[b + 1] : M;
-        uint64_t mask = 0;
-        for (uint32_t i = lo; i < hi; ++i) mask |= 1ull << (uint32_t(s_key[i]) & 63);
-        return mask;
+    // kept cells of each run (thread t takes runs [t q, t q + q)); the last run starts
+    // from the cells seen past the tile's end
+    const uint64_t tcells = s_tcells, tkeep = s_tkeep;
+    const uint32_t q = (R + kBlock - 1) / kBlock;
+    const uint32_t r_lo = min(threadIdx.x * q, R), r_hi = min(r_lo + q, R);
+    auto run_end = [&](uint32_t r) -> uint32_t { return r + 1 < R ? uint32_t(s_head[r + 1]) : sp.count; };
+    auto run_mask = [&](uint32_t r, uint32_t lo, uint32_t hi) -> uint64_t {
+        uint64_t seen = r + 1 == R ? tcells : 0, km = r + 1 == R ? tkeep : 0;
+        for (uint32_t i = hi; i-- > lo;) {
+            const KeyT k = s_key[i];
+            if (k & inv) continue;
+            const uint64_t bit = 1ull << (uint32_t(k) & 63);
+            if (!(seen & bit)) {
+                seen |= bit;
+                if (!(k & zero)) km |= bit;
+            }
+        }
+        return km;
     };
+    uint64_t m0 = 0, m1 = 0;  // the masks of the thread's first two runs, kept for the second walk
+    uint32_t packed = 0;      // kept voxels << 16 | bricks
+    for (uint32_t r = r_lo; r < r_hi; ++r) {
+        const uint64_t km = run_mask(r, s_head[r], run_end(r));
+        if (r == r_lo) m0 = km;
+        else if (r == r_lo + 1) m1 = km;
+        packed += (uint32_t(__popcll(km)) << 16) + (km != 0 ? 1u : 0u);
+    }
+    uint32_t ptotal;
+    const uint32_t pexcl = block_excl_scan(packed, s_scan, &ptotal);
+    const uint32_t total = ptotal >> 16, btotal = ptotal & 0xFFFFu;
+    if (threadIdx.x == 0 && tile != 0) {
+        st_relaxed(d.uniq_status + tile, kFlagAgg | total);
+        st_relaxed(d.brick_status + tile, kFlagAgg | btotal);
+    }
+    // positions are global over all segments: warps 0 and 1 look back to tile 0 for
+    // the voxel and the brick offsets while the others place the winners
     if (warp == 0) {
-        uint64_t ex = lookback_warp(d.uniq_status, tile, 0, total, d.counters + kCtrError);
+        const uint64_t ex = lookback_warp(d.uniq_status, tile, 0, total, d.counters + kCtrError);
         if (lane == 0) s_ubase = ex;
     } else if (warp == 1) {
-        uint64_t ex = lookback_warp(d.brick_status, tile, 0, btotal, d.counters + kCtrError);
+        const uint64_t ex = lookback_warp(d.brick_status, tile, 0, btotal, d.counters + kCtrError);
         if (lane == 0) s_bbase = ex;
     }
-    uint32_t lo0 = 0, lo1 = 0;
-    const uint32_t b0 = threadIdx.x, b1 = threadIdx.x + kBlock;
-    const uint64_t m0 = b0 < btotal ? brick_mask(b0, lo0) : 0, m1 = b1 < btotal ? brick_mask(b1, lo1) : 0;
+    // each kept cell's winner goes to the rank of its cell in the brick's mask
+    {
+        uint32_t uo = pexcl >> 16;
+        for (uint32_t r = r_lo; r < r_hi; ++r) {
+            const uint32_t lo = s_head[r], hi = run_end(r);
+            const uint64_t km = r == r_lo ? m0 : r == r_lo + 1 ? m1 : run_mask(r, lo, hi);
+            if (km == 0) continue;
+            uint64_t seen = r + 1 == R ? tcells : 0;
+            for (uint32_t i = hi; i-- > lo;) {
+                const KeyT k = s_key[i];
+                if (k & inv) continue;
+                const uint64_t bit = 1ull << (uint32_t(k) & 63);
+                if (!(seen & bit)) {
+                    seen |= bit;
+                    if (km & bit) s_dst[i] = uint16_t(uo + __popcll(km & (bit - 1)));
+                }
+            }
+            uo += uint32_t(__popcll(km));
+        }
+    }
     __syncthreads();
     const uint64_t ubase = s_ubase, bbase = s_bbase;
     const uint64_t segbits = uint64_t(sp.seg) << d.lb;
-    for (uint32_t i = threadIdx.x; i < total; i += kBlock) {
-        const uint64_t pos = ubase + i;
+    auto put = [&](uint64_t pos, uint64_t key, uint32_t val) {
         if (pos < d.n_total) {
-            d.ukey[pos] = segbits | uint64_t(s_key[i]);
-            d.uval[pos] = s_val[i];
+            d.ukey[pos] = key;
+            d.uval[pos] = val;
         } else {
             atomicOr(d.counters + kCtrError, kErrBound);
         }
+    };
+    // the voxels, in the tile's entry order (a row's winners land close together)
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+        const uint32_t idx = wbase + j * 32 + lane;
+        if (idx < sp.count) {
+            const uint32_t dst = s_dst[idx];
+            if (dst != kNoDst) put(ubase + dst, segbits | uint64_t(s_key[idx]), v[j]);
+        }
     }
-    for (uint32_t b = threadIdx.x; b < btotal; b += kBlock) {
-        uint32_t lo;
-        const uint64_t mask = b == b0 ? (lo = lo0, m0) : b == b1 ? (lo = lo1, m1) : brick_mask(b, lo);
-        const uint64_t g = bbase + b;
-        if (g < d.brick_bound) {
-            d.bkey[g] = (segbits | uint64_t(s_key[lo])) >> 6;
-            d.bmask[g] = mask;
-            d.bfirst[g] = uint32_t(ubase + lo);
-            if (regions) atomicAdd(&s_rcount[leaf_region(d, mask)], 1u);
-        } else {
-            atomicOr(d.counters + kCtrError, kErrBound);
+    // the bricks, and the last run's winners found past the tile's end
+    {
+        uint32_t uo = pexcl >> 16, bo = pexcl & 0xFFFFu;
+        for (uint32_t r = r_lo; r < r_hi; ++r) {
+            const uint32_t lo = s_head[r];
+            const uint64_t km = r == r_lo ? m0 : r == r_lo + 1 ? m1 : run_mask(r, lo, run_end(r));
+            if (km == 0) continue;
+            const uint64_t bk = uint64_t(brick(s_key[lo]));
+            const uint64_t first = ubase + uo, g = bbase + bo;
+            if (g < d.brick_bound) {
+                d.bkey[g] = (segbits >> 6) | bk;
+                d.bmask[g] = km;
+                d.bfirst[g] = uint32_t(first);
+                if (regions) atomicAdd(&s_rcount[leaf_region(d, km)], 1u);
+            } else {
+                atomicOr(d.counters + kCtrError, kErrBound);
+            }
+            if (r + 1 == R) {
+                for (uint64_t t = tkeep; t; t &= t - 1) {
+                    const uint32_t c = uint32_t(__ffsll(t) - 1);
+                    put(first + __popcll(km & ((1ull << c) - 1)), segbits | bk << 6 | c, s_tval[c]);
+                }
+            }
+            uo += uint32_t(__popcll(km));
+            ++bo;
         }
     }
     if (regions) {
