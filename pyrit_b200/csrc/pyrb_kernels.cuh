@@ -555,7 +555,6 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps + 2];
     __shared__ uint64_t s_ubase, s_bbase, s_tcells, s_tkeep;
-    __shared__ KeyT s_lead;
     __shared__ uint32_t s_tpos[64], s_tval[64];     // past the end: last entry (+1) and attribute per cell
     __shared__ uint32_t s_rcount[kMaxLeafRegions];  // the tile's bricks per leaf-table region
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -597,8 +596,13 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
         }
     }
     uint32_t v[IT];  // the attributes stay in registers until the voxels are written
+    unsigned hb[IT];  // runs that start in the tile: an entry whose brick differs from the one before it
+    uint32_t wheads = 0;
     {
         KeyT k[IT];
+        // the entry before the warp's first (lane 0): the tile's lead or the previous warp's last
+        KeyT kprev = NONE;
+        if (lane == 0 && wbase < sp.count && (wbase > 0 || sp.start > seg_begin)) kprev = brick(keys[sp.start + wbase - 1]);
 #pragma unroll
         for (int j = 0; j < IT; ++j) {
             const uint32_t idx = wbase + j * 32 + lane;
@@ -609,7 +613,13 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
 #pragma unroll
         for (int j = 0; j < IT; ++j) {
             const uint32_t idx = wbase + j * 32 + lane;
-            if (idx < sp.count) {
+            const bool in = idx < sp.count;
+            const KeyT up = __shfl_up_sync(kFull, k[j], 1);
+            const KeyT row_prev = __shfl_sync(kFull, j > 0 ? k[j > 0 ? j - 1 : 0] : k[0], 31);
+            const KeyT pb = lane > 0 ? brick(up) : j > 0 ? brick(row_prev) : kprev;
+            hb[j] = __ballot_sync(kFull, in && brick(k[j]) != pb);
+            wheads += __popc(hb[j]);
+            if (in) {
                 s_key[idx] = k[j] | (v[j] == 0 ? zero : KeyT(0));
                 s_dst[idx] = kNoDst;
             }
@@ -647,25 +657,11 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
             if (lane == 0) {
                 s_tcells = uint64_t(cb) << 32 | ca;
                 s_tkeep = uint64_t(kb) << 32 | ka;
-                s_lead = lead;
             }
         }
     }
-    __syncthreads();
-    // runs that start in the tile: an entry whose brick differs from the one before it
     uint32_t R;
     {
-        const KeyT lead_b = s_lead;
-        unsigned hb[IT];
-        uint32_t wheads = 0;
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            const uint32_t idx = wbase + j * 32 + lane;
-            bool head = false;
-            if (idx < sp.count) head = brick(s_key[idx]) != (idx == 0 ? lead_b : brick(s_key[idx - 1]));
-            hb[j] = __ballot_sync(kFull, head);
-            wheads += __popc(hb[j]);
-        }
         uint32_t hexcl = block_excl_scan(lane == 0 ? wheads : 0u, s_scan, &R);
         hexcl = __shfl_sync(kFull, hexcl, 0);
 #pragma unroll
@@ -681,17 +677,25 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     const uint32_t q = (R + kBlock - 1) / kBlock;
     const uint32_t r_lo = min(threadIdx.x * q, R), r_hi = min(r_lo + q, R);
     auto run_end = [&](uint32_t r) -> uint32_t { return r + 1 < R ? uint32_t(s_head[r + 1]) : sp.count; };
-    auto run_mask = [&](uint32_t r, uint32_t lo, uint32_t hi) -> uint64_t {
-        uint64_t seen = r + 1 == R ? tcells : 0, km = r + 1 == R ? tkeep : 0;
-        for (uint32_t i = hi; i-- > lo;) {
-            const KeyT k = s_key[i];
-            if (k & inv) continue;
-            const uint64_t bit = 1ull << (uint32_t(k) & 63);
-            if (!(seen & bit)) {
+    // a run from its last entry back, 4 entries a step (their loads in flight together);
+    // visit(i, first_sighting_bit, k) for each entry
+    auto walk = [&](uint32_t lo, uint32_t hi, uint64_t seen, auto&& visit) {
+        for (uint32_t i = hi; i > lo; i = i > lo + 4 ? i - 4 : lo) {
+            KeyT kq[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) kq[u] = i > lo + u ? s_key[i - 1 - u] : inv;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint64_t bit = (kq[u] & inv) ? 0ull : 1ull << (uint32_t(kq[u]) & 63);
+                const uint64_t nb = bit & ~seen;
                 seen |= bit;
-                if (!(k & zero)) km |= bit;
+                visit(i - 1 - u, nb, kq[u]);
             }
         }
+    };
+    auto run_mask = [&](uint32_t r, uint32_t lo, uint32_t hi) -> uint64_t {
+        uint64_t km = r + 1 == R ? tkeep : 0;
+        walk(lo, hi, r + 1 == R ? tcells : 0, [&](uint32_t, uint64_t nb, KeyT k) { km |= (k & zero) ? 0ull : nb; });
         return km;
     };
     uint64_t m0 = 0, m1 = 0;  // the masks of the thread's first two runs, kept for the second walk
@@ -725,16 +729,9 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
             const uint32_t lo = s_head[r], hi = run_end(r);
             const uint64_t km = r == r_lo ? m0 : r == r_lo + 1 ? m1 : run_mask(r, lo, hi);
             if (km == 0) continue;
-            uint64_t seen = r + 1 == R ? tcells : 0;
-            for (uint32_t i = hi; i-- > lo;) {
-                const KeyT k = s_key[i];
-                if (k & inv) continue;
-                const uint64_t bit = 1ull << (uint32_t(k) & 63);
-                if (!(seen & bit)) {
-                    seen |= bit;
-                    if (km & bit) s_dst[i] = uint16_t(uo + __popcll(km & (bit - 1)));
-                }
-            }
+            walk(lo, hi, r + 1 == R ? tcells : 0, [&](uint32_t i, uint64_t nb, KeyT) {
+                if (nb & km) s_dst[i] = uint16_t(uo + __popcll(km & (nb - 1)));
+            });
             uo += uint32_t(__popcll(km));
         }
     }
