@@ -351,7 +351,8 @@ void fill_stats(const uint32_t* ctr, const uint32_t* meta) {
 template <int RB, int IT, typename KeyT = uint32_t>
 cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
     constexpr int NT = IT > 16 ? 2 * kBlock : kBlock, SIT = IT * kBlock / NT;
-    constexpr uint32_t parts = uint32_t(IT / SIT);  // unique tiles per sort tile
+    constexpr int UIT = SIT < kUniqIT ? SIT : kUniqIT;
+    constexpr uint32_t parts = uint32_t(IT / UIT);  // unique tiles per sort tile
     const size_t hist_smem = size_t(d.passes) * (1u << RB) * 4;
     const size_t sort_smem = sort_smem_bytes<RB, SIT, KeyT, NT>();
     static std::once_flag once;
@@ -359,7 +360,7 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
         cudaFuncSetAttribute(k_encode_hist<RB, IT, KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
         cudaFuncSetAttribute(k_sort_pass<RB, SIT, KeyT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
         cudaFuncSetAttribute(k_sort_pass<RB, SIT, KeyT, NT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_unique<SIT, KeyT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_unique<UIT, KeyT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     });
     launch(k_encode_hist<RB, IT, KeyT>, d.sort_tiles, kBlock, hist_smem, st, d);
     prof.mark("encode_hist");
@@ -369,7 +370,7 @@ cudaError_t launch_sort(const BuildDesc& d, cudaStream_t st, Prof& prof) {
         launch(k_sort_pass<RB, SIT, KeyT, NT>, d.sort_tiles, NT, sort_smem, st, d, p, p & 1);
         prof.mark("sort_pass", p);
     }
-    launch(k_unique<SIT, KeyT>, d.sort_tiles * parts, kBlock, unique_smem_bytes<SIT, KeyT>(), st, d, d.passes & 1);
+    launch(k_unique<UIT, KeyT>, d.sort_tiles * parts, kBlock, unique_smem_bytes<UIT, KeyT>(), st, d, d.passes & 1);
     prof.mark("unique_brick");
     return cudaGetLastError();
 }
@@ -566,7 +567,7 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
     }
     if (words >= (uint64_t(1) << 32)) return fail(PYRB_ERROR_INVALID_ARGUMENT, "node buffer bound exceeds 2^32 words");
     d.brick_bound = B;
-    d.brick_tiles = d.sort_tiles * std::max(1u, tile_keys / 4096u);  // the unique tiles
+    d.brick_tiles = d.sort_tiles * std::max(1u, tile_keys / uint32_t(kBlock * kUniqIT));  // the unique tiles
     d.leafown_tiles = std::max((B + kBrickTile - 1) / kBrickTile, 1u);
     if ((uint64_t(B) * 100 + lf - 1) / lf > (uint64_t(1) << 31))
         return fail(PYRB_ERROR_INVALID_ARGUMENT, "brick bound exceeds the leaf table's 2^31 slots");

@@ -540,6 +540,10 @@ constexpr size_t unique_smem_bytes() {
     return size_t(kBlock) * IT * (sizeof(KeyT) + 2 + 2);  // keys, run starts, destinations
 }
 
+// Unique tiles of kBlock * kUniqIT entries (4096; a larger sort tile is taken in parts):
+// 2048-entry tiles at 5, 6 or 7 per SM measured 8-14 % slower, the fixed cost of a
+// tile (scans, look-backs) being paid twice as often.
+constexpr int kUniqIT = 16;
 template <int IT, typename KeyT>
 // 5 tiles per SM (48 registers): the tile mostly waits for its predecessors' counts,
 // so more tiles in flight per SM measured 17 % faster than 4 at 64 registers
