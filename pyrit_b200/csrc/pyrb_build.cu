@@ -420,7 +420,7 @@ struct Plan {
     uint32_t P[kMaxLevels + 2] = {};
     uint32_t cap[kMaxLevels + 2] = {}, btiles[kMaxLevels + 2] = {}, otiles[kMaxLevels + 2] = {};
     uint32_t bnb[kMaxLevels + 2] = {}, oit[kMaxLevels + 2] = {};
-    uint64_t o_counters = 0, o_hist = 0, o_sort_status = 0, o_uniq_status = 0, o_brick_status = 0,
+    uint64_t o_counters = 0, o_hist = 0, o_sort_status = 0, o_uniq_status = 0,
              o_leafown_status = 0, o_leaf_table = 0, o_regions = 0;
     uint64_t o_table[kMaxLevels + 2] = {}, o_bstat[kMaxLevels + 2] = {}, o_ostat[kMaxLevels + 2] = {};
     uint64_t o_chunk_first = 0, o_roots = 0, o_prim_start = 0, o_seg_entry = 0, o_seg_tile = 0;
@@ -600,7 +600,6 @@ pyrb_result plan_build(const Job& job, const Tune* fixed, Plan& p) {
         p.o_hist = zl.take(uint64_t(K) * passes * d.radix * 4);
         p.o_sort_status = zl.take(uint64_t(passes) * d.sort_tiles * d.radix * 8);
         p.o_uniq_status = zl.take(uint64_t(d.brick_tiles) * 8);
-        p.o_brick_status = zl.take(uint64_t(d.brick_tiles) * 8);
     }
     p.o_leafown_status = zl.take(uint64_t(d.leafown_tiles) * 8);
     p.o_binst = zl.take(uint64_t(B));
@@ -702,7 +701,6 @@ void bind_plan(Plan& p, uint64_t scratch, const uint64_t outs[6], const Job& job
     d.hist = static_cast<uint32_t*>(at(p.o_hist));
     d.sort_status = static_cast<uint64_t*>(at(p.o_sort_status));
     d.uniq_status = static_cast<uint64_t*>(at(p.o_uniq_status));
-    d.brick_status = static_cast<uint64_t*>(at(p.o_brick_status));
     d.leafown_status = static_cast<uint64_t*>(at(p.o_leafown_status));
     d.leaf_table = static_cast<uint4*>(at(p.o_leaf_table));
     d.region_count = static_cast<uint32_t*>(at(p.o_regions));

@@ -98,15 +98,14 @@ struct BuildDesc {
     uint32_t* vbuf[2];
 
     // unique voxels (outputs)
-    uint64_t* uniq_status;   // [sort_tiles]
+    uint64_t* uniq_status;   // [brick_tiles]: voxels << 31 | bricks of each unique tile
     uint64_t* ukey;
     uint32_t* uval;
     uint32_t* chunk_first;   // [K], 0xFFFFFFFF initialised
 
     // bricks + leaves
     uint32_t brick_bound;
-    uint32_t brick_tiles;
-    uint64_t* brick_status;  // [brick_tiles]: the unique tiles count bricks too
+    uint32_t brick_tiles;    // unique tiles (a sort tile of more than 4096 entries is taken in parts)
     uint64_t* bkey;
     uint64_t* bmask;
     uint32_t* bfirst;

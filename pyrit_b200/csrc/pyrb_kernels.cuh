@@ -675,11 +675,13 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
         }
     }
     __syncthreads();
-    // kept cells of each run (thread t takes runs [t q, t q + q)); the last run starts
-    // from the cells seen past the tile's end
+    // kept cells of each run (thread t of the first kRunThreads takes runs [t q, t q + q);
+    // the last warp is left free for the look-back); the last run starts from the cells
+    // seen past the tile's end
+    constexpr uint32_t kRunThreads = kBlock - 32;
     const uint64_t tcells = s_tcells, tkeep = s_tkeep;
-    const uint32_t q = (R + kBlock - 1) / kBlock;
-    const uint32_t r_lo = min(threadIdx.x * q, R), r_hi = min(r_lo + q, R);
+    const uint32_t q = (R + kRunThreads - 1) / kRunThreads;
+    const uint32_t r_lo = threadIdx.x < kRunThreads ? min(threadIdx.x * q, R) : R, r_hi = min(r_lo + q, R);
     auto run_end = [&](uint32_t r) -> uint32_t { return r + 1 < R ? uint32_t(s_head[r + 1]) : sp.count; };
     // a run from its last entry back, 4 entries a step (their loads in flight together);
     // visit(i, first_sighting_bit, k) for each entry
@@ -713,18 +715,18 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     uint32_t ptotal;
     const uint32_t pexcl = block_excl_scan(packed, s_scan, &ptotal);
     const uint32_t total = ptotal >> 16, btotal = ptotal & 0xFFFFu;
-    if (threadIdx.x == 0 && tile != 0) {
-        st_relaxed(d.uniq_status + tile, kFlagAgg | total);
-        st_relaxed(d.brick_status + tile, kFlagAgg | btotal);
-    }
-    // positions are global over all segments: warps 0 and 1 look back to tile 0 for
-    // the voxel and the brick offsets while the others place the winners
-    if (warp == 0) {
-        const uint64_t ex = lookback_warp(d.uniq_status, tile, 0, total, d.counters + kCtrError);
-        if (lane == 0) s_ubase = ex;
-    } else if (warp == 1) {
-        const uint64_t ex = lookback_warp(d.brick_status, tile, 0, btotal, d.counters + kCtrError);
-        if (lane == 0) s_bbase = ex;
+    // positions are global over all segments: the last warp publishes the tile's voxel
+    // and brick counts as one status word (voxels << 31 | bricks: both stay below 2^31)
+    // and looks back to tile 0 for both offsets at once, while the others place the
+    // winners
+    if (warp == kWarps - 1) {
+        const uint64_t agg = uint64_t(total) << 31 | btotal;
+        if (lane == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | agg);
+        const uint64_t ex = lookback_warp(d.uniq_status, tile, 0, agg, d.counters + kCtrError);
+        if (lane == 0) {
+            s_ubase = ex >> 31;
+            s_bbase = ex & 0x7FFFFFFFull;
+        }
     }
     // each kept cell's winner goes to the rank of its cell in the brick's mask
     {
