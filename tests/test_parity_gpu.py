@@ -232,6 +232,33 @@ def test_brick_runs_all_deleted(gb):
     assert_same_build(gb.build(5, 3, dev(pts)).download(), orc.gb_build(5, 3, pts), label="all deleted")
 
 
+@pytest.mark.parametrize("tuning", [(8, 4096), (9, 8192), (8, 1024)])
+def test_brick_runs_with_interleaved_cells(gb, tuning):
+    """The sort orders bricks only, so a brick's run keeps its entries in input order
+    with their cells interleaved: 12,800 entries cycling over the 64 cells of one brick
+    in shuffled order, attributes 0..3 (0 deletes), so that each cell's last entry lies
+    anywhere in a run over several tiles and past their ends; out-of-range entries
+    (keys without brick bits) interleaved with brick 0's own voxels; other bricks
+    around both."""
+    rng = np.random.default_rng(23)
+    cyc = np.concatenate([rng.permutation(64) for _ in range(200)])
+    brick = np.stack([4 + (cyc & 3), 4 + ((cyc >> 2) & 3), 4 + (cyc >> 4), rng.integers(0, 4, len(cyc))], 1)
+    b0 = np.concatenate([rng.integers(0, 4, (300, 3)), rng.integers(0, 4, (300, 1))], 1)
+    bad = np.concatenate([rng.integers(32, 40, (150, 1)), rng.integers(0, 4, (150, 2)), rng.integers(0, 4, (150, 1))], 1)
+    bad = np.concatenate([bad, np.array([[0xFFFFFFFF, 1, 1, 3]] * 150)])
+    mixed = np.concatenate([b0, bad])[rng.permutation(600)]
+    other = np.concatenate([rng.integers(8, 32, (2000, 3)), rng.integers(0, 4, (2000, 1))], 1)
+    pts = np.concatenate([other[:1000], brick, mixed, other[1000:], brick[:100]]).astype(np.uint32)
+    o = orc.gb_build(5, 3, pts)
+    old = gb.get_tuning()
+    try:
+        gb.set_tuning(tuning[0], tuning[1], 50, old.path)
+        g = gb.build(5, 3, dev(pts)).download()
+    finally:
+        gb.set_tuning(old.radix_bits, old.tile_keys, old.load_factor_pct, old.path)
+    assert_same_build(g, o, label=f"interleaved cells, tuning {tuning}")
+
+
 @pytest.mark.parametrize("lf", [50, 25])
 def test_leaf_table_regions_with_repeated_masks(gb, lf):
     """A leaf table larger than one region (64 MB; here at load factor 25 %) is filled
