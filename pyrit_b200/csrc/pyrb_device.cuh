@@ -227,6 +227,31 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* smem, 
     return r;
 }
 
+// The same scan with one barrier: every warp adds up the NW warp sums itself. The
+// caller must not write smem[0, NW) again before every thread has returned (a second
+// scan takes another buffer, or a barrier comes first).
+template <int NW = kWarps>
+__device__ __forceinline__ uint32_t block_excl_scan1(uint32_t v, uint32_t* smem, uint32_t* total) {
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= unsigned(o)) x += y;
+    }
+    if (lane == 31) smem[warp] = x;
+    __syncthreads();
+    uint32_t pre = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const uint32_t s = smem[w];
+        pre += unsigned(w) < warp ? s : 0u;
+        tot += s;
+    }
+    *total = tot;
+    return pre + x - v;
+}
+
 // 64-bit variant (two 31-bit fields packed are added together safely).
 __device__ __forceinline__ uint64_t block_excl_scan64(uint64_t v, uint64_t* smem, uint64_t* total) {
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     uint16_t* s_head = reinterpret_cast<uint16_t*>(s_key + TILE);  // [TILE] first entry of each run
     uint16_t* s_dst = s_head + TILE;                               // [TILE] a kept winner's place in the tile's voxels
     __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_scan[2 * kWarps + 2];
+    __shared__ uint32_t s_scan[2 * kWarps];  // warp sums of the two scans
     __shared__ uint64_t s_ubase, s_bbase, s_tcells, s_tkeep;
     __shared__ uint32_t s_tpos[64], s_tval[64];     // past the end: last entry (+1) and attribute per cell
     __shared__ uint32_t s_rcount[kMaxLeafRegions];  // the tile's bricks per leaf-table region
@@ -599,6 +599,16 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
             ra_v = vals[e_end + lane];
         }
     }
+    // no destination yet for any entry (IT 16-bit words per thread, 16 bytes a store)
+    static_assert(IT % 8 == 0 || IT < 8, "whole 16-byte stores, or the scalar loop");
+    if constexpr (IT % 8 == 0) {
+#pragma unroll
+        for (int q = 0; q < IT / 8; ++q)
+            reinterpret_cast<uint4*>(s_dst + threadIdx.x * IT)[q] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+    } else {
+#pragma unroll
+        for (int q = 0; q < IT; ++q) s_dst[threadIdx.x * IT + q] = kNoDst;
+    }
     uint32_t v[IT];  // the attributes stay in registers until the voxels are written
     unsigned hb[IT];  // runs that start in the tile: an entry whose brick differs from the one before it
     uint32_t wheads = 0;
@@ -623,10 +633,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
             const KeyT pb = lane > 0 ? brick(up) : j > 0 ? brick(row_prev) : kprev;
             hb[j] = __ballot_sync(kFull, in && brick(k[j]) != pb);
             wheads += __popc(hb[j]);
-            if (in) {
-                s_key[idx] = k[j] | (v[j] == 0 ? zero : KeyT(0));
-                s_dst[idx] = kNoDst;
-            }
+            if (in) s_key[idx] = k[j] | (v[j] == 0 ? zero : KeyT(0));
         }
         if (warp == RA) {
             // the tile's last run, if it started here, may go on past the end (only a
@@ -666,7 +673,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     }
     uint32_t R;
     {
-        uint32_t hexcl = block_excl_scan(lane == 0 ? wheads : 0u, s_scan, &R);
+        uint32_t hexcl = block_excl_scan1(lane == 0 ? wheads : 0u, s_scan, &R);
         hexcl = __shfl_sync(kFull, hexcl, 0);
 #pragma unroll
         for (int j = 0; j < IT; ++j) {
@@ -713,7 +720,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
         packed += (uint32_t(__popcll(km)) << 16) + (km != 0 ? 1u : 0u);
     }
     uint32_t ptotal;
-    const uint32_t pexcl = block_excl_scan(packed, s_scan, &ptotal);
+    const uint32_t pexcl = block_excl_scan1(packed, s_scan + kWarps, &ptotal);
     const uint32_t total = ptotal >> 16, btotal = ptotal & 0xFFFFu;
     // positions are global over all segments: the last warp publishes the tile's voxel
     // and brick counts as one status word (voxels << 31 | bricks: both stay below 2^31)
