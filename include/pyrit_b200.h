@@ -81,7 +81,7 @@ typedef struct pyrb_stats {
     uint32_t brick_count;            /* non-empty 4^3 bricks (B) */
     uint32_t level_parents[24];      /* P_l: parent nodes of level l before dedup (l = 2 .. log2-1) */
     uint32_t level_unique[24];       /* U_l: unique nodes of level l */
-    uint32_t sort_passes;            /* radix passes of the onesweep sort */
+    uint32_t sort_passes;            /* radix passes of the onesweep sort (over the 3 log2 - 6 brick bits) */
     uint32_t radix_bits;             /* widest digit */
     uint32_t kernel_launches;        /* kernels launched by the build */
     uint32_t reserved;
