@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     uint16_t* s_dst = s_head + TILE;                               // [TILE] a kept winner's place in the tile's voxels
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[2 * kWarps];  // warp sums of the two scans
-    __shared__ uint64_t s_ubase, s_bbase, s_tcells, s_tkeep;
+    __shared__ uint64_t s_ubase, s_bbase;
     __shared__ uint32_t s_tpos[64], s_tval[64];     // past the end: last entry (+1) and attribute per cell
     __shared__ uint32_t s_rcount[kMaxLeafRegions];  // the tile's bricks per leaf-table region
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -586,14 +586,13 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     const bool regions = d.leaf_regions > 1;
     if (threadIdx.x < kMaxLeafRegions) s_rcount[threadIdx.x] = 0;
 
-    // the read-ahead warp's first loads go out with the tile's: the entry before the
-    // tile and the 32 after it (a tile short of TILE entries ends its segment)
-    KeyT lead = NONE, ra_k = NONE;
+    // the read-ahead warp's first loads go out with the tile's: the 32 entries after
+    // the tile (a tile short of TILE entries ends its segment)
+    KeyT ra_k = NONE, klast = NONE;
     uint32_t ra_v = 0;
     if (warp == RA) {
         s_tpos[lane] = 0;
         s_tpos[lane + 32] = 0;
-        if (sp.count > 0 && sp.start > seg_begin) lead = brick(keys[sp.start - 1]);
         if (sp.count > 0 && e_end + lane < seg_end) {
             ra_k = keys[e_end + lane];
             ra_v = vals[e_end + lane];
@@ -635,12 +634,28 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
             wheads += __popc(hb[j]);
             if (in) s_key[idx] = k[j] | (v[j] == 0 ? zero : KeyT(0));
         }
-        if (warp == RA) {
-            // the tile's last run, if it started here, may go on past the end (only a
-            // full tile can have entries after it: its last entry is this lane 31's)
-            const KeyT klast = __shfl_sync(kFull, k[IT - 1], 31);
-            __syncwarp();  // the cleared s_tpos before any lane's atomicMax
-            if (sp.count > 0 && e_end < seg_end && brick(klast) != lead) {
+        // the tile's last entry (only a full tile can have entries after it: its last
+        // entry is the read-ahead warp's lane 31's)
+        klast = __shfl_sync(kFull, k[IT - 1], 31);
+    }
+    uint32_t R;
+    {
+        uint32_t hexcl = block_excl_scan1(lane == 0 ? wheads : 0u, s_scan, &R);
+        hexcl = __shfl_sync(kFull, hexcl, 0);
+#pragma unroll
+        for (int j = 0; j < IT; ++j) {
+            if ((hb[j] >> lane) & 1) s_head[hexcl + __popc(hb[j] & lanemask_lt())] = uint16_t(wbase + j * 32 + lane);
+            hexcl += __popc(hb[j]);
+        }
+    }
+    __syncthreads();
+    // The tile's last run (it started here when R > 0) may go on past the tile's end:
+    // the read-ahead warp keeps per cell the last entry there, while the other warps
+    // walk the other runs; its lane 0 then walks the last run.
+    uint64_t tcells = 0, tkeep = 0;
+    if (warp == RA) {
+        if (R > 0 && e_end < seg_end) {
+            {  // the cleared s_tpos is visible: block barriers since
                 const KeyT rb = brick(klast);
                 uint32_t base = e_end;
                 KeyT kk = ra_k;
@@ -661,34 +676,27 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
                     vv = e2 < seg_end ? vals[e2] : 0u;
                 }
             }
-            const uint32_t pa = s_tpos[lane], pb = s_tpos[lane + 32];
-            const unsigned ca = __ballot_sync(kFull, pa != 0), cb = __ballot_sync(kFull, pb != 0);
-            const unsigned ka = __ballot_sync(kFull, pa != 0 && s_tval[lane] != 0);
-            const unsigned kb = __ballot_sync(kFull, pb != 0 && s_tval[lane + 32] != 0);
-            if (lane == 0) {
-                s_tcells = uint64_t(cb) << 32 | ca;
-                s_tkeep = uint64_t(kb) << 32 | ka;
-            }
         }
+        const uint32_t pa = s_tpos[lane], pb = s_tpos[lane + 32];
+        const unsigned ca = __ballot_sync(kFull, pa != 0), cb = __ballot_sync(kFull, pb != 0);
+        const unsigned ka = __ballot_sync(kFull, pa != 0 && s_tval[lane] != 0);
+        const unsigned kb = __ballot_sync(kFull, pb != 0 && s_tval[lane + 32] != 0);
+        tcells = uint64_t(cb) << 32 | ca;
+        tkeep = uint64_t(kb) << 32 | ka;
     }
-    uint32_t R;
-    {
-        uint32_t hexcl = block_excl_scan1(lane == 0 ? wheads : 0u, s_scan, &R);
-        hexcl = __shfl_sync(kFull, hexcl, 0);
-#pragma unroll
-        for (int j = 0; j < IT; ++j) {
-            if ((hb[j] >> lane) & 1) s_head[hexcl + __popc(hb[j] & lanemask_lt())] = uint16_t(wbase + j * 32 + lane);
-            hexcl += __popc(hb[j]);
-        }
-    }
-    __syncthreads();
-    // kept cells of each run (thread t of the first kRunThreads takes runs [t q, t q + q);
-    // the last warp is left free for the look-back); the last run starts from the cells
-    // seen past the tile's end
+    // kept cells of each run: thread t of the first kRunThreads takes runs [t q, t q + q)
+    // of all but the last, the read-ahead warp's lane 0 the last one (it starts from the
+    // cells seen past the tile's end); the read-ahead warp then looks back
     constexpr uint32_t kRunThreads = kBlock - 32;
-    const uint64_t tcells = s_tcells, tkeep = s_tkeep;
-    const uint32_t q = (R + kRunThreads - 1) / kRunThreads;
-    const uint32_t r_lo = threadIdx.x < kRunThreads ? min(threadIdx.x * q, R) : R, r_hi = min(r_lo + q, R);
+    const uint32_t Rw = R > 0 ? R - 1 : 0;
+    const uint32_t q = (Rw + kRunThreads - 1) / kRunThreads;
+    uint32_t r_lo = R, r_hi = R;
+    if (threadIdx.x < kRunThreads) {
+        r_lo = min(threadIdx.x * q, Rw);
+        r_hi = min(r_lo + q, Rw);
+    } else if (threadIdx.x == kRunThreads && R > 0) {
+        r_lo = R - 1;
+    }
     auto run_end = [&](uint32_t r) -> uint32_t { return r + 1 < R ? uint32_t(s_head[r + 1]) : sp.count; };
     // a run from its last entry back, 4 entries a step (their loads in flight together);
     // visit(i, first_sighting_bit, k) for each entry
@@ -722,19 +730,12 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
     uint32_t ptotal;
     const uint32_t pexcl = block_excl_scan1(packed, s_scan + kWarps, &ptotal);
     const uint32_t total = ptotal >> 16, btotal = ptotal & 0xFFFFu;
-    // positions are global over all segments: the last warp publishes the tile's voxel
-    // and brick counts as one status word (voxels << 31 | bricks: both stay below 2^31)
-    // and looks back to tile 0 for both offsets at once, while the others place the
-    // winners
-    if (warp == kWarps - 1) {
-        const uint64_t agg = uint64_t(total) << 31 | btotal;
-        if (lane == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | agg);
-        const uint64_t ex = lookback_warp(d.uniq_status, tile, 0, agg, d.counters + kCtrError);
-        if (lane == 0) {
-            s_ubase = ex >> 31;
-            s_bbase = ex & 0x7FFFFFFFull;
-        }
-    }
+    // positions are global over all segments: the read-ahead warp publishes the tile's
+    // voxel and brick counts as one status word (voxels << 31 | bricks: both stay below
+    // 2^31), places the last run's winners and looks back to tile 0 for both offsets at
+    // once, while the others place the winners of their runs
+    const uint64_t agg = uint64_t(total) << 31 | btotal;
+    if (warp == RA && lane == 0 && tile != 0) st_relaxed(d.uniq_status + tile, kFlagAgg | agg);
     // each kept cell's winner goes to the rank of its cell in the brick's mask
     {
         uint32_t uo = pexcl >> 16;
@@ -746,6 +747,13 @@ __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin)
                 if (nb & km) s_dst[i] = uint16_t(uo + __popcll(km & (nb - 1)));
             });
             uo += uint32_t(__popcll(km));
+        }
+    }
+    if (warp == RA) {
+        const uint64_t ex = lookback_warp(d.uniq_status, tile, 0, agg, d.counters + kCtrError);
+        if (lane == 0) {
+            s_ubase = ex >> 31;
+            s_bbase = ex & 0x7FFFFFFFull;
         }
     }
     __syncthreads();
