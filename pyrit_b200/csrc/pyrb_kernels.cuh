@@ -550,7 +550,7 @@ template <int IT, typename KeyT>
 __global__ void __launch_bounds__(kBlock, 5) k_unique(BuildDesc d, uint32_t fin) {
     grid_dep_wait();
     constexpr int TILE = kBlock * IT;
-    constexpr unsigned RA = kWarps - 1;  // the warp that reads past the tile's end
+    constexpr unsigned RA = kWarps - 1;  // reads past the tile's end, takes its last run, looks back
     constexpr uint16_t kNoDst = 0xFFFF;
     extern __shared__ __align__(16) unsigned char usmem[];
     KeyT* s_key = reinterpret_cast<KeyT*>(usmem);                  // [TILE] the tile's keys (+ zero flag)
